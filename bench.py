@@ -1,0 +1,328 @@
+"""Benchmark: explicit DG time stepping on one B200 (and N replicas on N GPUs).
+
+Workload (the largest single-GPU configuration): 3D linear advection,
+a = (1, 0.7, 0.3), 64^3 periodic hexahedra on [0,1]^3, hpGEM's default basis
+of order p = 3 (64 DoF per element, 16,777,216 DoF), classical RK4,
+dt = 2e-4, FP64; initial condition the Gaussian bump exp(-|x-0.5|^2/0.01),
+L2-projected.  Synthetic mesh from the structured description, so no data
+files.
+
+A "step" is one RK4 time step of the whole mesh (4 stage kernels).
+  value   DoF-updates/s = elements * basis functions * steps / device time,
+          state resident in HBM, CUDA events on the launching stream, max
+          over ranks; each rank advances its own copy of the mesh
+          (independent replicas, weak scaling).
+  e2e     the same metric through the C ABI with host buffers: per e2e step,
+          one full 200-step solve including the host->device copy of the
+          initial coefficients (pinned) and the device->host copy of the result.
+The five state vectors (134 MB each) exceed the 126 MB L2, so no flush is
+needed between steps.
+
+--impl reference times the CPU oracle (the restated hpGEM loop: quadrature
+loops, per-element mass matrix rebuilt and LU-solved every stage) on all host
+cores as independent replica processes, each on a 2^3 sample of the same mesh
+family (same order, same per-element work), one RK4 step per bench step.
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "DG DoF-updates/s FP64 vs FP32-mixed at stated error; served p50/p99 latency"
+UNIT = "DoF-updates/s"
+N_CELLS = 64
+ORDER = 3
+ADV = [1.0, 0.7, 0.3]
+DT = 2e-4
+SOLVE_STEPS = 200
+# algorithmic bytes per DoF-update of one RK4 step (stored-stage RK4, FP64):
+# state 16 + 24 + 24 + 48 = 112 B, plus per-stage geometry
+# 4 * (G_e + (F/E) G_f) / nB = 4 * (80 + 3 * 48) / 64 = 14 B
+B_ALG = 112.0 + 4.0 * (8 * (3 * 3 + 1) + 3 * (8 * (3 + 1) + 16)) / 64.0
+
+
+def description(n):
+    return "structured 1 3\n%d %d %d\n0 0 0\n1 1 1\nrectangular\ntrue true true\n" % (n, n, n)
+
+
+def bump(x):
+    return np.exp(-((x - 0.5) ** 2).sum(axis=1) / 0.01)
+
+
+def config():
+    return {"workload": "advection3d_hex64_p3_rk4", "mesh": "64^3 periodic hexahedra",
+            "order": ORDER, "dof": N_CELLS ** 3 * (ORDER + 1) ** 3, "velocity": ADV, "dt": DT,
+            "tableau": "RK4_4", "form": "fp64", "flush": "none: 5 state vectors of 134 MB exceed L2"}
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled while the timed region runs."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "20"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 8:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        sm = [float(r[0]) for r in rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[4 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
+
+
+def traffic_per_dof_stage():
+    """DRAM bytes per DoF and stage launch from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f).get("tensor_stage_hex_p3_bytes_per_dof_launch")
+    except (OSError, ValueError):
+        return None
+
+
+def measured_peak_hbm():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, ValueError, KeyError):
+        return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+def cpu_sample_rate(budget_s=12.0):
+    """The oracle on one core: 4^3 hexahedra, p = 3, RK4 steps until the budget is used."""
+    from oracle.dg import ADVECTION, Problem
+    from oracle.mesh import mesh_from_description
+
+    n = 4
+    prob = Problem(mesh_from_description(description(n)), ORDER, ADVECTION, a=ADV)
+    u = prob.project(lambda x: bump(x)[:, None])
+    steps, t0 = 0, time.perf_counter()
+    while True:
+        u = prob.step(u, DT, 1, "RK4_4")
+        steps += 1
+        el = time.perf_counter() - t0
+        if el > budget_s or steps >= 1000:
+            break
+    return prob.n_dof * steps / el, "%d^3 hexahedra p=3 (%d DoF), %d RK4 steps, %.1f s" % (
+        n, prob.n_dof, steps, el)
+
+
+def _replica(args):
+    n_steps, n_warm, barrier_time = args
+    from oracle.dg import ADVECTION, Problem
+    from oracle.mesh import mesh_from_description
+
+    prob = Problem(mesh_from_description(description(2)), ORDER, ADVECTION, a=ADV)
+    u = prob.project(lambda x: bump(x)[:, None])
+    u = prob.step(u, DT, n_warm, "RK4_4") if n_warm else u
+    while time.time() < barrier_time:
+        time.sleep(0.001)
+    t0 = time.perf_counter()
+    u = prob.step(u, DT, n_steps, "RK4_4")
+    return time.perf_counter() - t0, prob.n_dof
+
+
+def run_reference(args):
+    import multiprocessing as mp
+
+    from oracle.build import build as build_oracle
+
+    build_oracle()
+    cores = os.cpu_count() or 1
+    ctx = mp.get_context("spawn")
+    start_at = time.time() + 5.0 + 0.5 * cores
+    with ctx.Pool(cores) as pool:
+        res = pool.map(_replica, [(args.steps, args.warmup, start_at)] * cores)
+    wall = max(r[0] for r in res)
+    dof = res[0][1]
+    value = dof * cores * args.steps / wall
+    sample = ("%d replica processes, each 2^3 periodic hexahedra p=3 (%d DoF), %d timed RK4 "
+              "steps after %d warm-up" % (cores, dof, args.steps, args.warmup))
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * wall / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": config(),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+def run_ours(args):
+    import torch
+
+    import hpgem_b200
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    solver = hpgem_b200.Advection(3, ORDER, ADV, tableau="RK4_4").readMesh(description(N_CELLS))
+    h = solver.handle
+    ndof = h.vector_length
+    solver.setInitialSolution(bump)
+    u0 = solver.getTimeIntegrationVector(0).reshape(-1).copy()
+    stream = torch.cuda.current_stream()
+    h.set_stream(stream.cuda_stream)
+    h.set_store_last_stage(False)
+    assert h.kernel_kind == "tensor"
+
+    # warm-up
+    t = h.step(0.0, DT, max(args.warmup, 3))
+    torch.cuda.synchronize()
+
+    sampler = ClockSampler(dev)
+    sampler.start()
+    time.sleep(0.2)
+    launches0 = h.launch_count
+    barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    t = h.step(t, DT, args.steps)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clocks = sampler.stop()
+    launches = h.launch_count - launches0
+    ms = ev0.elapsed_time(ev1)
+    if dist is not None:
+        tt = torch.tensor([ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    value = ndof * args.steps * world / (ms / 1e3)
+
+    # end to end: host initial coefficients in, host solution out, one 200-step solve each
+    host_in = torch.from_numpy(u0).pin_memory()
+    host_out = torch.empty_like(host_in).pin_memory()
+    reps = 2
+    h.step(0.0, DT, 1)
+    torch.cuda.synchronize()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        h.set_state_ptr(0, host_in.data_ptr())
+        h.step(0.0, DT, SOLVE_STEPS)
+        h.get_state_ptr(0, host_out.data_ptr())
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    e2e_ms = e0.elapsed_time(e1) / reps
+    if dist is not None:
+        tt = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_ms = float(tt.item())
+    e2e_value = ndof * SOLVE_STEPS * world / (e2e_ms / 1e3)
+    finite = bool(np.isfinite(host_out.numpy()).all())
+
+    peak, peak_kind = measured_peak_hbm()
+    step_s = (ms / 1e3) / args.steps
+    achieved = B_ALG * ndof / step_s / 1e9
+    tr = traffic_per_dof_stage()
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": dict(config(), parallelism="replicas%d" % world),
+            "clocks": clocks,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": ndof * 8,
+                    "d2h_bytes_per_step": ndof * 8, "step": "one %d-step solve" % SOLVE_STEPS,
+                    "ms_per_step": e2e_ms, "finite": finite},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind,
+                         "kernel": "tensor_stage<3,3,4>",
+                         "algorithmic_bytes_per_dof_update": B_ALG,
+                         "traffic": (tr * ndof * 4 if tr else None),
+                         "traffic_unit": "bytes per RK4 step (4 launches)"}}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, sample = cpu_sample_rate()
+        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
+                                "sample": sample}
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        if int(os.environ.get("RANK", "0")) != 0:
+            return
+        run_reference(args)
+        return
+    run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,573 @@
+// C ABI of hpgem_b200 (include/hpgem_b200.h): handle management, device
+// buffers, stage launches and CUDA-graph capture of the Runge-Kutta step.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/hpgem_b200.h"
+#include "dg_kernels.cuh"
+#include "host/operators.h"
+#include "host/setup.h"
+
+using namespace hgg;
+
+namespace {
+
+thread_local std::string g_create_error = "no error";
+
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+};
+
+}  // namespace
+
+struct hgg_handle {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr;
+    HostOperators op;
+    std::unique_ptr<StructuredProblem> sp;  // set when built from a structured description
+    int S = 0;
+    std::vector<double> rk_a, rk_b, rk_c;
+    int64_t N = 0;                 // doubles per vector
+    double *sol[2] = {nullptr, nullptr};
+    int cur = 0;                   // which sol[] holds the solution
+    std::vector<double *> k;       // S stage vectors
+    std::vector<DevBuf> bufs;      // every device allocation
+    // device operator / geometry arrays
+    double *d_vol = nullptr, *d_pairs = nullptr, *d_elem_geo = nullptr, *d_face_geo = nullptr;
+    int32_t *d_nbr = nullptr, *d_self = nullptr, *d_nbrp = nullptr;
+    int8_t *d_mode = nullptr;
+    double *d_ahat = nullptr, *d_tsigma = nullptr;
+    int32_t *d_tnbr = nullptr;
+    int8_t *d_tmode = nullptr;
+    int *d_status = nullptr;
+    bool store_last = true;
+    int64_t launches = 0;
+    // graph of one full step, per starting buffer, valid for (dt, store_last)
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    double graph_dt = 0.0;
+    bool graph_store_last = true;
+    std::string err = "no error";
+};
+
+namespace {
+
+int fail(hgg_handle *h, int code, const std::string &msg) {
+    if (h) h->err = msg;
+    else g_create_error = msg;
+    return code;
+}
+
+#define HGG_CUDA(h, call)                                                                    \
+    do {                                                                                     \
+        cudaError_t _e = (call);                                                             \
+        if (_e != cudaSuccess)                                                               \
+            return fail(h, HGG_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(_e)); \
+    } while (0)
+
+template <typename T>
+int upload(hgg_handle *h, const std::vector<T> &v, T **dst) {
+    *dst = nullptr;
+    if (v.empty()) return 0;
+    void *p = nullptr;
+    size_t bytes = v.size() * sizeof(T);
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) return fail(h, HGG_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    h->bufs.push_back({p, bytes});
+    e = cudaMemcpyAsync(p, v.data(), bytes, cudaMemcpyHostToDevice, h->stream);
+    if (e != cudaSuccess) return fail(h, HGG_ERR_CUDA, std::string("cudaMemcpyAsync: ") + cudaGetErrorString(e));
+    *dst = (T *)p;
+    return 0;
+}
+
+int alloc(hgg_handle *h, size_t bytes, void **dst) {
+    void *p = nullptr;
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) return fail(h, HGG_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    h->bufs.push_back({p, bytes});
+    *dst = p;
+    return 0;
+}
+
+void release_graphs(hgg_handle *h) {
+    for (auto &g : h->graph)
+        if (g) {
+            cudaGraphExecDestroy(g);
+            g = nullptr;
+        }
+}
+
+// ---- kernel dispatch ---------------------------------------------------------
+template <int P, int DIM>
+int launch_tensor(hgg_handle *h, const StageIO &io) {
+    using TC = TensorConsts<P, DIM>;
+    constexpr int EPB = (256 / TC::NB) > 0 ? (256 / TC::NB) : 1;
+    TC tc;
+    const HostOperators &op = h->op;
+    for (int i = 0; i < TC::NP * TC::NP; ++i) tc.D1[i] = op.D1[i];
+    for (int i = 0; i < 2 * TC::NP; ++i) tc.lift[i] = op.lift[i];
+    tc.trace_pos[0] = op.trace_pos[0];
+    tc.trace_pos[1] = op.trace_pos[1];
+    for (int i = 0; i < TC::NB; ++i) {
+        tc.tpos[i] = (short)op.tpos[i];
+        tc.tinv[op.tpos[i]] = (short)i;
+        tc.tsign[i] = op.tsign[i];
+    }
+    TensorGeom geo{h->d_ahat, h->d_tnbr, h->d_tmode, h->d_tsigma};
+    int64_t blocks = (op.nE + EPB - 1) / EPB;
+    tensor_stage<P, DIM, EPB><<<(unsigned)blocks, EPB * TC::NB, 0, h->stream>>>(io, geo, tc);
+    return 0;
+}
+
+template <int DIM>
+int launch_tensor_dim(hgg_handle *h, const StageIO &io) {
+    switch (h->op.order) {
+        case 1: return launch_tensor<1, DIM>(h, io);
+        case 2: return launch_tensor<2, DIM>(h, io);
+        case 3: return launch_tensor<3, DIM>(h, io);
+        case 4: return launch_tensor<4, DIM>(h, io);
+        case 5: return launch_tensor<5, DIM>(h, io);
+    }
+    return fail(h, HGG_ERR_UNSUPPORTED, "tensor kernel: order out of range");
+}
+
+template <int DIM, int NFL, int WAVE>
+int launch_dense(hgg_handle *h, const StageIO &io) {
+    const HostOperators &op = h->op;
+    const int V = WAVE ? DIM + 1 : 1;
+    const int R = V * op.nB;
+    if (R > 256) return fail(h, HGG_ERR_UNSUPPORTED, "dense kernel: more than 256 coefficients per element");
+    int epb = std::max(1, 256 / R);
+    DenseGeom g{h->d_vol, h->d_pairs, h->d_nbr, h->d_self, h->d_nbrp, h->d_mode,
+                h->d_elem_geo, h->d_face_geo, 1.0 / op.c_inv, op.nB, epb};
+    size_t smem = sizeof(double) * (size_t)epb * R * (1 + NFL);
+    if (smem > 48 * 1024) {
+        cudaFuncSetAttribute(dense_stage<DIM, NFL, WAVE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
+    }
+    int64_t blocks = (op.nE + epb - 1) / epb;
+    int threads = ((epb * R + 31) / 32) * 32;
+    dense_stage<DIM, NFL, WAVE><<<(unsigned)blocks, threads, smem, h->stream>>>(io, g);
+    return 0;
+}
+
+int launch_stage(hgg_handle *h, const StageIO &io) {
+    const HostOperators &op = h->op;
+    int rc;
+    if (op.tensor) {
+        rc = op.dim == 2 ? launch_tensor_dim<2>(h, io)
+                         : (op.dim == 3 ? launch_tensor_dim<3>(h, io)
+                                        : fail(h, HGG_ERR_UNSUPPORTED, "tensor kernel needs dim 2 or 3"));
+    } else {
+        const bool wave = op.physics == HGG_PHYSICS_WAVE;
+        switch (op.shape) {
+            case HGG_SHAPE_LINE: rc = wave ? launch_dense<1, 2, 1>(h, io) : launch_dense<1, 2, 0>(h, io); break;
+            case HGG_SHAPE_TRIANGLE: rc = wave ? launch_dense<2, 3, 1>(h, io) : launch_dense<2, 3, 0>(h, io); break;
+            case HGG_SHAPE_SQUARE: rc = wave ? launch_dense<2, 4, 1>(h, io) : launch_dense<2, 4, 0>(h, io); break;
+            case HGG_SHAPE_TETRAHEDRON: rc = wave ? launch_dense<3, 4, 1>(h, io) : launch_dense<3, 4, 0>(h, io); break;
+            case HGG_SHAPE_CUBE: rc = wave ? launch_dense<3, 6, 1>(h, io) : launch_dense<3, 6, 0>(h, io); break;
+            default: rc = fail(h, HGG_ERR_UNSUPPORTED, "shape");
+        }
+    }
+    if (rc) return rc;
+    h->launches++;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(h, HGG_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+    return 0;
+}
+
+double *vector_ptr(hgg_handle *h, int vec) {
+    if (vec == 0) return h->sol[h->cur];
+    if (vec >= 1 && vec <= h->S) return h->k[vec - 1];
+    return nullptr;
+}
+
+// One Runge-Kutta step from sol[from] into sol[1 - from] (stages as in
+// HpgemAPISimplified_Impl.h:788-820; zero tableau entries are skipped).
+int enqueue_step(hgg_handle *h, int from, double dt) {
+    const int S = h->S;
+    const double *u = h->sol[from];
+    for (int i = 0; i < S; ++i) {
+        StageIO io{};
+        io.u = u;
+        io.n_elements = h->op.nE;
+        io.status = h->d_status;
+        for (int j = 0; j < i; ++j) {
+            double c = dt * h->rk_a[i * S + j];
+            if (c != 0.0) {
+                io.kin[io.nin] = h->k[j];
+                io.cin[io.nin] = c;
+                io.nin++;
+            }
+        }
+        const bool last = i == S - 1;
+        io.kout = (!last || h->store_last) ? h->k[i] : nullptr;
+        if (last) {
+            io.unew = h->sol[1 - from];
+            for (int j = 0; j < S - 1; ++j) {
+                double b = dt * h->rk_b[j];
+                if (b != 0.0) {
+                    io.kfin[io.nfin] = h->k[j];
+                    io.bfin[io.nfin] = b;
+                    io.nfin++;
+                }
+            }
+            io.blast = dt * h->rk_b[S - 1];
+        }
+        int rc = launch_stage(h, io);
+        if (rc) return rc;
+    }
+    return 0;
+}
+
+int check_status(hgg_handle *h) {
+    int st = 0;
+    HGG_CUDA(h, cudaMemcpyAsync(&st, h->d_status, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    HGG_CUDA(h, cudaStreamSynchronize(h->stream));
+    if (st) return fail(h, HGG_ERR_DEVICE, "kernel status word " + std::to_string(st) + " (bad neighbour index)");
+    return 0;
+}
+
+int create_from_desc(const hgg_problem_desc *desc, hgg_handle *h) {
+    try {
+        h->op = build_operators(*desc);
+    } catch (const std::exception &ex) {
+        return fail(h, HGG_ERR_INVALID, ex.what());
+    }
+    if (desc->n_stages < 1 || desc->n_stages > kMaxStages || !desc->rk_a || !desc->rk_b)
+        return fail(h, HGG_ERR_INVALID, "Butcher tableau must have 1..8 stages");
+    h->S = desc->n_stages;
+    h->rk_a.assign(desc->rk_a, desc->rk_a + h->S * h->S);
+    h->rk_b.assign(desc->rk_b, desc->rk_b + h->S);
+    h->rk_c = desc->rk_c ? std::vector<double>(desc->rk_c, desc->rk_c + h->S) : std::vector<double>(h->S, 0.0);
+    if (desc->precision != HGG_PRECISION_FP64)
+        return fail(h, HGG_ERR_UNSUPPORTED, "only the FP64 precision form is available in this build");
+    const HostOperators &op = h->op;
+    h->N = op.nE * op.V * op.nB;
+
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return fail(h, HGG_ERR_NOT_LOADED, "no CUDA device available");
+    HGG_CUDA(h, cudaGetDevice(&h->device));
+    HGG_CUDA(h, cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
+    h->stream = h->own_stream;
+    int rc;
+    for (int i = 0; i < 2; ++i)
+        if ((rc = alloc(h, sizeof(double) * h->N, (void **)&h->sol[i]))) return rc;
+    h->k.resize(h->S);
+    for (int i = 0; i < h->S; ++i)
+        if ((rc = alloc(h, sizeof(double) * h->N, (void **)&h->k[i]))) return rc;
+    for (int i = 0; i < 2; ++i) HGG_CUDA(h, cudaMemsetAsync(h->sol[i], 0, sizeof(double) * h->N, h->stream));
+    for (int i = 0; i < h->S; ++i) HGG_CUDA(h, cudaMemsetAsync(h->k[i], 0, sizeof(double) * h->N, h->stream));
+    if ((rc = alloc(h, sizeof(int), (void **)&h->d_status))) return rc;
+    HGG_CUDA(h, cudaMemsetAsync(h->d_status, 0, sizeof(int), h->stream));
+    if (op.tensor) {
+        if ((rc = upload(h, op.elem_geo, &h->d_ahat)) || (rc = upload(h, op.t_nbr, &h->d_tnbr)) ||
+            (rc = upload(h, op.t_mode, &h->d_tmode)) || (rc = upload(h, op.t_sigma, &h->d_tsigma)))
+            return rc;
+    } else {
+        if ((rc = upload(h, op.vol, &h->d_vol)) || (rc = upload(h, op.pairs, &h->d_pairs)) ||
+            (rc = upload(h, op.nbr, &h->d_nbr)) || (rc = upload(h, op.self_pair, &h->d_self)) ||
+            (rc = upload(h, op.nbr_pair, &h->d_nbrp)) || (rc = upload(h, op.mode, &h->d_mode)) ||
+            (rc = upload(h, op.elem_geo, &h->d_elem_geo)) || (rc = upload(h, op.face_geo, &h->d_face_geo)))
+            return rc;
+    }
+    HGG_CUDA(h, cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+void destroy_handle(hgg_handle *h) {
+    if (!h) return;
+    release_graphs(h);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    if (h->own_stream) cudaStreamSynchronize(h->own_stream);
+    for (auto &b : h->bufs) cudaFree(b.p);
+    if (h->own_stream) cudaStreamDestroy(h->own_stream);
+    delete h;
+}
+
+}  // namespace
+
+extern "C" {
+
+int hgg_create(const hgg_problem_desc *desc, hgg_handle **out) {
+    if (!desc || !out) return fail(nullptr, HGG_ERR_INVALID, "null argument");
+    *out = nullptr;
+    hgg_handle *h = new (std::nothrow) hgg_handle();
+    if (!h) return fail(nullptr, HGG_ERR_NOMEM, "host allocation failed");
+    int rc = create_from_desc(desc, h);
+    if (rc) {
+        g_create_error = h->err;
+        destroy_handle(h);
+        return rc;
+    }
+    *out = h;
+    return 0;
+}
+
+int hgg_destroy(hgg_handle *h) {
+    destroy_handle(h);
+    return 0;
+}
+
+const char *hgg_last_error(const hgg_handle *h) { return h ? h->err.c_str() : g_create_error.c_str(); }
+
+int hgg_set_state(hgg_handle *h, int32_t vec, const double *host) {
+    if (!h || !host) return fail(h, HGG_ERR_INVALID, "null argument");
+    double *d = vector_ptr(h, vec);
+    if (!d) return fail(h, HGG_ERR_INVALID, "vector id out of range");
+    HGG_CUDA(h, cudaMemcpyAsync(d, host, sizeof(double) * h->N, cudaMemcpyHostToDevice, h->stream));
+    HGG_CUDA(h, cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+int hgg_get_state(hgg_handle *h, int32_t vec, double *host) {
+    if (!h || !host) return fail(h, HGG_ERR_INVALID, "null argument");
+    double *d = vector_ptr(h, vec);
+    if (!d) return fail(h, HGG_ERR_INVALID, "vector id out of range");
+    HGG_CUDA(h, cudaMemcpyAsync(host, d, sizeof(double) * h->N, cudaMemcpyDeviceToHost, h->stream));
+    HGG_CUDA(h, cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+int hgg_step(hgg_handle *h, double *time, double dt, int32_t nsteps) {
+    if (!h || nsteps < 0) return fail(h, HGG_ERR_INVALID, "bad argument");
+    if (nsteps == 0) return 0;
+    if (!(dt == h->graph_dt && h->store_last == h->graph_store_last && h->graph[0] && h->graph[1])) {
+        release_graphs(h);
+        for (int from = 0; from < 2; ++from) {
+            cudaGraph_t g = nullptr;
+            HGG_CUDA(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+            int64_t before = h->launches;
+            int rc = enqueue_step(h, from, dt);
+            cudaError_t ce = cudaStreamEndCapture(h->stream, &g);
+            h->launches = before;  // capture does not launch
+            if (rc) {
+                if (g) cudaGraphDestroy(g);
+                return rc;
+            }
+            if (ce != cudaSuccess) return fail(h, HGG_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(ce));
+            cudaError_t ie = cudaGraphInstantiate(&h->graph[from], g, 0);
+            cudaGraphDestroy(g);
+            if (ie != cudaSuccess) return fail(h, HGG_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ie));
+        }
+        h->graph_dt = dt;
+        h->graph_store_last = h->store_last;
+    }
+    for (int s = 0; s < nsteps; ++s) {
+        HGG_CUDA(h, cudaGraphLaunch(h->graph[h->cur], h->stream));
+        h->launches += h->S;
+        h->cur = 1 - h->cur;
+        if (time) *time += dt;
+    }
+    return 0;
+}
+
+int hgg_time_derivative(hgg_handle *h, int32_t in_vec, int32_t out_vec) {
+    if (!h) return fail(h, HGG_ERR_INVALID, "null handle");
+    double *in = vector_ptr(h, in_vec), *outp = vector_ptr(h, out_vec);
+    if (!in || !outp || in == outp) return fail(h, HGG_ERR_INVALID, "bad vector ids");
+    StageIO io{};
+    io.u = in;
+    io.kout = outp;
+    io.n_elements = h->op.nE;
+    io.status = h->d_status;
+    int rc = launch_stage(h, io);
+    if (rc) return rc;
+    return check_status(h);
+}
+
+int hgg_synchronize(hgg_handle *h) {
+    if (!h) return fail(h, HGG_ERR_INVALID, "null handle");
+    HGG_CUDA(h, cudaStreamSynchronize(h->stream));
+    return check_status(h);
+}
+
+int64_t hgg_vector_length(const hgg_handle *h) { return h ? h->N : -1; }
+
+int hgg_kernel_kind(const hgg_handle *h) { return h ? (h->op.tensor ? 1 : 0) : -1; }
+
+int hgg_set_store_last_stage(hgg_handle *h, int32_t enable) {
+    if (!h) return fail(h, HGG_ERR_INVALID, "null handle");
+    h->store_last = enable != 0;
+    return 0;
+}
+
+int hgg_set_stream(hgg_handle *h, void *stream) {
+    if (!h) return fail(h, HGG_ERR_INVALID, "null handle");
+    HGG_CUDA(h, cudaStreamSynchronize(h->stream));
+    cudaStream_t s = stream ? (cudaStream_t)stream : h->own_stream;
+    if (s != h->stream) {
+        release_graphs(h);  // captured on the previous stream
+        h->stream = s;
+    }
+    return 0;
+}
+
+int64_t hgg_launch_count(const hgg_handle *h) { return h ? h->launches : -1; }
+
+// ---- stand-alone set-up ------------------------------------------------------
+
+namespace {
+void fill_descriptor(const StructuredProblem &P, int32_t precision, hgg_problem_desc &d) {
+    d = hgg_problem_desc{};
+    d.dim = P.mesh.dim;
+    d.shape = P.mesh.shape;
+    d.order = P.order;
+    d.n_vars = P.n_vars;
+    d.physics = P.physics;
+    d.precision = precision;
+    for (int i = 0; i < 3; ++i) d.advection[i] = P.advection[i];
+    d.c_inv = P.c_inv;
+    d.n_elements = P.mesh.n_elements;
+    d.n_basis = P.n_basis;
+    d.n_quad = P.rule.size();
+    d.quad_weights = P.rule.weights.data();
+    d.basis_values = P.basis_values.data();
+    d.basis_grads = P.basis_grads.data();
+    d.n_face_quad = P.face_rule.size();
+    d.face_weights = P.face_rule.weights.data();
+    d.n_face_tabs = P.n_face_tabs;
+    d.face_tabs = P.face_tabs.data();
+    d.jacobians = P.jacobians.data();
+    d.n_faces = P.mesh.n_faces();
+    d.face_elements = P.mesh.face_elements.data();
+    d.face_local = P.mesh.face_local.data();
+    d.face_tab_index = P.face_tab_index.data();
+    d.face_normals = P.normals.data();
+    d.n_stages = P.n_stages;
+    d.rk_a = P.rk_a.data();
+    d.rk_b = P.rk_b.data();
+    d.rk_c = P.rk_c.data();
+}
+}  // namespace
+
+int hgg_structured_descriptor(const char *description, int32_t order, int32_t physics, const double *params,
+                              const char *tableau, int32_t precision, hgg_problem_desc *out, void **owner) {
+    if (!description || !tableau || !out || !owner) return fail(nullptr, HGG_ERR_INVALID, "null argument");
+    *owner = nullptr;
+    StructuredProblem *sp = new (std::nothrow) StructuredProblem();
+    if (!sp) return fail(nullptr, HGG_ERR_NOMEM, "host allocation failed");
+    try {
+        *sp = build_structured(description, order, physics, params, tableau);
+    } catch (const std::exception &ex) {
+        delete sp;
+        return fail(nullptr, HGG_ERR_INVALID, ex.what());
+    }
+    fill_descriptor(*sp, precision, *out);
+    *owner = sp;
+    return 0;
+}
+
+void hgg_free_descriptor(void *owner) { delete static_cast<StructuredProblem *>(owner); }
+
+int hgg_create_structured(const char *description, int32_t order, int32_t physics, const double *params,
+                          const char *tableau, int32_t precision, hgg_handle **out) {
+    if (!description || !out || !tableau) return fail(nullptr, HGG_ERR_INVALID, "null argument");
+    *out = nullptr;
+    std::unique_ptr<StructuredProblem> sp(new StructuredProblem());
+    try {
+        *sp = build_structured(description, order, physics, params, tableau);
+    } catch (const std::exception &ex) {
+        return fail(nullptr, HGG_ERR_INVALID, ex.what());
+    }
+    hgg_problem_desc d;
+    fill_descriptor(*sp, precision, d);
+    hgg_handle *h = nullptr;
+    int rc = hgg_create(&d, &h);
+    if (rc) return rc;
+    h->sp = std::move(sp);
+    *out = h;
+    return 0;
+}
+
+int32_t hgg_num_quadrature_points(const hgg_handle *h) { return h && h->sp ? h->sp->rule.size() : -1; }
+
+int hgg_quadrature_points(const hgg_handle *h, double *xyz) {
+    if (!h || !xyz) return HGG_ERR_INVALID;
+    if (!h->sp) return fail(const_cast<hgg_handle *>(h), HGG_ERR_UNSUPPORTED, "handle not built from a structured mesh");
+    const StructuredProblem &P = *h->sp;
+    const int d = P.mesh.dim, nQ = P.rule.size();
+    for (int64_t e = 0; e < P.mesh.n_elements; ++e)
+        for (int q = 0; q < nQ; ++q) reference_to_physical(P.mesh, e, &P.rule.points[q * d], xyz + (e * nQ + q) * d);
+    return 0;
+}
+
+int32_t hgg_num_error_points(const hgg_handle *h) { return h && h->sp ? h->sp->error_rule.size() : -1; }
+
+int hgg_error_points(const hgg_handle *h, double *xyz) {
+    if (!h || !xyz) return HGG_ERR_INVALID;
+    if (!h->sp) return fail(const_cast<hgg_handle *>(h), HGG_ERR_UNSUPPORTED, "handle not built from a structured mesh");
+    const StructuredProblem &P = *h->sp;
+    const int d = P.mesh.dim, nQ = P.error_rule.size();
+    for (int64_t e = 0; e < P.mesh.n_elements; ++e)
+        for (int q = 0; q < nQ; ++q)
+            reference_to_physical(P.mesh, e, &P.error_rule.points[q * d], xyz + (e * nQ + q) * d);
+    return 0;
+}
+
+int hgg_project(hgg_handle *h, const double *values, int32_t vec) {
+    if (!h || !values) return fail(h, HGG_ERR_INVALID, "null argument");
+    if (!h->sp) return fail(h, HGG_ERR_UNSUPPORTED, "projection needs a handle built from a structured mesh");
+    const StructuredProblem &P = *h->sp;
+    const HostOperators &op = h->op;
+    const int nB = op.nB, V = op.V, nQ = P.rule.size();
+    // M^{-1} int phi u0 = Mhat^{-1} sum_q w_q phi u0(x_q): |J| and cInv cancel on affine elements
+    std::vector<double> out((size_t)h->N), rhs(nB);
+    for (int64_t e = 0; e < op.nE; ++e)
+        for (int v = 0; v < V; ++v) {
+            std::fill(rhs.begin(), rhs.end(), 0.0);
+            for (int q = 0; q < nQ; ++q) {
+                double val = P.rule.weights[q] * values[(e * nQ + q) * V + v];
+                for (int i = 0; i < nB; ++i) rhs[i] += val * P.basis_values[q * nB + i];
+            }
+            double *o = &out[(e * V + v) * nB];
+            for (int i = 0; i < nB; ++i) {
+                double s = 0.0;
+                for (int j = 0; j < nB; ++j) s += op.mass_inv[i * nB + j] * rhs[j];
+                o[i] = s;
+            }
+        }
+    return hgg_set_state(h, vec, out.data());
+}
+
+int hgg_l2_error(hgg_handle *h, int32_t vec, const double *exact, double *error) {
+    if (!h || !exact || !error) return fail(h, HGG_ERR_INVALID, "null argument");
+    if (!h->sp) return fail(h, HGG_ERR_UNSUPPORTED, "error norms need a handle built from a structured mesh");
+    if (h->sp->error_rule.size() == 0)
+        return fail(h, HGG_ERR_UNSUPPORTED, "no quadrature rule of order 2p+2 for this shape");
+    std::vector<double> u((size_t)h->N);
+    int rc = hgg_get_state(h, vec, u.data());
+    if (rc) return rc;
+    const StructuredProblem &P = *h->sp;
+    const HostOperators &op = h->op;
+    const int nB = op.nB, V = op.V, nQ = P.error_rule.size();
+    double total = 0.0;
+    for (int64_t e = 0; e < op.nE; ++e) {
+        double loc = 0.0;
+        for (int q = 0; q < nQ; ++q) {
+            double s = 0.0;
+            for (int v = 0; v < V; ++v) {
+                double uh = 0.0;
+                for (int j = 0; j < nB; ++j) uh += P.error_basis[q * nB + j] * u[(e * V + v) * nB + j];
+                double diff = exact[(e * nQ + q) * V + v] - uh;
+                s += diff * diff;
+            }
+            loc += P.error_rule.weights[q] * op.abs_det[e] * s;
+        }
+        total += loc;
+    }
+    *error = std::sqrt(std::fabs(total));
+    return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,312 @@
+// Runge-Kutta stage kernels of the explicit DG step (sm_100a, FP64).
+//
+// One launch = one Runge-Kutta stage of hpGEM's computeOneTimeStep
+// (kernel/Base/HpgemAPISimplified_Impl.h:788-820) for every element:
+//   w      = u + sum_j dt a_ij k_j                  (getLinearCombinationOfVectors, :599-620)
+//   k_i    = M^{-1} [ volume(w) + sum_faces flux ]  (computeRightHandSide :625-695 +
+//                                                    solveMassMatrixEquations :205-225)
+//   last stage only: u_new = u + sum_j dt b_j k_j    (scaleAndAddVector, :707-717, :812-816)
+// Each element gathers its own faces (element-centric, as hpGEM evaluates
+// every internal face once per side, :662-668): no atomics, deterministic.
+// The mass solve is folded into the reference operators (operators.h).
+//
+// Two kernel families:
+//   tensor_stage  hypercube advection, sum-factorised: the default H1 basis
+//                 is a signed tensor product of 1D hierarchical functions, so
+//                 the volume term is one 1D matrix per axis and every face
+//                 term is a 1D lift times a single-mode trace.
+//   dense_stage   any shape / physics: dense reference operators per element.
+#pragma once
+
+#include <cstdint>
+
+namespace hgg {
+
+constexpr int kMaxStages = 8;
+
+// Linear combination inputs and the fused final update of one stage.
+struct StageIO {
+    const double *u;                 // current solution
+    const double *kin[kMaxStages];   // stage vectors entering the stage input
+    double cin[kMaxStages];          // their coefficients dt * a_ij
+    int nin;
+    double *kout;                    // this stage's derivative (nullptr: not stored)
+    double *unew;                    // final stage: new solution (nullptr otherwise)
+    const double *kfin[kMaxStages];  // earlier stage vectors of the final update
+    double bfin[kMaxStages];         // their weights dt * b_j
+    int nfin;
+    double blast;                    // dt * b_S for the derivative computed in this stage
+    int64_t n_elements;
+    int *status;                     // device status word, bit 0: bad neighbour index
+};
+
+__device__ __forceinline__ double stage_input(const StageIO &io, int64_t idx) {
+    double w = io.u[idx];
+#pragma unroll 1
+    for (int j = 0; j < io.nin; ++j) w += io.cin[j] * io.kin[j][idx];
+    return w;
+}
+
+__device__ __forceinline__ void stage_output(const StageIO &io, int64_t idx, double u, double k) {
+    if (io.kout) io.kout[idx] = k;
+    if (io.unew) {
+        double r = u;
+#pragma unroll 1
+        for (int j = 0; j < io.nfin; ++j) r += io.bfin[j] * io.kfin[j][idx];
+        r += io.blast * k;
+        io.unew[idx] = r;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// sum-factorised hypercube advection
+// ---------------------------------------------------------------------------
+template <int P, int DIM>
+struct TensorConsts {
+    static constexpr int NP = P + 1;
+    static constexpr int NB = DIM == 2 ? NP * NP : NP * NP * NP;
+    static constexpr int NF = DIM == 2 ? NP : NP * NP;
+    static constexpr int NS = 2 * DIM;
+    double D1[NP * NP];
+    double lift[2 * NP];
+    int trace_pos[2];
+    short tpos[NB];    // hpGEM index -> tensor position (x fastest)
+    short tinv[NB];    // tensor position -> hpGEM index
+    double tsign[NB];  // sign of hpGEM function i relative to its tensor product
+};
+
+struct TensorGeom {
+    const double *ahat;    // [E][DIM]  J^{-1} a
+    const int32_t *nbr;    // [E][2*DIM] slots x-, x+, y-, y+, z-, z+
+    const int8_t *mode;    // [E][2*DIM]
+    const double *sigma;   // [E][2*DIM]
+};
+
+template <int P, int DIM, int EPB>
+__global__ void __launch_bounds__(EPB *TensorConsts<P, DIM>::NB)
+    tensor_stage(const StageIO io, const TensorGeom geo, const TensorConsts<P, DIM> tc) {
+    using TC = TensorConsts<P, DIM>;
+    constexpr int NP = TC::NP, NB = TC::NB, NF = TC::NF, NS = TC::NS;
+    __shared__ double W[EPB][NB];
+    __shared__ double TR[EPB][NS][NF];
+
+    const int tid = threadIdx.x;
+    const int el = tid / NB;
+    const int t = tid % NB;  // hpGEM basis index of this thread's DoF
+    const int64_t e0 = (int64_t)blockIdx.x * EPB;
+    const int64_t e = e0 + el;
+    const bool active = e < io.n_elements;
+
+    double u_own = 0.0;
+    if (active) {
+        const int64_t idx = e * NB + t;
+        u_own = io.u[idx];
+        double w = u_own;
+        for (int j = 0; j < io.nin; ++j) w += io.cin[j] * io.kin[j][idx];
+        W[el][tc.tpos[t]] = tc.tsign[t] * w;
+    }
+    __syncthreads();
+
+    // flux traces, already multiplied by sigma, per element slot
+    for (int i = tid; i < EPB * NS * NF; i += EPB * NB) {
+        const int l = i / (NS * NF);
+        const int s = (i / NF) % NS;
+        const int m = i % NF;
+        const int64_t ee = e0 + l;
+        double val = 0.0;
+        if (ee < io.n_elements) {
+            const int axis = s >> 1, side = s & 1;
+            const int8_t mode = geo.mode[ee * NS + s];
+            // tangential coordinates of trace entry m
+            int c[3];
+            if (DIM == 2) {
+                c[1 - axis] = m;
+            } else {
+                const int a0 = m % NP, a1 = m / NP;
+                if (axis == 0) { c[1] = a0; c[2] = a1; }
+                else if (axis == 1) { c[0] = a0; c[2] = a1; }
+                else { c[0] = a0; c[1] = a1; }
+            }
+            double tself = 0.0, tnbr = 0.0;
+            if (mode == 1 || mode == 3) {
+                c[axis] = tc.trace_pos[side];
+                int pos = c[0] + NP * c[1] + (DIM == 3 ? NP * NP * c[2] : 0);
+                tself = W[l][pos];
+            }
+            if (mode == 2 || mode == 3) {
+                const int32_t n = geo.nbr[ee * NS + s];
+                if (n >= 0 && n < io.n_elements) {
+                    c[axis] = tc.trace_pos[1 - side];
+                    int pos = c[0] + NP * c[1] + (DIM == 3 ? NP * NP * c[2] : 0);
+                    const int hi = tc.tinv[pos];
+                    tnbr = tc.tsign[hi] * stage_input(io, (int64_t)n * NB + hi);
+                } else {
+                    atomicOr(io.status, 1);
+                }
+            }
+            const double sg = geo.sigma[ee * NS + s];
+            val = mode == 1 ? sg * tself : (mode == 2 ? sg * tnbr : (mode == 3 ? 0.5 * sg * (tself + tnbr) : 0.0));
+        }
+        TR[l][s][m] = val;
+    }
+    __syncthreads();
+
+    if (!active) return;
+    const int pos = tc.tpos[t];
+    int a[3];
+    a[0] = pos % NP;
+    a[1] = (pos / NP) % NP;
+    a[2] = DIM == 3 ? pos / (NP * NP) : 0;
+    double acc = 0.0;
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) {
+        const double ah = geo.ahat[e * DIM + c];
+        const int stride = c == 0 ? 1 : (c == 1 ? NP : NP * NP);
+        const int base = pos - a[c] * stride;
+        double s = 0.0;
+#pragma unroll
+        for (int b = 0; b < NP; ++b) s += tc.D1[a[c] * NP + b] * W[el][base + b * stride];
+        acc += ah * s;
+    }
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+        const int axis = s >> 1, side = s & 1;
+        int m;
+        if (DIM == 2) m = a[1 - axis];
+        else m = axis == 0 ? a[1] + NP * a[2] : (axis == 1 ? a[0] + NP * a[2] : a[0] + NP * a[1]);
+        acc -= tc.lift[side * NP + a[axis]] * TR[el][s][m];
+    }
+    stage_output(io, e * NB + t, u_own, tc.tsign[t] * acc);
+}
+
+// ---------------------------------------------------------------------------
+// dense reference operators, any shape and physics
+// ---------------------------------------------------------------------------
+struct DenseGeom {
+    const double *vol;         // [DIM][NB][NB]
+    const double *pairs;       // [n_pairs][NB][NB]
+    const int32_t *nbr;        // [E][NFL]
+    const int32_t *self_pair;  // [E][NFL]
+    const int32_t *nbr_pair;   // [E][NFL]
+    const int8_t *mode;        // [E][NFL] advection
+    const double *elem_geo;    // advection [E][DIM]; wave [E][DIM][DIM]
+    const double *face_geo;    // advection [E][NFL]; wave [E][NFL][DIM]
+    double inv_cinv;           // 1 / c_inv (wave)
+    int nB;
+    int epb;                   // elements per block
+};
+
+template <int DIM, int NFL, int WAVE>
+__global__ void __launch_bounds__(256) dense_stage(const StageIO io, const DenseGeom g) {
+    constexpr int V = WAVE ? DIM + 1 : 1;
+    extern __shared__ double smem[];
+    const int nB = g.nB, R = V * nB, epb = g.epb;
+    double *W = smem;                        // [epb][R]
+    double *WN = smem + (size_t)epb * R;     // [epb][NFL][R]
+    const int tid = threadIdx.x;
+    const int64_t e0 = (int64_t)blockIdx.x * epb;
+
+    const int el = tid / R, r = tid % R;
+    const int64_t e = e0 + el;
+    const bool active = el < epb && e < io.n_elements;
+    double u_own = 0.0;
+    if (active) {
+        const int64_t idx = e * R + r;
+        u_own = io.u[idx];
+        double w = u_own;
+        for (int j = 0; j < io.nin; ++j) w += io.cin[j] * io.kin[j][idx];
+        W[el * R + r] = w;
+    }
+    for (int i = tid; i < epb * NFL * R; i += blockDim.x) {
+        const int l = i / (NFL * R), f = (i / R) % NFL, rr = i % R;
+        const int64_t ee = e0 + l;
+        double v = 0.0;
+        if (ee < io.n_elements && !(WAVE == 0 && g.mode[ee * NFL + f] == 1)) {
+            const int32_t n = g.nbr[ee * NFL + f];
+            if (n >= 0 && n < io.n_elements) v = stage_input(io, (int64_t)n * R + rr);
+            else atomicOr(io.status, 1);
+        }
+        WN[(size_t)(l * NFL + f) * R + rr] = v;
+    }
+    __syncthreads();
+    if (!active) return;
+
+    const double *w = W + el * R;
+    const double *wn = WN + (size_t)el * NFL * R;
+    double acc = 0.0;
+    if (!WAVE) {
+        const int i = r;
+        for (int c = 0; c < DIM; ++c) {
+            const double *op = g.vol + ((size_t)c * nB + i) * nB;
+            double s = 0.0;
+            for (int j = 0; j < nB; ++j) s += op[j] * w[j];
+            acc += g.elem_geo[e * DIM + c] * s;
+        }
+        for (int f = 0; f < NFL; ++f) {
+            const int8_t mode = g.mode[e * NFL + f];
+            const double sg = g.face_geo[e * NFL + f];
+            double ts = 0.0, tn = 0.0;
+            if (mode == 1 || mode == 3) {
+                const double *op = g.pairs + ((size_t)g.self_pair[e * NFL + f] * nB + i) * nB;
+                for (int j = 0; j < nB; ++j) ts += op[j] * w[j];
+            }
+            if (mode == 2 || mode == 3) {
+                const double *op = g.pairs + ((size_t)g.nbr_pair[e * NFL + f] * nB + i) * nB;
+                for (int j = 0; j < nB; ++j) tn += op[j] * wn[f * R + j];
+            }
+            acc -= mode == 1 ? sg * ts : (mode == 2 ? sg * tn : (mode == 3 ? 0.5 * sg * (ts + tn) : 0.0));
+        }
+    } else {
+        const int v = r / nB, i = r % nB;
+        const double *G = g.elem_geo + e * DIM * DIM;  // G[d][c] = (J^{-T})_{dc}
+        if (v == 0) {
+            // k_q = sum_c vol[c] (sum_d G[d][c] s_d)   (strong-form divergence)
+            for (int c = 0; c < DIM; ++c) {
+                const double *op = g.vol + ((size_t)c * nB + i) * nB;
+                double s = 0.0;
+                for (int j = 0; j < nB; ++j) {
+                    double t = 0.0;
+                    for (int d = 0; d < DIM; ++d) t += G[d * DIM + c] * w[(d + 1) * nB + j];
+                    s += op[j] * t;
+                }
+                acc += s;
+            }
+            for (int f = 0; f < NFL; ++f) {
+                const double *nu = g.face_geo + ((size_t)e * NFL + f) * DIM;
+                const double *ops = g.pairs + ((size_t)g.self_pair[e * NFL + f] * nB + i) * nB;
+                const double *opn = g.pairs + ((size_t)g.nbr_pair[e * NFL + f] * nB + i) * nB;
+                double s = 0.0;
+                for (int j = 0; j < nB; ++j) {
+                    double js = 0.0, jn = 0.0;
+                    for (int d = 0; d < DIM; ++d) {
+                        js += nu[d] * w[(d + 1) * nB + j];
+                        jn += nu[d] * wn[f * R + (d + 1) * nB + j];
+                    }
+                    s += ops[j] * js - opn[j] * jn;
+                }
+                acc -= s;
+            }
+        } else {
+            // k_{s_d} = (1/cInv) [ sum_c G[d][c] vol[c] q  - face jumps of q ]
+            const int d = v - 1;
+            for (int c = 0; c < DIM; ++c) {
+                const double *op = g.vol + ((size_t)c * nB + i) * nB;
+                double s = 0.0;
+                for (int j = 0; j < nB; ++j) s += op[j] * w[j];
+                acc += G[d * DIM + c] * s;
+            }
+            for (int f = 0; f < NFL; ++f) {
+                const double nud = g.face_geo[((size_t)e * NFL + f) * DIM + d];
+                const double *ops = g.pairs + ((size_t)g.self_pair[e * NFL + f] * nB + i) * nB;
+                const double *opn = g.pairs + ((size_t)g.nbr_pair[e * NFL + f] * nB + i) * nB;
+                double s = 0.0;
+                for (int j = 0; j < nB; ++j) s += ops[j] * w[j] - opn[j] * wn[f * R + j];
+                acc -= nud * s;
+            }
+            acc *= g.inv_cinv;
+        }
+    }
+    stage_output(io, e * R + r, u_own, acc);
+}
+
+}  // namespace hgg

@@ -1,0 +1,247 @@
+"""Python face of the library, shaped like hpGEM's HpgemAPISimplified<DIM>.
+
+The method names follow the reference (kernel/Base/HpgemAPISimplified.h:
+readMesh, setInitialSolution, computeOneTimeStep, computeTimeDerivative,
+solve, computeTotalError, getTimeIntegrationVector) so that a caller of the
+reference's stepping loop finds the same calls.  All work runs in the native
+library through the C ABI; there is no Python or CPU fallback.
+"""
+import ctypes
+import math
+
+import numpy as np
+
+from . import _native
+
+
+def _ptr(a):
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+class Handle:
+    """Owns one hgg_handle."""
+
+    def __init__(self, raw):
+        self._raw = raw
+        self._lib = _native.load()
+
+    @classmethod
+    def from_descriptor(cls, desc: _native.ProblemDesc):
+        lib = _native.load()
+        h = ctypes.c_void_p()
+        _native.check(lib.hgg_create(ctypes.byref(desc), ctypes.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def structured(cls, description, order, physics, params, tableau="RK4_4",
+                   precision=_native.PRECISION_FP64):
+        lib = _native.load()
+        h = ctypes.c_void_p()
+        p = np.ascontiguousarray(np.asarray(params, dtype=np.float64).reshape(-1))
+        _native.check(lib.hgg_create_structured(description.encode(), int(order), int(physics),
+                                                _ptr(p), tableau.encode(), int(precision),
+                                                ctypes.byref(h)))
+        return cls(h)
+
+    def close(self):
+        if self._raw is not None and self._raw.value:
+            self._lib.hgg_destroy(self._raw)
+        self._raw = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, code):
+        return _native.check(code, self._raw)
+
+    @property
+    def vector_length(self):
+        return int(self._lib.hgg_vector_length(self._raw))
+
+    @property
+    def kernel_kind(self):
+        return "tensor" if self._lib.hgg_kernel_kind(self._raw) == 1 else "dense"
+
+    @property
+    def launch_count(self):
+        return int(self._lib.hgg_launch_count(self._raw))
+
+    def set_state(self, vec, values):
+        a = np.ascontiguousarray(values, dtype=np.float64).reshape(-1)
+        if a.size != self.vector_length:
+            raise ValueError("vector has %d entries, expected %d" % (a.size, self.vector_length))
+        self._check(self._lib.hgg_set_state(self._raw, int(vec), _ptr(a)))
+
+    def set_state_ptr(self, vec, host_ptr):
+        self._check(self._lib.hgg_set_state(self._raw, int(vec), ctypes.c_void_p(host_ptr)))
+
+    def get_state(self, vec, out=None):
+        if out is None:
+            out = np.empty(self.vector_length)
+        self._check(self._lib.hgg_get_state(self._raw, int(vec), _ptr(out)))
+        return out
+
+    def get_state_ptr(self, vec, host_ptr):
+        self._check(self._lib.hgg_get_state(self._raw, int(vec), ctypes.c_void_p(host_ptr)))
+
+    def step(self, time, dt, nsteps):
+        t = ctypes.c_double(time)
+        self._check(self._lib.hgg_step(self._raw, ctypes.byref(t), float(dt), int(nsteps)))
+        return t.value
+
+    def time_derivative(self, in_vec, out_vec):
+        self._check(self._lib.hgg_time_derivative(self._raw, int(in_vec), int(out_vec)))
+
+    def synchronize(self):
+        self._check(self._lib.hgg_synchronize(self._raw))
+
+    def set_stream(self, stream_ptr):
+        self._check(self._lib.hgg_set_stream(self._raw, ctypes.c_void_p(stream_ptr or None)))
+
+    def set_store_last_stage(self, enable):
+        self._check(self._lib.hgg_set_store_last_stage(self._raw, 1 if enable else 0))
+
+    def quadrature_points(self, n_elements, dim):
+        n = self._lib.hgg_num_quadrature_points(self._raw)
+        if n < 0:
+            raise _native.NativeError(-2, "no quadrature points for this handle")
+        out = np.empty(n_elements * n * dim)
+        self._check(self._lib.hgg_quadrature_points(self._raw, _ptr(out)))
+        return out.reshape(n_elements, n, dim)
+
+    def project(self, values, vec=0):
+        a = np.ascontiguousarray(values, dtype=np.float64).reshape(-1)
+        self._check(self._lib.hgg_project(self._raw, _ptr(a), int(vec)))
+
+    def error_points(self, n_elements, dim):
+        n = self._lib.hgg_num_error_points(self._raw)
+        out = np.empty(n_elements * n * dim)
+        self._check(self._lib.hgg_error_points(self._raw, _ptr(out)))
+        return out.reshape(n_elements, n, dim)
+
+    def l2_error(self, vec, exact_values):
+        a = np.ascontiguousarray(exact_values, dtype=np.float64).reshape(-1)
+        err = ctypes.c_double()
+        self._check(self._lib.hgg_l2_error(self._raw, int(vec), _ptr(a), ctypes.byref(err)))
+        return err.value
+
+
+class HpgemAPISimplified:
+    """Explicit DG solver for one mesh, driven through the GPU library.
+
+    ``physics`` is "advection" (linear advection, weak form, upwind flux,
+    tests/self/Basic/090Advection_SelfTest.cpp) or "wave" (linear acoustic
+    wave, strong form, central flux, applications/ExampleMultipleVariableProblem/
+    AcousticWave_Impl.h).  ``tableau`` names one of hpGEM's Butcher tableaux;
+    the reference's default for HpgemAPISimplified is Dormand-Prince
+    (HpgemAPISimplified.h:150-155).
+    """
+
+    def __init__(self, dim, order, physics="advection", advection=None, c_inv=1.0,
+                 tableau="DormandPrince", precision=_native.PRECISION_FP64):
+        self.dim = int(dim)
+        self.polynomialOrder = int(order)
+        self.physics = physics
+        self.tableau = tableau
+        self.precision = precision
+        if physics == "advection":
+            self.numberOfVariables = 1
+            a = np.zeros(3)
+            if advection is not None:
+                a[:self.dim] = np.asarray(advection, dtype=float)[:self.dim]
+            self.params = a[:self.dim]
+            self._physics_code = _native.PHYSICS_ADVECTION
+        elif physics == "wave":
+            self.numberOfVariables = self.dim + 1
+            self.params = np.array([float(c_inv)])
+            self._physics_code = _native.PHYSICS_WAVE
+        else:
+            raise ValueError("physics must be 'advection' or 'wave'")
+        self.handle = None
+        self.n_elements = 0
+
+    # -- set-up -------------------------------------------------------------
+    def readMesh(self, description):
+        """Creates the device problem from a Preprocessor 'structured' description."""
+        self.handle = Handle.structured(description, self.polynomialOrder, self._physics_code,
+                                        self.params, self.tableau, self.precision)
+        self.n_basis = _basis_count(self.dim, description, self.polynomialOrder)
+        self.n_elements = self.handle.vector_length // (self.numberOfVariables * self.n_basis)
+        return self
+
+    def quadraturePoints(self):
+        return self.handle.quadrature_points(self.n_elements, self.dim)
+
+    def setInitialSolution(self, u0, vec=0):
+        """L2 projection of u0(x[n, dim]) -> [n] or [n, V] (setInitialSolution)."""
+        x = self.quadraturePoints()
+        vals = np.asarray(u0(x.reshape(-1, self.dim)), dtype=float)
+        self.handle.project(vals.reshape(-1, self.numberOfVariables), vec)
+
+    # -- time stepping ------------------------------------------------------
+    def computeOneTimeStep(self, time, dt):
+        return self.handle.step(time, dt, 1)
+
+    def computeTimeSteps(self, time, dt, nsteps):
+        return self.handle.step(time, dt, nsteps)
+
+    def computeTimeDerivative(self, in_vec, out_vec):
+        self.handle.time_derivative(in_vec, out_vec)
+
+    def solve(self, initialTime, finalTime, dt, numberOfOutputFrames=1, u0=None):
+        """Time loop of HpgemAPISimplified::solve (HpgemAPISimplified_Impl.h:976-1045):
+        the step count is ceil(T/dt) rounded up to a multiple of the number of
+        output frames, and dt is recomputed from it."""
+        T = finalTime - initialTime
+        steps = int(math.ceil(T / dt))
+        if numberOfOutputFrames > 0:
+            steps += (numberOfOutputFrames - steps % numberOfOutputFrames) % numberOfOutputFrames
+            dt = T / steps
+        if u0 is not None:
+            self.setInitialSolution(u0)
+        return self.handle.step(initialTime, dt, steps), steps, dt
+
+    # -- state and errors -----------------------------------------------------
+    def getTimeIntegrationVector(self, vec=0):
+        return self.handle.get_state(vec).reshape(self.n_elements, self.numberOfVariables * self.n_basis)
+
+    def setTimeIntegrationVector(self, vec, values):
+        self.handle.set_state(vec, values)
+
+    def computeTotalError(self, exact, time, vec=0):
+        """L2 error against exact(x[n, dim], t) -> [n] or [n, V], rule of order 2p+2."""
+        x = self.handle.error_points(self.n_elements, self.dim)
+        vals = np.asarray(exact(x.reshape(-1, self.dim), time), dtype=float)
+        return self.handle.l2_error(vec, vals.reshape(-1, self.numberOfVariables))
+
+
+def _basis_count(dim, description, p):
+    tri = "triangular" in description.split()
+    if dim == 1:
+        return p + 1
+    if dim == 2:
+        return (p + 1) * (p + 2) // 2 if tri else (p + 1) ** 2
+    return (p + 1) * (p + 2) * (p + 3) // 6 if tri else (p + 1) ** 3
+
+
+def Advection(dim, order, a, tableau="DormandPrince", **kw):
+    """The matrix-free advection application of 090Advection_SelfTest.cpp."""
+    return HpgemAPISimplified(dim, order, "advection", advection=a, tableau=tableau, **kw)
+
+
+def AcousticWave(dim, order, c_inv=1.0, tableau="RK4_4", **kw):
+    """The acoustic-wave application of ExampleMultipleVariableProblem (RK4 default, main.cpp:74-75)."""
+    return HpgemAPISimplified(dim, order, "wave", c_inv=c_inv, tableau=tableau, **kw)
+
+
+def structured_description(n, lower, upper, triangular=False, periodic=True):
+    """Text of a Preprocessor 'structured' mesh description (Preprocessor README)."""
+    d = len(n)
+    per = periodic if isinstance(periodic, (list, tuple)) else [periodic] * d
+    return "structured 1 %d\n%s\n%s\n%s\n%s\n%s\n" % (
+        d, " ".join(str(int(v)) for v in n), " ".join(repr(float(v)) for v in lower),
+        " ".join(repr(float(v)) for v in upper), "triangular" if triangular else "rectangular",
+        " ".join("true" if p else "false" for p in per))

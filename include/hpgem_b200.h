@@ -1,0 +1,213 @@
+/*
+ * hpgem_b200: B200 (sm_100a) explicit discontinuous-Galerkin time stepping,
+ * a drop-in for hpGEM's HpgemAPISimplified<DIM> time loop.
+ *
+ * The library advances the element coefficient vectors of one (or many)
+ * meshes through explicit Runge-Kutta steps on the GPU.  The physics is
+ * selected by an enum instead of hpGEM's virtual integrands:
+ *   HGG_PHYSICS_ADVECTION  linear advection, weak form, upwind flux
+ *                          (tests/self/Basic/090Advection_SelfTest.cpp:92-220)
+ *   HGG_PHYSICS_WAVE       linear acoustic wave, first-order system,
+ *                          strong form, central flux
+ *                          (applications/ExampleMultipleVariableProblem/
+ *                           AcousticWave_Impl.h:102-373)
+ *
+ * Conventions shared by every entry point:
+ *   - Return value 0 on success, a negative HGG_ERR_* code otherwise; the
+ *     message is available from hgg_last_error().  No C++ exception crosses
+ *     this boundary.
+ *   - Coefficient vectors are FP64, element-major, and inside an element
+ *     variable-major: index (e * n_vars + v) * n_basis + i, exactly hpGEM's
+ *     ElementData::convertToSingleIndex layout (kernel/Base/ElementData.h:209-225)
+ *     concatenated over elements in element-id order.
+ *   - Vector ids follow hpGEM's time-integration vectors: 0 is the solution,
+ *     1..S are the Runge-Kutta stage derivatives
+ *     (kernel/Base/HpgemAPISimplified_Impl.h:93-99).
+ *   - A handle is used by one host thread at a time; all device work of a
+ *     handle runs on its own CUDA stream.
+ */
+#ifndef HPGEM_B200_H
+#define HPGEM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum hgg_shape {
+    HGG_SHAPE_LINE = 1,
+    HGG_SHAPE_SQUARE = 2,
+    HGG_SHAPE_TRIANGLE = 3,
+    HGG_SHAPE_CUBE = 4,
+    HGG_SHAPE_TETRAHEDRON = 5
+};
+
+enum hgg_physics { HGG_PHYSICS_ADVECTION = 0, HGG_PHYSICS_WAVE = 1 };
+
+enum hgg_precision {
+    HGG_PRECISION_FP64 = 0,  /* everything in FP64 (parity form) */
+    HGG_PRECISION_FP32 = 1   /* contractions in FP32, geometry / mass inverse / RK sums in FP64 */
+};
+
+enum hgg_error {
+    HGG_OK = 0,
+    HGG_ERR_INVALID = -1,      /* bad argument or descriptor */
+    HGG_ERR_UNSUPPORTED = -2,  /* valid hpGEM input outside what this library implements */
+    HGG_ERR_CUDA = -3,         /* a CUDA call failed */
+    HGG_ERR_NOMEM = -4,        /* host or device allocation failed */
+    HGG_ERR_DEVICE = -5,       /* a kernel reported an error through its status word */
+    HGG_ERR_NOT_LOADED = -6    /* no CUDA device / kernels not loadable */
+};
+
+typedef struct hgg_handle hgg_handle;
+
+/*
+ * Everything hpGEM knows about one mesh that the time loop needs, taken
+ * from its own objects (see INTEGRATION.md for the code that fills it):
+ *   - basis values and reference gradients at the element quadrature points
+ *     (PhysicalElement::basisFunction / basisFunctionDeriv before the
+ *     J^{-T} transform; GaussQuadratureRule::eval caches),
+ *   - basis values at face quadrature points mapped into the element through
+ *     a local face and a face-to-face orientation (PhysicalFace::basisFunction
+ *     on the LEFT and RIGHT side; FaceGeometry::mapRefFaceToRefElemL/R),
+ *   - the element Jacobians (ElementGeometry::calcJacobian; the elements must
+ *     be affine, which every structured Preprocessor mesh is),
+ *   - per face, the normal of FaceGeometry::getNormalVector (outward from the
+ *     left element, length = physical / reference face measure),
+ *   - the Butcher tableau (TimeIntegration::ButcherTableau).
+ * All arrays are copied during hgg_create; the caller may free them after.
+ */
+typedef struct hgg_problem_desc {
+    int32_t dim;            /* 1, 2 or 3 */
+    int32_t shape;          /* enum hgg_shape of every element */
+    int32_t order;          /* polynomial order p of hpGEM's default DG basis */
+    int32_t n_vars;         /* 1 for advection, dim + 1 for the wave system */
+    int32_t physics;        /* enum hgg_physics */
+    int32_t precision;      /* enum hgg_precision */
+    double advection[3];    /* advection velocity a (first dim entries used) */
+    double c_inv;           /* wave material parameter cInv = 1/c^2 (AcousticWave::cInv_) */
+
+    int64_t n_elements;
+    int32_t n_basis;        /* basis functions per element and variable */
+
+    int32_t n_quad;                /* element quadrature points */
+    const double *quad_weights;    /* [n_quad] reference weights */
+    const double *basis_values;    /* [n_quad][n_basis] */
+    const double *basis_grads;     /* [n_quad][n_basis][dim] reference gradients */
+
+    int32_t n_face_quad;           /* face quadrature points */
+    const double *face_weights;    /* [n_face_quad] reference-face weights */
+    int32_t n_face_tabs;           /* number of distinct face tabulations */
+    const double *face_tabs;       /* [n_face_tabs][n_face_quad][n_basis] */
+
+    const double *jacobians;       /* [n_elements][dim][dim], J[r][c] = dx_r / dxi_c */
+
+    int64_t n_faces;
+    const int64_t *face_elements;  /* [n_faces][2]: left, right element (right >= 0) */
+    const int32_t *face_local;     /* [n_faces][2]: local face number on left, right */
+    const int32_t *face_tab_index; /* [n_faces][2]: tabulation index of the left, right side */
+    const double *face_normals;    /* [n_faces][dim] */
+
+    int32_t n_stages;              /* S */
+    const double *rk_a;            /* [S][S], row i holds a_ij for j < i */
+    const double *rk_b;            /* [S] */
+    const double *rk_c;            /* [S] */
+} hgg_problem_desc;
+
+/* ---- drop-in boundary: what hpGEM's HpgemAPISimplified<DIM> calls ------- */
+
+/* Builds the device problem.  Replaces the host set-up hpGEM does before its
+ * time loop (HpgemAPISimplified::readMesh + tasksBeforeSolving,
+ * kernel/Base/HpgemAPISimplified_Impl.h:139-160).  Device: current device. */
+int hgg_create(const hgg_problem_desc *desc, hgg_handle **out);
+
+/* Frees the handle and all its device memory. */
+int hgg_destroy(hgg_handle *h);
+
+/* Message of the last failure on this handle (or of the last failed create
+ * when h is NULL).  Never NULL. */
+const char *hgg_last_error(const hgg_handle *h);
+
+/* Host -> device copy of time-integration vector `vec` (0..S).
+ * Replaces writing Element::getTimeIntegrationVector(vec) element by element. */
+int hgg_set_state(hgg_handle *h, int32_t vec, const double *host);
+
+/* Device -> host copy of time-integration vector `vec`.  Replaces reading
+ * Element::getTimeIntegrationVector(vec) (output frames, error norms). */
+int hgg_get_state(hgg_handle *h, int32_t vec, double *host);
+
+/* `nsteps` explicit Runge-Kutta steps of size dt; *time advances by dt each.
+ * Replaces HpgemAPISimplified::computeOneTimeStep(double&, double)
+ * (kernel/Base/HpgemAPISimplified_Impl.h:788-820) called nsteps times.
+ * Stage vectors 1..S hold the last step's stage derivatives afterwards. */
+int hgg_step(hgg_handle *h, double *time, double dt, int32_t nsteps);
+
+/* out = M^{-1} R(in): replaces HpgemAPISimplified::computeTimeDerivative(in,
+ * out, t) (kernel/Base/HpgemAPISimplified_Impl.h:764-770), i.e.
+ * computeRightHandSide + solveMassMatrixEquations for one vector. */
+int hgg_time_derivative(hgg_handle *h, int32_t in_vec, int32_t out_vec);
+
+/* Blocks until all device work of the handle is done. */
+int hgg_synchronize(hgg_handle *h);
+
+/* Number of coefficients of one vector (n_elements * n_vars * n_basis). */
+int64_t hgg_vector_length(const hgg_handle *h);
+
+/* 1 when the sum-factorised tensor-product kernel drives this handle,
+ * 0 when the dense reference-operator kernel does. */
+int hgg_kernel_kind(const hgg_handle *h);
+
+/* When enabled (default), the last stage derivative k_S is stored like the
+ * other stages; disabling it saves one vector write per step when no caller
+ * reads vector S after a step. */
+int hgg_set_store_last_stage(hgg_handle *h, int32_t enable);
+
+/* Runs the handle's device work on `stream` (a cudaStream_t of the handle's
+ * device; NULL restores the handle's own stream). */
+int hgg_set_stream(hgg_handle *h, void *stream);
+
+/* Number of kernel launches the library issued on this handle so far. */
+int64_t hgg_launch_count(const hgg_handle *h);
+
+/* ---- stand-alone set-up: hpGEM's host side, restated ------------------- */
+
+/* Builds the descriptor hpGEM would build from a Preprocessor "structured"
+ * mesh description (applications/Preprocessor/lib/hpgem.cpp:55-265), its
+ * default DG basis of order p, the Gauss rules of order 2p+1 and the named
+ * Butcher tableau ("RK4_4", "DormandPrince", "ForwardEuler", "MidPoint",
+ * "RK2TVD", "RK3TVD", "BogackiShampine"), and creates the handle from it.
+ * params: advection velocity (dim values) for advection, {c_inv} for the wave. */
+int hgg_create_structured(const char *description, int32_t order, int32_t physics,
+                          const double *params, const char *tableau, int32_t precision,
+                          hgg_handle **out);
+
+/* The same descriptor, built on the host only (no device needed): fills *out
+ * with arrays owned by *owner, valid until hgg_free_descriptor(*owner). */
+int hgg_structured_descriptor(const char *description, int32_t order, int32_t physics,
+                              const double *params, const char *tableau, int32_t precision,
+                              hgg_problem_desc *out, void **owner);
+void hgg_free_descriptor(void *owner);
+
+/* Element quadrature points in physical coordinates, [n_elements][n_quad][dim]
+ * (PhysicalElement::getPointPhysical at each point of the element rule). */
+int hgg_quadrature_points(const hgg_handle *h, double *xyz);
+int32_t hgg_num_quadrature_points(const hgg_handle *h);
+
+/* setInitialSolution (HpgemAPISimplified_Impl.h:751-758): L2 projection of
+ * the initial condition, given at the element quadrature points as
+ * values[n_elements][n_quad][n_vars], into vector `vec`. */
+int hgg_project(hgg_handle *h, const double *values, int32_t vec);
+
+/* computeTotalError (HpgemAPISimplified_Impl.h:370-401): the L2 error of
+ * vector `vec` against exact values given at the error-rule points
+ * (rule of order 2p+2, :354-361) returned by hgg_error_points. */
+int32_t hgg_num_error_points(const hgg_handle *h);
+int hgg_error_points(const hgg_handle *h, double *xyz);
+int hgg_l2_error(hgg_handle *h, int32_t vec, const double *exact, double *error);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HPGEM_B200_H */
