@@ -224,7 +224,9 @@ def run_ours(args):
     ndof = h.vector_length
     solver.setInitialSolution(bump)
     u0 = solver.getTimeIntegrationVector(0).reshape(-1).copy()
-    stream = torch.cuda.current_stream()
+    # a dedicated (non-default) stream: the library launches on it, the events are recorded on it
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     h.set_stream(stream.cuda_stream)
     h.set_store_last_stage(False)
     assert h.kernel_kind == "tensor"

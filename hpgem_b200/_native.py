@@ -20,7 +20,7 @@ ERRORS = {0: "HGG_OK", -1: "HGG_ERR_INVALID", -2: "HGG_ERR_UNSUPPORTED", -3: "HG
 # every symbol include/hpgem_b200.h declares (checked by the CPU tests)
 EXPORTED = ["hgg_create", "hgg_destroy", "hgg_last_error", "hgg_set_state", "hgg_get_state",
             "hgg_step", "hgg_time_derivative", "hgg_synchronize", "hgg_vector_length",
-            "hgg_kernel_kind", "hgg_set_store_last_stage", "hgg_set_stream", "hgg_launch_count",
+            "hgg_kernel_kind", "hgg_set_store_last_stage", "hgg_set_stream", "hgg_set_kernel_variant", "hgg_launch_count",
             "hgg_create_structured", "hgg_structured_descriptor", "hgg_free_descriptor",
             "hgg_quadrature_points", "hgg_num_quadrature_points",
             "hgg_project", "hgg_num_error_points", "hgg_error_points", "hgg_l2_error"]
@@ -80,6 +80,7 @@ def load():
         "hgg_set_store_last_stage": (ctypes.c_int, [H, ctypes.c_int32]),
         "hgg_set_stream": (ctypes.c_int, [H, P]),
         "hgg_launch_count": (ctypes.c_int64, [H]),
+        "hgg_set_kernel_variant": (ctypes.c_int, [H, ctypes.c_int32]),
         "hgg_create_structured": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int32, ctypes.c_int32, P,
                                                  ctypes.c_char_p, ctypes.c_int32, ctypes.POINTER(H)]),
         "hgg_structured_descriptor": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int32, ctypes.c_int32, P,

@@ -13,6 +13,7 @@
 
 #include "../../include/hpgem_b200.h"
 #include "dg_kernels.cuh"
+#include "tensor_pipe.cuh"
 #include "host/operators.h"
 #include "host/setup.h"
 
@@ -38,6 +39,7 @@ struct hgg_handle {
     int S = 0;
     std::vector<double> rk_a, rk_b, rk_c;
     int64_t N = 0;                 // doubles per vector
+    int64_t N_alloc = 0;           // doubles allocated per vector (whole tiles)
     double *sol[2] = {nullptr, nullptr};
     int cur = 0;                   // which sol[] holds the solution
     std::vector<double *> k;       // S stage vectors
@@ -49,6 +51,10 @@ struct hgg_handle {
     double *d_ahat = nullptr, *d_tsigma = nullptr;
     int32_t *d_tnbr = nullptr;
     int8_t *d_tmode = nullptr;
+    unsigned char *d_pgeo = nullptr;  // packed per-element geometry of the pipelined kernel
+    int tile_elems = 1;               // elements per tile of the pipelined kernel
+    int variant = 0;                  // 0: pipelined tensor kernel, 1: one-shot tensor kernel
+    int num_sms = 148;
     int *d_status = nullptr;
     bool store_last = true;
     int64_t launches = 0;
@@ -108,11 +114,9 @@ void release_graphs(hgg_handle *h) {
 
 // ---- kernel dispatch ---------------------------------------------------------
 template <int P, int DIM>
-int launch_tensor(hgg_handle *h, const StageIO &io) {
+TensorConsts<P, DIM> tensor_consts(const HostOperators &op) {
     using TC = TensorConsts<P, DIM>;
-    constexpr int EPB = (256 / TC::NB) > 0 ? (256 / TC::NB) : 1;
     TC tc;
-    const HostOperators &op = h->op;
     for (int i = 0; i < TC::NP * TC::NP; ++i) tc.D1[i] = op.D1[i];
     for (int i = 0; i < 2 * TC::NP; ++i) tc.lift[i] = op.lift[i];
     tc.trace_pos[0] = op.trace_pos[0];
@@ -122,11 +126,66 @@ int launch_tensor(hgg_handle *h, const StageIO &io) {
         tc.tinv[op.tpos[i]] = (short)i;
         tc.tsign[i] = op.tsign[i];
     }
-    TensorGeom geo{h->d_ahat, h->d_tnbr, h->d_tmode, h->d_tsigma};
-    int64_t blocks = (op.nE + EPB - 1) / EPB;
-    tensor_stage<P, DIM, EPB><<<(unsigned)blocks, EPB * TC::NB, 0, h->stream>>>(io, geo, tc);
+    return tc;
+}
+
+// shared memory of the pipelined kernel for a ring of `nbuf` slots of `nv` vectors
+template <int P, int DIM>
+size_t pipe_smem(int nbuf, int nv) {
+    using S = PipeShape<P, DIM>;
+    size_t tab_end = (64 + 8 * (S::NP * S::NP + 2 * S::NP + S::NB) + 4 * S::NB + 127) / 128 * 128;
+    size_t slot = (size_t)nv * S::TILE_VEC_BYTES + S::TILE_GEO_BYTES;
+    size_t tail = 8 * ((size_t)S::TE * S::NB * 3 + (size_t)S::TE * S::NS * S::NF);
+    return tab_end + nbuf * slot + tail;
+}
+
+template <int P, int DIM>
+int launch_tensor(hgg_handle *h, const StageIO &io) {
+    using TC = TensorConsts<P, DIM>;
+    const HostOperators &op = h->op;
+    TC tc = tensor_consts<P, DIM>(op);
+    if (h->variant == 1) {
+        constexpr int EPB = (256 / TC::NB) > 0 ? (256 / TC::NB) : 1;
+        TensorGeom geo{h->d_ahat, h->d_tnbr, h->d_tmode, h->d_tsigma};
+        int64_t blocks = (op.nE + EPB - 1) / EPB;
+        tensor_stage<P, DIM, EPB><<<(unsigned)blocks, EPB * TC::NB, 0, h->stream>>>(io, geo, tc);
+        return 0;
+    }
+    using S = PipeShape<P, DIM>;
+    PipeArgs pa;
+    pa.geo = h->d_pgeo;
+    pa.n_tiles = (op.nE + S::TE - 1) / S::TE;
+    pa.nv = 1 + io.nin + (io.unew ? io.nfin : 0);
+    pa.slot_bytes = (uint32_t)((size_t)pa.nv * S::TILE_VEC_BYTES + S::TILE_GEO_BYTES);
+    // two blocks per SM when a ring of >= 3 slots fits, else one block with up to 8 slots
+    const size_t budget = 227 * 1024;
+    int per_sm = 2, nbuf = 0;
+    for (int b = 8; b >= 3; --b)
+        if (2 * (pipe_smem<P, DIM>(b, pa.nv) + 1024) <= budget) { nbuf = b; break; }
+    if (!nbuf) {
+        per_sm = 1;
+        for (int b = 8; b >= 2; --b)
+            if (pipe_smem<P, DIM>(b, pa.nv) <= budget) { nbuf = b; break; }
+    }
+    if (!nbuf) return fail(h, HGG_ERR_UNSUPPORTED, "pipelined kernel: tile does not fit in shared memory");
+    pa.nbuf = nbuf;
+    size_t smem = pipe_smem<P, DIM>(nbuf, pa.nv);
+    cudaFuncSetAttribute(tensor_pipe<P, DIM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int64_t grid = std::min<int64_t>(pa.n_tiles, (int64_t)h->num_sms * per_sm);
+    tensor_pipe<P, DIM><<<(unsigned)grid, S::THREADS, smem, h->stream>>>(io, pa, tc);
     return 0;
 }
+
+// elements per tile of the pipelined kernel for (order, dim)
+int pipe_tile_elems(int order, int dim) {
+#define HGG_TE(P) \
+    case P: return dim == 2 ? PipeShape<P, 2>::TE : PipeShape<P, 3>::TE;
+    switch (order) { HGG_TE(1) HGG_TE(2) HGG_TE(3) HGG_TE(4) HGG_TE(5) }
+#undef HGG_TE
+    return 1;
+}
+
+int pipe_geo_bytes(int dim) { return dim == 2 ? PipeShape<1, 2>::GEO_BYTES : PipeShape<1, 3>::GEO_BYTES; }
 
 template <int DIM>
 int launch_tensor_dim(hgg_handle *h, const StageIO &io) {
@@ -253,6 +312,9 @@ int create_from_desc(const hgg_problem_desc *desc, hgg_handle *h) {
         return fail(h, HGG_ERR_UNSUPPORTED, "only the FP64 precision form is available in this build");
     const HostOperators &op = h->op;
     h->N = op.nE * op.V * op.nB;
+    h->tile_elems = op.tensor ? pipe_tile_elems(op.order, op.dim) : 1;
+    const int64_t n_pad = (op.nE + h->tile_elems - 1) / h->tile_elems * h->tile_elems;
+    h->N_alloc = n_pad * op.V * op.nB;
 
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
@@ -261,19 +323,35 @@ int create_from_desc(const hgg_problem_desc *desc, hgg_handle *h) {
     HGG_CUDA(h, cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
     h->stream = h->own_stream;
     int rc;
+    HGG_CUDA(h, cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device));
     for (int i = 0; i < 2; ++i)
-        if ((rc = alloc(h, sizeof(double) * h->N, (void **)&h->sol[i]))) return rc;
+        if ((rc = alloc(h, sizeof(double) * h->N_alloc, (void **)&h->sol[i]))) return rc;
     h->k.resize(h->S);
     for (int i = 0; i < h->S; ++i)
-        if ((rc = alloc(h, sizeof(double) * h->N, (void **)&h->k[i]))) return rc;
-    for (int i = 0; i < 2; ++i) HGG_CUDA(h, cudaMemsetAsync(h->sol[i], 0, sizeof(double) * h->N, h->stream));
-    for (int i = 0; i < h->S; ++i) HGG_CUDA(h, cudaMemsetAsync(h->k[i], 0, sizeof(double) * h->N, h->stream));
+        if ((rc = alloc(h, sizeof(double) * h->N_alloc, (void **)&h->k[i]))) return rc;
+    for (int i = 0; i < 2; ++i) HGG_CUDA(h, cudaMemsetAsync(h->sol[i], 0, sizeof(double) * h->N_alloc, h->stream));
+    for (int i = 0; i < h->S; ++i) HGG_CUDA(h, cudaMemsetAsync(h->k[i], 0, sizeof(double) * h->N_alloc, h->stream));
     if ((rc = alloc(h, sizeof(int), (void **)&h->d_status))) return rc;
     HGG_CUDA(h, cudaMemsetAsync(h->d_status, 0, sizeof(int), h->stream));
     if (op.tensor) {
         if ((rc = upload(h, op.elem_geo, &h->d_ahat)) || (rc = upload(h, op.t_nbr, &h->d_tnbr)) ||
             (rc = upload(h, op.t_mode, &h->d_tmode)) || (rc = upload(h, op.t_sigma, &h->d_tsigma)))
             return rc;
+        // packed geometry records of the pipelined kernel, padded to whole tiles:
+        // ahat[dim], sigma[2 dim] (double), nbr[2 dim] (int32), mode[2 dim] (int8)
+        const int d = op.dim, ns = 2 * d, gb = pipe_geo_bytes(d);
+        std::vector<unsigned char> pg((size_t)n_pad * gb, 0);
+        for (int64_t e = 0; e < op.nE; ++e) {
+            unsigned char *r = &pg[(size_t)e * gb];
+            double *dd = reinterpret_cast<double *>(r);
+            for (int c = 0; c < d; ++c) dd[c] = op.elem_geo[e * d + c];
+            for (int s2 = 0; s2 < ns; ++s2) dd[d + s2] = op.t_sigma[e * ns + s2];
+            int32_t *ni = reinterpret_cast<int32_t *>(r + 8 * (d + ns));
+            for (int s2 = 0; s2 < ns; ++s2) ni[s2] = op.t_nbr[e * ns + s2];
+            int8_t *mi = reinterpret_cast<int8_t *>(r + 8 * (d + ns) + 4 * ns);
+            for (int s2 = 0; s2 < ns; ++s2) mi[s2] = op.t_mode[e * ns + s2];
+        }
+        if ((rc = upload(h, pg, &h->d_pgeo))) return rc;
     } else {
         if ((rc = upload(h, op.vol, &h->d_vol)) || (rc = upload(h, op.pairs, &h->d_pairs)) ||
             (rc = upload(h, op.nbr, &h->d_nbr)) || (rc = upload(h, op.self_pair, &h->d_self)) ||
@@ -414,6 +492,15 @@ int hgg_set_stream(hgg_handle *h, void *stream) {
 }
 
 int64_t hgg_launch_count(const hgg_handle *h) { return h ? h->launches : -1; }
+
+int hgg_set_kernel_variant(hgg_handle *h, int32_t variant) {
+    if (!h || variant < 0 || variant > 1) return fail(h, HGG_ERR_INVALID, "variant must be 0 or 1");
+    if (variant != h->variant) {
+        release_graphs(h);
+        h->variant = variant;
+    }
+    return 0;
+}
 
 // ---- stand-alone set-up ------------------------------------------------------
 

@@ -89,8 +89,21 @@ __global__ void __launch_bounds__(EPB *TensorConsts<P, DIM>::NB)
     constexpr int NP = TC::NP, NB = TC::NB, NF = TC::NF, NS = TC::NS;
     __shared__ double W[EPB][NB];
     __shared__ double TR[EPB][NS][NF];
+    // the small tables live in shared memory: indexing kernel parameters with a
+    // thread-dependent index would serialise the warp on the constant cache
+    __shared__ double sD1[NP * NP], slift[2 * NP], ssign[NB];
+    __shared__ short spos[NB], sinv[NB];
 
     const int tid = threadIdx.x;
+    for (int i = tid; i < NB; i += EPB * NB) {
+        spos[i] = tc.tpos[i];
+        sinv[i] = tc.tinv[i];
+        ssign[i] = tc.tsign[i];
+    }
+    if (tid < NP * NP) sD1[tid] = tc.D1[tid];
+    if (tid < 2 * NP) slift[tid] = tc.lift[tid];
+    __syncthreads();
+
     const int el = tid / NB;
     const int t = tid % NB;  // hpGEM basis index of this thread's DoF
     const int64_t e0 = (int64_t)blockIdx.x * EPB;
@@ -103,7 +116,7 @@ __global__ void __launch_bounds__(EPB *TensorConsts<P, DIM>::NB)
         u_own = io.u[idx];
         double w = u_own;
         for (int j = 0; j < io.nin; ++j) w += io.cin[j] * io.kin[j][idx];
-        W[el][tc.tpos[t]] = tc.tsign[t] * w;
+        W[el][spos[t]] = ssign[t] * w;
     }
     __syncthreads();
 
@@ -138,8 +151,8 @@ __global__ void __launch_bounds__(EPB *TensorConsts<P, DIM>::NB)
                 if (n >= 0 && n < io.n_elements) {
                     c[axis] = tc.trace_pos[1 - side];
                     int pos = c[0] + NP * c[1] + (DIM == 3 ? NP * NP * c[2] : 0);
-                    const int hi = tc.tinv[pos];
-                    tnbr = tc.tsign[hi] * stage_input(io, (int64_t)n * NB + hi);
+                    const int hi = sinv[pos];
+                    tnbr = ssign[hi] * stage_input(io, (int64_t)n * NB + hi);
                 } else {
                     atomicOr(io.status, 1);
                 }
@@ -152,7 +165,7 @@ __global__ void __launch_bounds__(EPB *TensorConsts<P, DIM>::NB)
     __syncthreads();
 
     if (!active) return;
-    const int pos = tc.tpos[t];
+    const int pos = spos[t];
     int a[3];
     a[0] = pos % NP;
     a[1] = (pos / NP) % NP;
@@ -165,7 +178,7 @@ __global__ void __launch_bounds__(EPB *TensorConsts<P, DIM>::NB)
         const int base = pos - a[c] * stride;
         double s = 0.0;
 #pragma unroll
-        for (int b = 0; b < NP; ++b) s += tc.D1[a[c] * NP + b] * W[el][base + b * stride];
+        for (int b = 0; b < NP; ++b) s += sD1[a[c] * NP + b] * W[el][base + b * stride];
         acc += ah * s;
     }
 #pragma unroll
@@ -174,9 +187,9 @@ __global__ void __launch_bounds__(EPB *TensorConsts<P, DIM>::NB)
         int m;
         if (DIM == 2) m = a[1 - axis];
         else m = axis == 0 ? a[1] + NP * a[2] : (axis == 1 ? a[0] + NP * a[2] : a[0] + NP * a[1]);
-        acc -= tc.lift[side * NP + a[axis]] * TR[el][s][m];
+        acc -= slift[side * NP + a[axis]] * TR[el][s][m];
     }
-    stage_output(io, e * NB + t, u_own, tc.tsign[t] * acc);
+    stage_output(io, e * NB + t, u_own, ssign[t] * acc);
 }
 
 // ---------------------------------------------------------------------------

@@ -74,7 +74,7 @@ void psi1d(int np, double x, double *v, double *dv) {
 // of `op` and returns true when every check passes.
 bool try_tensor(const hgg_problem_desc &desc, HostOperators &op) {
     const int d = op.dim, nB = op.nB, p = op.order, np = p + 1;
-    if (!is_hypercube(op.shape)) { op.tensor_reason = "not a hypercube"; return false; }
+    if (!is_hypercube(op.shape) || op.dim < 2) { op.tensor_reason = "not a square or cube"; return false; }
     if (op.physics != HGG_PHYSICS_ADVECTION) { op.tensor_reason = "wave uses the dense form"; return false; }
     // The tensor form is derived from hpGEM's default H1 set; it is only taken
     // when the dense operators built from the caller's own tabulations agree

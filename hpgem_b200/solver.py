@@ -101,6 +101,9 @@ class Handle:
     def set_stream(self, stream_ptr):
         self._check(self._lib.hgg_set_stream(self._raw, ctypes.c_void_p(stream_ptr or None)))
 
+    def set_kernel_variant(self, variant):
+        self._check(self._lib.hgg_set_kernel_variant(self._raw, int(variant)))
+
     def set_store_last_stage(self, enable):
         self._check(self._lib.hgg_set_store_last_stage(self._raw, 1 if enable else 0))
 

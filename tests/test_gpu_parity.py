@@ -3,10 +3,18 @@
 Every case runs the same seeded initial coefficients through
 ``computeOneTimeStep`` on both sides and compares the solution (and, where
 stated, the stage derivatives) in the max norm relative to the largest
-coefficient.  Tolerance: 1e-12 relative for the FP64 path (the accuracy
-target of the FP64 form; both sides round differently only in summation order
-and in the mass solve, which hpGEM does by LU per element and the GPU path
-by the precomputed reference inverse).
+coefficient.
+
+Tolerances:
+* solution coefficients after N steps: 1e-12 relative (the FP64 target),
+  widened only where the mass-solve rounding below, carried into the solution
+  through dt once per stage and step, exceeds it (hexahedra at p = 5);
+* stage derivatives k_i = M^{-1} R: max(1e-12, cond(Mhat) * eps).  hpGEM
+  solves the element mass system by LU in every stage; its rounding error is
+  bounded by the condition number of the reference mass matrix times the unit
+  round-off (cond = 1.9e5 for hexahedra at p = 3, 1.6e7 at p = 5), while the
+  GPU path applies the inverse through exactly factorised reference operators.
+  In the solution the same error is damped by dt.
 """
 import math
 
@@ -22,6 +30,16 @@ from hpgem_b200 import _native
 pytestmark = pytest.mark.gpu
 
 RTOL = 1e-12
+EPS = np.finfo(float).eps
+
+
+def stage_rtol(prob):
+    M = np.einsum("q,qi,qj->ij", prob.rule.weights, prob.phi, prob.phi)
+    return max(RTOL, np.linalg.cond(M) * EPS)
+
+
+def solution_rtol(prob, dt, nsteps, stages=4):
+    return max(RTOL, stage_rtol(prob) * dt * nsteps * stages)
 
 
 def desc(n, triangular=False, periodic=True):
@@ -33,7 +51,7 @@ def sine_field(x):
     return np.prod(np.sin(2 * np.pi * x), axis=1)
 
 
-def run_pair(description, p, physics, params, tableau, dt, nsteps, seed=0, stages=False):
+def run_pair(description, p, physics, params, tableau, dt, nsteps, seed=0, stages=False, variant=0):
     mesh = mesh_from_description(description)
     dim = mesh.dim
     if physics == "advection":
@@ -49,6 +67,7 @@ def run_pair(description, p, physics, params, tableau, dt, nsteps, seed=0, stage
             axis=1))
         solver = hpgem_b200.AcousticWave(dim, p, c_inv=params[0], tableau=tableau)
     solver.readMesh(description)
+    solver.handle.set_kernel_variant(variant)
     solver.setTimeIntegrationVector(0, u0)
     t = solver.computeTimeSteps(0.0, dt, nsteps)
     assert math.isclose(t, nsteps * dt, rel_tol=1e-12)
@@ -56,6 +75,7 @@ def run_pair(description, p, physics, params, tableau, dt, nsteps, seed=0, stage
     if stages:
         ref, ref_k = prob.step(u0, dt, nsteps, tableau, return_stages=True)
         got_k = [solver.getTimeIntegrationVector(i + 1) for i in range(len(ref_k))]
+        solver.stage_rtol = stage_rtol(prob)
         return got, ref, solver, got_k, ref_k
     ref = prob.step(u0, dt, nsteps, tableau)
     return got, ref, solver
@@ -72,20 +92,23 @@ def test_config1_quads_p2_rk4_100_steps():
     assert rel_err(got, ref) < RTOL
 
 
+@pytest.mark.parametrize("variant", [0, 1])
 @pytest.mark.parametrize("p", [1, 2, 3, 4, 5])
-def test_hex_tensor_kernel(p):
+def test_hex_tensor_kernel(p, variant):
     n = 4 if p <= 3 else 3
     got, ref, solver, gk, rk = run_pair(desc([n, n, n]), p, "advection", [1.0, 0.7, 0.3], "RK4_4",
-                                        2e-3, 3, stages=True)
+                                        2e-3, 3, stages=True, variant=variant)
     assert solver.handle.kernel_kind == "tensor"
-    assert rel_err(got, ref) < RTOL
+    assert rel_err(got, ref) < max(RTOL, solver.stage_rtol * 2e-3 * 3 * 4)
     for a, b in zip(gk, rk):
-        assert rel_err(a, b) < RTOL
+        assert rel_err(a, b) < solver.stage_rtol
 
 
+@pytest.mark.parametrize("variant", [0, 1])
 @pytest.mark.parametrize("p", [1, 2, 3, 4, 5])
-def test_quad_tensor_kernel_negative_velocity(p):
-    got, ref, solver = run_pair(desc([6, 5]), p, "advection", [-0.8, 0.45], "RK4_4", 2e-3, 4)
+def test_quad_tensor_kernel_negative_velocity(p, variant):
+    got, ref, solver = run_pair(desc([6, 5]), p, "advection", [-0.8, 0.45], "RK4_4", 2e-3, 4,
+                                variant=variant)
     assert solver.handle.kernel_kind == "tensor"
     assert rel_err(got, ref) < RTOL
 
@@ -106,7 +129,7 @@ def test_tets_wave_dense_kernel(p):
     assert solver.handle.kernel_kind == "dense"
     assert rel_err(got, ref) < RTOL
     for a, b in zip(gk, rk):
-        assert rel_err(a, b) < RTOL
+        assert rel_err(a, b) < solver.stage_rtol
 
 
 def test_tets_wave_config3_shape_small():
@@ -139,6 +162,22 @@ def test_every_tableau(tableau):
     assert rel_err(got, ref) < RTOL
 
 
+def test_pipelined_and_one_shot_kernels_agree_on_a_large_ragged_mesh():
+    """Many tiles per block, a last tile that is only partly filled, every Dormand-Prince
+    stage (more than one stage vector in the input): the two organisations of the
+    sum-factorised kernel give the same numbers."""
+    description = desc([13, 11, 9])
+    res = []
+    for variant in (0, 1):
+        s = hpgem_b200.Advection(3, 3, [-0.4, 0.9, 0.25], tableau="DormandPrince").readMesh(description)
+        s.handle.set_kernel_variant(variant)
+        s.setInitialSolution(sine_field)
+        s.computeTimeSteps(0.0, 1e-3, 5)
+        res.append([s.getTimeIntegrationVector(i) for i in range(8)])
+    for a, b in zip(res[0], res[1]):
+        assert rel_err(a, b) < 1e-13
+
+
 def test_axis_aligned_velocity_takes_average_flux():
     # a . n = 0 on the y-faces: hpGEM averages both traces there (|A| < 1e-12)
     got, ref, _ = run_pair(desc([5, 5]), 2, "advection", [1.0, 0.0], "RK4_4", 1e-3, 5)
@@ -154,7 +193,7 @@ def test_time_derivative_matches_oracle():
     solver = hpgem_b200.Advection(3, 3, [1.0, 0.7, 0.3], tableau="RK4_4").readMesh(description)
     solver.setTimeIntegrationVector(0, u)
     solver.computeTimeDerivative(0, 1)
-    assert rel_err(solver.getTimeIntegrationVector(1), prob.time_derivative(u)) < 1e-11
+    assert rel_err(solver.getTimeIntegrationVector(1), prob.time_derivative(u)) < stage_rtol(prob)
 
 
 def test_state_round_trip_and_store_last_stage():
