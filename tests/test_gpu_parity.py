@@ -175,7 +175,7 @@ def test_pipelined_and_one_shot_kernels_agree_on_a_large_ragged_mesh():
         s.computeTimeSteps(0.0, 1e-3, 5)
         res.append([s.getTimeIntegrationVector(i) for i in range(8)])
     for a, b in zip(res[0], res[1]):
-        assert rel_err(a, b) < 1e-13
+        assert rel_err(a, b) < RTOL
 
 
 def test_axis_aligned_velocity_takes_average_flux():
