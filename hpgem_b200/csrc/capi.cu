@@ -14,6 +14,7 @@
 #include "../../include/hpgem_b200.h"
 #include "dg_kernels.cuh"
 #include "tensor_pipe.cuh"
+#include "tensor_plane.cuh"
 #include "host/operators.h"
 #include "host/setup.h"
 
@@ -52,8 +53,18 @@ struct hgg_handle {
     int32_t *d_tnbr = nullptr;
     int8_t *d_tmode = nullptr;
     unsigned char *d_pgeo = nullptr;  // packed per-element geometry of the pipelined kernel
-    int tile_elems = 1;               // elements per tile of the pipelined kernel
-    int variant = 0;                  // 0: pipelined tensor kernel, 1: one-shot tensor kernel
+    int tile_elems = 1;               // elements per tile (common multiple of the tensor kernels' tiles)
+    int variant = 0;                  // 0: automatic, 1: one-shot, 2: pipelined pencil kernel
+    bool tensor_layout = false;       // device vectors in tensor order (signs folded)
+    double *d_scratch = nullptr;      // one vector, for layout conversion of set/get_state
+    int32_t *d_tpos = nullptr;        // hpGEM index -> tensor position
+    double *d_tsign = nullptr;
+    // half-plane kernel (hexahedra, p = 3)
+    bool plane_ok = false;
+    unsigned char *d_plane_geo = nullptr;
+    int64_t *d_plan = nullptr;
+    int32_t *d_plan_off = nullptr;
+    int plane_halo_slots = 0;
     int num_sms = 148;
     int *d_status = nullptr;
     bool store_last = true;
@@ -113,6 +124,8 @@ void release_graphs(hgg_handle *h) {
 }
 
 // ---- kernel dispatch ---------------------------------------------------------
+// The device vectors of a sum-factorised handle are already in tensor order
+// with the signs folded in, so the kernels see the identity permutation.
 template <int P, int DIM>
 TensorConsts<P, DIM> tensor_consts(const HostOperators &op) {
     using TC = TensorConsts<P, DIM>;
@@ -122,11 +135,62 @@ TensorConsts<P, DIM> tensor_consts(const HostOperators &op) {
     tc.trace_pos[0] = op.trace_pos[0];
     tc.trace_pos[1] = op.trace_pos[1];
     for (int i = 0; i < TC::NB; ++i) {
-        tc.tpos[i] = (short)op.tpos[i];
-        tc.tinv[op.tpos[i]] = (short)i;
-        tc.tsign[i] = op.tsign[i];
+        tc.tpos[i] = (short)i;
+        tc.tinv[i] = (short)i;
+        tc.tsign[i] = 1.0;
     }
     return tc;
+}
+
+// layout conversion kernels (hpGEM order <-> tensor order, signs folded)
+__global__ void to_tensor_order(const double *src, double *dst, const int32_t *tpos, const double *tsign,
+                                int nb, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t e = i / nb;
+        const int k = (int)(i - e * nb);
+        dst[e * nb + tpos[k]] = tsign[k] * src[i];
+    }
+}
+__global__ void from_tensor_order(const double *src, double *dst, const int32_t *tpos, const double *tsign,
+                                  int nb, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t e = i / nb;
+        const int k = (int)(i - e * nb);
+        dst[i] = tsign[k] * src[e * nb + tpos[k]];
+    }
+}
+
+int launch_plane(hgg_handle *h, const StageIO &io) {
+    using S = PlaneShape;
+    const HostOperators &op = h->op;
+    PlaneArgs pa;
+    pa.geo = h->d_plane_geo;
+    pa.plan = h->d_plan;
+    pa.plan_off = h->d_plan_off;
+    pa.n_tiles = (op.nE + S::TE - 1) / S::TE;
+    pa.nv = 1 + io.nin + (io.unew ? io.nfin : 0);
+    pa.nhv = 1 + io.nin;
+    pa.halo_slots = h->plane_halo_slots;
+    pa.halo_bytes = (uint32_t)((size_t)pa.halo_slots * (pa.nhv * 16 + 2) * 8);
+    pa.slot_bytes = (uint32_t)((size_t)pa.nv * S::TILE_VEC_BYTES + S::TILE_GEO_BYTES + pa.halo_bytes);
+    pa.trace_pos[0] = op.trace_pos[0];
+    pa.trace_pos[1] = op.trace_pos[1];
+    const size_t fixed = 128 + 2 * (size_t)S::TE * S::ES * 8;
+    const size_t budget = 227 * 1024;
+    int nbuf = 0;
+    for (int b = 6; b >= 2; --b)
+        if (fixed + (size_t)b * pa.slot_bytes <= budget) { nbuf = b; break; }
+    if (!nbuf) return fail(h, HGG_ERR_UNSUPPORTED, "half-plane kernel: tile does not fit in shared memory");
+    pa.nbuf = nbuf;
+    PlaneOps pops;
+    for (int i = 0; i < 16; ++i) pops.D[i] = op.D1[i];
+    for (int sd = 0; sd < 2; ++sd)
+        for (int a = 0; a < 4; ++a) pops.L[sd][a] = op.lift[sd * 4 + a];
+    const size_t smem = fixed + (size_t)nbuf * pa.slot_bytes;
+    cudaFuncSetAttribute(tensor_plane, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const int64_t grid = std::min<int64_t>(pa.n_tiles, (int64_t)h->num_sms);
+    tensor_plane<<<(unsigned)grid, S::THREADS, smem, h->stream>>>(io, pa, pops);
+    return 0;
 }
 
 // shared memory of the pipelined kernel for a ring of `nbuf` slots of `nv` vectors
@@ -144,7 +208,7 @@ int launch_tensor(hgg_handle *h, const StageIO &io) {
     using TC = TensorConsts<P, DIM>;
     const HostOperators &op = h->op;
     TC tc = tensor_consts<P, DIM>(op);
-    if (h->variant == 1) {
+    if (h->variant == 1) {  // one-shot kernel
         constexpr int EPB = (256 / TC::NB) > 0 ? (256 / TC::NB) : 1;
         TensorGeom geo{h->d_ahat, h->d_tnbr, h->d_tmode, h->d_tsigma};
         int64_t blocks = (op.nE + EPB - 1) / EPB;
@@ -222,7 +286,9 @@ int launch_dense(hgg_handle *h, const StageIO &io) {
 int launch_stage(hgg_handle *h, const StageIO &io) {
     const HostOperators &op = h->op;
     int rc;
-    if (op.tensor) {
+    if (op.tensor && h->plane_ok && h->variant == 0 && io.nin <= 1) {
+        rc = launch_plane(h, io);
+    } else if (op.tensor) {
         rc = op.dim == 2 ? launch_tensor_dim<2>(h, io)
                          : (op.dim == 3 ? launch_tensor_dim<3>(h, io)
                                         : fail(h, HGG_ERR_UNSUPPORTED, "tensor kernel needs dim 2 or 3"));
@@ -313,6 +379,9 @@ int create_from_desc(const hgg_problem_desc *desc, hgg_handle *h) {
     const HostOperators &op = h->op;
     h->N = op.nE * op.V * op.nB;
     h->tile_elems = op.tensor ? pipe_tile_elems(op.order, op.dim) : 1;
+    h->tensor_layout = op.tensor;
+    h->plane_ok = op.tensor && op.dim == 3 && op.order == 3 && op.trace_pos[0] == 0 && op.trace_pos[1] == 1;
+    if (h->plane_ok) h->tile_elems = 32;  // PipeShape<3,3>::TE = 16 divides PlaneShape::TE = 32
     const int64_t n_pad = (op.nE + h->tile_elems - 1) / h->tile_elems * h->tile_elems;
     h->N_alloc = n_pad * op.V * op.nB;
 
@@ -352,6 +421,56 @@ int create_from_desc(const hgg_problem_desc *desc, hgg_handle *h) {
             for (int s2 = 0; s2 < ns; ++s2) mi[s2] = op.t_mode[e * ns + s2];
         }
         if ((rc = upload(h, pg, &h->d_pgeo))) return rc;
+        // layout conversion tables and scratch vector
+        std::vector<int32_t> tp(op.tpos.begin(), op.tpos.end());
+        if ((rc = upload(h, tp, &h->d_tpos)) || (rc = upload(h, op.tsign, &h->d_tsign))) return rc;
+        if ((rc = alloc(h, sizeof(double) * h->N_alloc, (void **)&h->d_scratch))) return rc;
+        if (h->plane_ok) {
+            // records of the half-plane kernel and the halo gather plan, tiles of 32 elements
+            using PS = PlaneShape;
+            const int64_t n_tiles = n_pad / PS::TE;
+            std::vector<unsigned char> rec((size_t)n_pad * PS::GEO_BYTES, 0);
+            std::vector<int64_t> plan;
+            std::vector<int32_t> off(1, 0);
+            int max_slots = 1;
+            for (int64_t t = 0; t < n_tiles; ++t) {
+                int slots = 0;
+                for (int el = 0; el < PS::TE; ++el) {
+                    const int64_t e = t * PS::TE + el;
+                    if (e >= op.nE) break;
+                    unsigned char *r = &rec[(size_t)e * PS::GEO_BYTES];
+                    double *dd = reinterpret_cast<double *>(r);
+                    int8_t *mode = reinterpret_cast<int8_t *>(r + 72);
+                    int8_t *nloc = reinterpret_cast<int8_t *>(r + 78);
+                    int16_t *hslot = reinterpret_cast<int16_t *>(r + 84);
+                    for (int c = 0; c < 3; ++c) dd[c] = op.elem_geo[e * 3 + c];
+                    for (int s2 = 0; s2 < 6; ++s2) {
+                        dd[3 + s2] = op.t_sigma[e * 6 + s2];
+                        mode[s2] = op.t_mode[e * 6 + s2];
+                        nloc[s2] = -1;
+                        hslot[s2] = -1;
+                        if (mode[s2] < 2) continue;
+                        const int64_t n = op.t_nbr[e * 6 + s2];
+                        if (n >= t * PS::TE && n < (t + 1) * PS::TE) {
+                            nloc[s2] = (int8_t)(n - t * PS::TE);
+                        } else {
+                            if (slots >= 32767) return fail(h, HGG_ERR_UNSUPPORTED, "halo plan overflow");
+                            hslot[s2] = (int16_t)slots;
+                            const int slice = (s2 / 2) * 2 + (1 - s2 % 2);  // the neighbour's opposite face
+                            plan.push_back((int64_t)(uint32_t)n | ((int64_t)slice << 32) | ((int64_t)slots << 40));
+                            ++slots;
+                        }
+                    }
+                }
+                max_slots = std::max(max_slots, slots);
+                off.push_back((int32_t)plan.size());
+            }
+            if (plan.empty()) plan.push_back(0);
+            h->plane_halo_slots = max_slots;
+            if ((rc = upload(h, rec, &h->d_plane_geo)) || (rc = upload(h, plan, &h->d_plan)) ||
+                (rc = upload(h, off, &h->d_plan_off)))
+                return rc;
+        }
     } else {
         if ((rc = upload(h, op.vol, &h->d_vol)) || (rc = upload(h, op.pairs, &h->d_pairs)) ||
             (rc = upload(h, op.nbr, &h->d_nbr)) || (rc = upload(h, op.self_pair, &h->d_self)) ||
@@ -403,7 +522,15 @@ int hgg_set_state(hgg_handle *h, int32_t vec, const double *host) {
     if (!h || !host) return fail(h, HGG_ERR_INVALID, "null argument");
     double *d = vector_ptr(h, vec);
     if (!d) return fail(h, HGG_ERR_INVALID, "vector id out of range");
-    HGG_CUDA(h, cudaMemcpyAsync(d, host, sizeof(double) * h->N, cudaMemcpyHostToDevice, h->stream));
+    if (h->tensor_layout) {
+        HGG_CUDA(h, cudaMemcpyAsync(h->d_scratch, host, sizeof(double) * h->N, cudaMemcpyHostToDevice, h->stream));
+        to_tensor_order<<<4 * h->num_sms, 256, 0, h->stream>>>(h->d_scratch, d, h->d_tpos, h->d_tsign,
+                                                               h->op.nB, h->N);
+        h->launches++;
+        HGG_CUDA(h, cudaGetLastError());
+    } else {
+        HGG_CUDA(h, cudaMemcpyAsync(d, host, sizeof(double) * h->N, cudaMemcpyHostToDevice, h->stream));
+    }
     HGG_CUDA(h, cudaStreamSynchronize(h->stream));
     return 0;
 }
@@ -412,6 +539,13 @@ int hgg_get_state(hgg_handle *h, int32_t vec, double *host) {
     if (!h || !host) return fail(h, HGG_ERR_INVALID, "null argument");
     double *d = vector_ptr(h, vec);
     if (!d) return fail(h, HGG_ERR_INVALID, "vector id out of range");
+    if (h->tensor_layout) {
+        from_tensor_order<<<4 * h->num_sms, 256, 0, h->stream>>>(d, h->d_scratch, h->d_tpos, h->d_tsign,
+                                                                 h->op.nB, h->N);
+        h->launches++;
+        HGG_CUDA(h, cudaGetLastError());
+        d = h->d_scratch;
+    }
     HGG_CUDA(h, cudaMemcpyAsync(host, d, sizeof(double) * h->N, cudaMemcpyDeviceToHost, h->stream));
     HGG_CUDA(h, cudaStreamSynchronize(h->stream));
     return 0;
@@ -494,7 +628,7 @@ int hgg_set_stream(hgg_handle *h, void *stream) {
 int64_t hgg_launch_count(const hgg_handle *h) { return h ? h->launches : -1; }
 
 int hgg_set_kernel_variant(hgg_handle *h, int32_t variant) {
-    if (!h || variant < 0 || variant > 1) return fail(h, HGG_ERR_INVALID, "variant must be 0 or 1");
+    if (!h || variant < 0 || variant > 2) return fail(h, HGG_ERR_INVALID, "variant must be 0, 1 or 2");
     if (variant != h->variant) {
         release_graphs(h);
         h->variant = variant;

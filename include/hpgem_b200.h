@@ -167,10 +167,12 @@ int hgg_set_store_last_stage(hgg_handle *h, int32_t enable);
  * device; NULL restores the handle's own stream). */
 int hgg_set_stream(hgg_handle *h, void *stream);
 
-/* Selects the kernel organisation of the sum-factorised path: 0 (default) the
- * persistent kernel fed by bulk asynchronous copies, 1 one block per small
- * group of elements.  Both compute the same result; the choice exists for
- * comparison and profiling.  Ignored by the dense path. */
+/* Selects the kernel organisation of the sum-factorised path: 0 (default)
+ * automatic (the half-plane kernel for hexahedra of order 3 whenever a stage
+ * input combines at most one stage vector, else the pipelined pencil kernel),
+ * 1 one block per small group of elements, 2 the pipelined pencil kernel.
+ * All compute the same result; the choice exists for comparison and
+ * profiling.  Ignored by the dense path. */
 int hgg_set_kernel_variant(hgg_handle *h, int32_t variant);
 
 /* Number of kernel launches the library issued on this handle so far. */
