@@ -168,7 +168,20 @@ int launch_plane(hgg_handle *h, const StageIO &io) {
     pa.plan = h->d_plan;
     pa.plan_off = h->d_plan_off;
     pa.n_tiles = (op.nE + S::TE - 1) / S::TE;
-    pa.nv = 1 + io.nin + (io.unew ? io.nfin : 0);
+    // vectors to bring per tile: u, the stage inputs, then final-update vectors not already among them
+    pa.nv = 0;
+    pa.lv[pa.nv++] = io.u;
+    for (int j = 0; j < io.nin; ++j) pa.lv[pa.nv++] = io.kin[j];
+    for (int j = 0; j < (io.unew ? io.nfin : 0); ++j) {
+        int at = -1;
+        for (int v = 0; v < pa.nv; ++v)
+            if (pa.lv[v] == io.kfin[j]) at = v;
+        if (at < 0) {
+            at = pa.nv;
+            pa.lv[pa.nv++] = io.kfin[j];
+        }
+        pa.fin_idx[j] = at;
+    }
     pa.nhv = 1 + io.nin;
     pa.halo_slots = h->plane_halo_slots;
     pa.halo_bytes = (uint32_t)((size_t)pa.halo_slots * (pa.nhv * 16 + 2) * 8);

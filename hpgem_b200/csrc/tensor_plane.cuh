@@ -69,7 +69,9 @@ struct PlaneArgs {
     const int32_t *plan_off;   // [n_tiles + 1]
     int64_t n_tiles;
     int nbuf;
-    int nv;                    // vectors bulk-loaded per tile: u, kin[..], kfin[..]
+    int nv;                    // vectors bulk-loaded per tile: u, kin[..], then kfin[..] not already loaded
+    const double *lv[1 + 2 * kMaxStages];  // the loaded vectors
+    int fin_idx[kMaxStages];   // position in lv of each kfin vector
     int nhv;                   // vectors gathered per halo slice: u, kin[..] (1 + nin)
     int halo_slots;            // slices per tile
     uint32_t slot_bytes;       // nv * 16 KB + geo
@@ -219,7 +221,6 @@ __global__ void __launch_bounds__(PlaneShape::THREADS, 1)
     const int tid = threadIdx.x;
     const int warp = tid >> 5;
     const int el = tid & 31;
-    const int C = warp & 3, H = warp >> 2;
     const int nin = io.nin, nfin = io.nfin;
     const int64_t my_tiles = (pa.n_tiles - blockIdx.x + gridDim.x - 1) / gridDim.x;
     if (my_tiles <= 0) return;
@@ -230,9 +231,7 @@ __global__ void __launch_bounds__(PlaneShape::THREADS, 1)
     }
     __syncthreads();
 
-    auto vec_ptr = [&](int v) -> const double * {
-        return v == 0 ? io.u : (v <= nin ? io.kin[v - 1] : io.kfin[v - 1 - nin]);
-    };
+    auto vec_ptr = [&](int v) -> const double * { return pa.lv[v]; };
     auto slot_of = [&](int64_t j) { return ring + (size_t)(j % pa.nbuf) * pa.slot_bytes; };
     auto issue = [&](int64_t j) {  // thread 0: bulk loads of local tile j
         const int64_t tile = blockIdx.x + j * gridDim.x;
@@ -335,7 +334,7 @@ __global__ void __launch_bounds__(PlaneShape::THREADS, 1)
             for (int i = tid; i < TE * NB; i += S::THREADS) {
                 double r = ru[i];
                 for (int v = 0; v < nfin; ++v)
-                    r += io.bfin[v] * reinterpret_cast<const double *>(slot + (size_t)(1 + nin + v) * TV)[i];
+                    r += io.bfin[v] * reinterpret_cast<const double *>(slot + (size_t)pa.fin_idx[v] * TV)[i];
                 r += io.blast * KS[(i >> 6) * ES + (i & 63)];
                 io.unew[e0 * NB + i] = r;
             }
