@@ -15,6 +15,8 @@
 #include "dg_kernels.cuh"
 #include "tensor_pipe.cuh"
 #include "tensor_plane.cuh"
+#include "tensor_reg.cuh"
+#include "tensor_pencil.cuh"
 #include "host/operators.h"
 #include "host/setup.h"
 
@@ -160,6 +162,23 @@ __global__ void from_tensor_order(const double *src, double *dst, const int32_t 
     }
 }
 
+int launch_reg(hgg_handle *h, const StageIO &io) {
+    const HostOperators &op = h->op;
+    RegOps rops;
+    for (int i = 0; i < 16; ++i) rops.D[i] = op.D1[i];
+    for (int sd = 0; sd < 2; ++sd)
+        for (int a = 0; a < 4; ++a) rops.L[sd][a] = op.lift[sd * 4 + a];
+    RegGeom geo{h->d_ahat, h->d_tnbr, h->d_tmode, h->d_tsigma};
+    if (h->variant == 4) {
+        const int64_t blocks = (op.nE + 127) / 128;
+        tensor_reg<<<(unsigned)blocks, 128, 0, h->stream>>>(io, geo, rops);
+    } else {
+        const int64_t blocks = (op.nE + PencilShape::TE - 1) / PencilShape::TE;
+        tensor_pencil<<<(unsigned)blocks, PencilShape::THREADS, 0, h->stream>>>(io, geo, rops);
+    }
+    return 0;
+}
+
 int launch_plane(hgg_handle *h, const StageIO &io) {
     using S = PlaneShape;
     const HostOperators &op = h->op;
@@ -188,7 +207,7 @@ int launch_plane(hgg_handle *h, const StageIO &io) {
     pa.slot_bytes = (uint32_t)((size_t)pa.nv * S::TILE_VEC_BYTES + S::TILE_GEO_BYTES + pa.halo_bytes);
     pa.trace_pos[0] = op.trace_pos[0];
     pa.trace_pos[1] = op.trace_pos[1];
-    const size_t fixed = 128 + 2 * (size_t)S::TE * S::ES * 8;
+    const size_t fixed = 256 + 2 * (size_t)S::TE * S::ES * 8;
     const size_t budget = 227 * 1024;
     int nbuf = 0;
     for (int b = 6; b >= 2; --b)
@@ -299,7 +318,9 @@ int launch_dense(hgg_handle *h, const StageIO &io) {
 int launch_stage(hgg_handle *h, const StageIO &io) {
     const HostOperators &op = h->op;
     int rc;
-    if (op.tensor && h->plane_ok && h->variant == 0 && io.nin <= 1) {
+    if (op.tensor && h->plane_ok && (h->variant == 0 || h->variant == 4)) {
+        rc = launch_reg(h, io);
+    } else if (op.tensor && h->plane_ok && h->variant == 3 && io.nin <= 1) {
         rc = launch_plane(h, io);
     } else if (op.tensor) {
         rc = op.dim == 2 ? launch_tensor_dim<2>(h, io)
@@ -641,7 +662,7 @@ int hgg_set_stream(hgg_handle *h, void *stream) {
 int64_t hgg_launch_count(const hgg_handle *h) { return h ? h->launches : -1; }
 
 int hgg_set_kernel_variant(hgg_handle *h, int32_t variant) {
-    if (!h || variant < 0 || variant > 2) return fail(h, HGG_ERR_INVALID, "variant must be 0, 1 or 2");
+    if (!h || variant < 0 || variant > 4) return fail(h, HGG_ERR_INVALID, "variant must be 0..4");
     if (variant != h->variant) {
         release_graphs(h);
         h->variant = variant;

@@ -18,9 +18,9 @@
 //     stride 65 doubles, so a warp reading one entry of 32 elements touches 32
 //     different banks);
 //   * each thread owns half of one z-plane of one element (8 outputs); the
-//     plane index and the half are uniform per warp, so the code is
-//     specialised on them and every 1D operator entry is a compile-time index
-//     into the kernel parameters (a constant-bank operand);
+//     plane index and the half are uniform per warp, so the operator rows
+//     they select are shared-memory broadcasts and every other operator entry
+//     is a compile-time index into the kernel parameters;
 //   * stage derivatives leave from registers in 32-byte runs; the final RK
 //     update runs over the tile in coefficient order from the staged k.
 // Every mbarrier wait is bounded (status bit 1 on expiry).
@@ -101,11 +101,15 @@ __device__ __forceinline__ double plane_flux(int md, double sg, double self, dou
 
 // Eight outputs (a = 0..3, b = 2H, 2H+1) of plane C of element `el`; written to
 // k (global, two 32-byte runs) and/or to the staged tile KS for the final update.
-template <int C, int H>
-__device__ __forceinline__ void plane_compute(const PlaneOps &op, const PlaneArgs &pa, const double *W,
-                                              const unsigned char *geo, const double *halo, int halo_stride,
-                                              int el, int nin, double cin0, double *kout, double *ks) {
+// C and H are uniform across the warp: the operator rows they select are read
+// from shared memory as broadcasts, while every other operator entry has a
+// compile-time index into the kernel parameters.
+__device__ __forceinline__ void plane_compute(const PlaneOps &op, const double *sD, const double *sL,
+                                              const double *W, const unsigned char *geo, const double *halo,
+                                              int halo_stride, int el, int C, int H, int nin, double cin0,
+                                              double *kout, double *ks) {
     const double *w = W + el * PlaneShape::ES;
+    const double *wc = w + 16 * C;
     const double *g = reinterpret_cast<const double *>(geo);
     const int8_t *mode = reinterpret_cast<const int8_t *>(geo + 72);
     const int8_t *nloc = reinterpret_cast<const int8_t *>(geo + 78);
@@ -115,27 +119,38 @@ __device__ __forceinline__ void plane_compute(const PlaneOps &op, const PlaneArg
     // psi_1 = (1+x)/2 the only one at +1 (checked on the host before this kernel is chosen)
     constexpr int tp0 = 0, tp1 = 1;
 
+    double Db[2][4], Dc[4];  // derivative rows of b = 2H + bb and of c = C
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        Db[0][k] = sD[(2 * H) * 4 + k];
+        Db[1][k] = sD[(2 * H + 1) * 4 + k];
+        Dc[k] = sD[C * 4 + k];
+    }
+
     double acc[2][4];
     {
         double P[4][4];  // P[b][a] of plane C
 #pragma unroll
         for (int b = 0; b < 4; ++b)
 #pragma unroll
-            for (int a = 0; a < 4; ++a) P[b][a] = w[16 * C + a + 4 * b];
+            for (int a = 0; a < 4; ++a) P[b][a] = wc[a + 4 * b];
+        double R[2][4];  // the two rows b = 2H, 2H+1 owned by this thread
 #pragma unroll
-        for (int bb = 0; bb < 2; ++bb) {
-            const int b = 2 * H + bb;
+        for (int bb = 0; bb < 2; ++bb)
+#pragma unroll
+            for (int a = 0; a < 4; ++a) R[bb][a] = H ? P[2 + bb][a] : P[bb][a];
+#pragma unroll
+        for (int bb = 0; bb < 2; ++bb)
 #pragma unroll
             for (int a = 0; a < 4; ++a) {
                 double sx = 0.0, sy = 0.0;
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
-                    sx += op.D[a * 4 + k] * P[b][k];
-                    sy += op.D[b * 4 + k] * P[k][a];
+                    sx += op.D[a * 4 + k] * R[bb][k];
+                    sy += Db[bb][k] * P[k][a];
                 }
                 acc[bb][a] = ax * sx + ay * sy;
             }
-        }
         // x faces (entry b + 4C at (b, C)) and y faces (entry a + 4C at (a, C))
 #pragma unroll
         for (int side = 0; side < 2; ++side) {
@@ -148,22 +163,25 @@ __device__ __forceinline__ void plane_compute(const PlaneOps &op, const PlaneArg
                 const double nb = mx >= 2 ? plane_nbr(W, halo, halo_stride, nloc[side], hslot[side], b + 4 * C,
                                                       tpo + 4 * b + 16 * C, nin, cin0)
                                           : 0.0;
-                const double f = plane_flux(mx, sgx, P[b][tps], nb);
+                const double f = plane_flux(mx, sgx, R[bb][tps], nb);
 #pragma unroll
                 for (int a = 0; a < 4; ++a) acc[bb][a] -= op.L[side][a] * f;
             }
+            const double lb0 = sL[side * 4 + 2 * H], lb1 = sL[side * 4 + 2 * H + 1];
 #pragma unroll
             for (int a = 0; a < 4; ++a) {
                 const double nb = my >= 2 ? plane_nbr(W, halo, halo_stride, nloc[2 + side], hslot[2 + side],
                                                       a + 4 * C, a + 4 * tpo + 16 * C, nin, cin0)
                                           : 0.0;
                 const double f = plane_flux(my, sgy, P[tps][a], nb);
-#pragma unroll
-                for (int bb = 0; bb < 2; ++bb) acc[bb][a] -= op.L[side][2 * H + bb] * f;
+                acc[0][a] -= lb0 * f;
+                acc[1][a] -= lb1 * f;
             }
         }
     }
     // z derivative over the planes, then z faces (entry a + 4b at (a, b))
+    const double lc0 = sL[C], lc1 = sL[4 + C];
+    const int mz0 = mode[4], mz1 = mode[5];
 #pragma unroll
     for (int bb = 0; bb < 2; ++bb) {
         const int b = 2 * H + bb;
@@ -173,20 +191,19 @@ __device__ __forceinline__ void plane_compute(const PlaneOps &op, const PlaneArg
 #pragma unroll
             for (int c2 = 0; c2 < 4; ++c2) {
                 const double v = w[16 * c2 + a + 4 * b];
-                sz += op.D[C * 4 + c2] * v;
+                sz += Dc[c2] * v;
                 if (c2 == tp0) z0 = v;
                 if (c2 == tp1) z1 = v;
             }
             double r = acc[bb][a] + az * sz;
-#pragma unroll
-            for (int side = 0; side < 2; ++side) {
-                const int tpo = side ? tp0 : tp1;
-                const int mz = mode[4 + side];
-                const double nb = mz >= 2 ? plane_nbr(W, halo, halo_stride, nloc[4 + side], hslot[4 + side],
-                                                      a + 4 * b, a + 4 * b + 16 * tpo, nin, cin0)
-                                          : 0.0;
-                r -= op.L[side][C] * plane_flux(mz, g[7 + side], side ? z1 : z0, nb);
-            }
+            const double n0 = mz0 >= 2 ? plane_nbr(W, halo, halo_stride, nloc[4], hslot[4], a + 4 * b,
+                                                   a + 4 * b + 16 * tp1, nin, cin0)
+                                       : 0.0;
+            const double n1 = mz1 >= 2 ? plane_nbr(W, halo, halo_stride, nloc[5], hslot[5], a + 4 * b,
+                                                   a + 4 * b + 16 * tp0, nin, cin0)
+                                       : 0.0;
+            r -= lc0 * plane_flux(mz0, g[7], z0, n0);
+            r -= lc1 * plane_flux(mz1, g[8], z1, n1);
             acc[bb][a] = r;
         }
     }
@@ -211,10 +228,11 @@ __global__ void __launch_bounds__(PlaneShape::THREADS, 1)
     constexpr int TE = S::TE, NB = S::NB, ES = S::ES, TV = S::TILE_VEC_BYTES;
     extern __shared__ __align__(128) unsigned char plane_smem_raw[];
     unsigned char *smem = plane_smem_raw;
-    uint64_t *mbar = reinterpret_cast<uint64_t *>(smem);             // [nbuf <= 8]
-    unsigned char *ring = smem + 128;
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(smem);             // [nbuf <= 8], bytes 0..63
+    unsigned char *ring = smem + 256;  // bytes 64..255: operator tables
     double *W = reinterpret_cast<double *>(ring + (size_t)pa.nbuf * pa.slot_bytes);  // [TE][ES]
     double *KS = W + TE * ES;                                                         // [TE][ES]
+    double *sD = reinterpret_cast<double *>(smem + 64);  // 16 + 8 doubles: D, lifts (fits before the ring)
     // per slot: vectors [nv][TE*NB], geometry [TE][136], halo [halo_slots][stride]
     const int halo_stride = pa.nhv * 16 + 2;
 
@@ -229,7 +247,10 @@ __global__ void __launch_bounds__(PlaneShape::THREADS, 1)
         for (int s = 0; s < pa.nbuf; ++s) ptx::mbar_init(&mbar[s], 1);
         ptx::fence_mbar_init();
     }
+    if (tid < 16) sD[tid] = op.D[tid];
+    if (tid >= 16 && tid < 24) sD[tid] = op.L[(tid - 16) / 4][(tid - 16) % 4];
     __syncthreads();
+    const double *sL = sD + 16;
 
     auto vec_ptr = [&](int v) -> const double * { return pa.lv[v]; };
     auto slot_of = [&](int64_t j) { return ring + (size_t)(j % pa.nbuf) * pa.slot_bytes; };
@@ -317,15 +338,7 @@ __global__ void __launch_bounds__(PlaneShape::THREADS, 1)
             const double cin0 = nin >= 1 ? io.cin[0] : 0.0;
             double *kdst = io.kout ? io.kout + (e0 + el) * NB : nullptr;
             double *ks = io.unew ? KS + el * ES : nullptr;
-            switch (warp) {
-#define HGG_PLANE(Cc, Hh)                                                                           \
-    case Cc + 4 * Hh:                                                                               \
-        plane_compute<Cc, Hh>(op, pa, W, g, halo, halo_stride, el, nin, cin0, kdst, ks);            \
-        break;
-                HGG_PLANE(0, 0) HGG_PLANE(1, 0) HGG_PLANE(2, 0) HGG_PLANE(3, 0)
-                HGG_PLANE(0, 1) HGG_PLANE(1, 1) HGG_PLANE(2, 1) HGG_PLANE(3, 1)
-#undef HGG_PLANE
-            }
+            plane_compute(op, sD, sL, W, g, halo, halo_stride, el, warp & 3, warp >> 2, nin, cin0, kdst, ks);
         }
         if (__syncthreads_or(!ok)) break;
 

@@ -168,11 +168,13 @@ int hgg_set_store_last_stage(hgg_handle *h, int32_t enable);
 int hgg_set_stream(hgg_handle *h, void *stream);
 
 /* Selects the kernel organisation of the sum-factorised path: 0 (default)
- * automatic (the half-plane kernel for hexahedra of order 3 whenever a stage
- * input combines at most one stage vector, else the pipelined pencil kernel),
- * 1 one block per small group of elements, 2 the pipelined pencil kernel.
- * All compute the same result; the choice exists for comparison and
- * profiling.  Ignored by the dense path. */
+ * automatic (for hexahedra of order 3 the warp-per-pencil kernel, otherwise
+ * the pipelined pencil kernel), 1 one block per small group of elements,
+ * 2 the pipelined pencil kernel, 3 the half-plane kernel (hexahedra of order
+ * 3, stages whose input combines at most one stage vector), 4 one element
+ * per thread in registers (hexahedra of order 3).  All compute the same
+ * result; the choice exists for comparison and profiling.  Ignored by the
+ * dense path. */
 int hgg_set_kernel_variant(hgg_handle *h, int32_t variant);
 
 /* Number of kernel launches the library issued on this handle so far. */

@@ -92,7 +92,7 @@ def test_config1_quads_p2_rk4_100_steps():
     assert rel_err(got, ref) < RTOL
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4])
 @pytest.mark.parametrize("p", [1, 2, 3, 4, 5])
 def test_hex_tensor_kernel(p, variant):
     n = 4 if p <= 3 else 3
@@ -168,7 +168,7 @@ def test_pipelined_and_one_shot_kernels_agree_on_a_large_ragged_mesh():
     sum-factorised kernel give the same numbers."""
     description = desc([13, 11, 9])
     res = []
-    for variant in (0, 1, 2):
+    for variant in (0, 1, 2, 3, 4):
         s = hpgem_b200.Advection(3, 3, [-0.4, 0.9, 0.25], tableau="DormandPrince").readMesh(description)
         s.handle.set_kernel_variant(variant)
         s.setInitialSolution(sine_field)
@@ -179,7 +179,7 @@ def test_pipelined_and_one_shot_kernels_agree_on_a_large_ragged_mesh():
             assert rel_err(a, b) < RTOL
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4])
 def test_hex_p3_kernels_on_a_ragged_mesh_rk4(variant):
     """Hexahedra p = 3 with RK4 (the half-plane kernel in variant 0): element count not
     a multiple of the tile, negative and positive velocity components, against the oracle."""
