@@ -4,6 +4,7 @@ nvcc compiles the CUDA stage kernels and the C ABI (csrc/capi.cu) for sm_100a
 only, together with the C++ host set-up (csrc/host/*.cpp).  Run
 ``python -m hpgem_b200.build``.
 """
+import glob
 import os
 import shutil
 import subprocess
@@ -16,7 +17,7 @@ LIB = os.path.join(LIB_DIR, "libhpgem_b200.so")
 SOURCES = [os.path.join(CSRC, "capi.cu"),
            os.path.join(CSRC, "host", "setup.cpp"),
            os.path.join(CSRC, "host", "operators.cpp")]
-DEPS = SOURCES + [os.path.join(CSRC, "dg_kernels.cuh"),
+DEPS = SOURCES + sorted(glob.glob(os.path.join(CSRC, "*.cuh"))) + [
                   os.path.join(CSRC, "host", "refshapes.h"),
                   os.path.join(CSRC, "host", "setup.h"),
                   os.path.join(CSRC, "host", "operators.h"),

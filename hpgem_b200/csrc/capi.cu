@@ -54,6 +54,7 @@ struct hgg_handle {
     double *d_ahat = nullptr, *d_tsigma = nullptr;
     int32_t *d_tnbr = nullptr;
     int8_t *d_tmode = nullptr;
+    double *d_pencil_geo = nullptr;   // per-element records of the pencil kernel (PencilShape::GR doubles)
     unsigned char *d_pgeo = nullptr;  // packed per-element geometry of the pipelined kernel
     int tile_elems = 1;               // elements per tile (common multiple of the tensor kernels' tiles)
     int variant = 0;                  // 0: automatic, 1: one-shot, 2: pipelined pencil kernel
@@ -174,7 +175,7 @@ int launch_reg(hgg_handle *h, const StageIO &io) {
         tensor_reg<<<(unsigned)blocks, 128, 0, h->stream>>>(io, geo, rops);
     } else {
         const int64_t blocks = (op.nE + PencilShape::TE - 1) / PencilShape::TE;
-        tensor_pencil<<<(unsigned)blocks, PencilShape::THREADS, 0, h->stream>>>(io, geo, rops);
+        tensor_pencil<<<(unsigned)blocks, PencilShape::THREADS, 0, h->stream>>>(io, h->d_pencil_geo, rops);
     }
     return 0;
 }
@@ -455,6 +456,24 @@ int create_from_desc(const hgg_problem_desc *desc, hgg_handle *h) {
             for (int s2 = 0; s2 < ns; ++s2) mi[s2] = op.t_mode[e * ns + s2];
         }
         if ((rc = upload(h, pg, &h->d_pgeo))) return rc;
+        if (h->plane_ok) {
+            // pencil kernel records, padded to whole tiles: ahat[3], sigma[6] (double),
+            // nbr[6] (int32), mode[6] (int8), 2 bytes of padding
+            constexpr int GR = PencilShape::GR;
+            std::vector<double> rec((size_t)n_pad * GR, 0.0);
+            for (int64_t e = 0; e < op.nE; ++e) {
+                double *r = &rec[(size_t)e * GR];
+                for (int c = 0; c < 3; ++c) r[c] = op.elem_geo[e * 3 + c];
+                for (int s2 = 0; s2 < 6; ++s2) r[3 + s2] = op.t_sigma[e * 6 + s2];
+                int32_t *ni = reinterpret_cast<int32_t *>(r + 9);
+                int8_t *mi = reinterpret_cast<int8_t *>(r + 12);
+                for (int s2 = 0; s2 < 6; ++s2) {
+                    ni[s2] = op.t_nbr[e * 6 + s2];
+                    mi[s2] = op.t_mode[e * 6 + s2];
+                }
+            }
+            if ((rc = upload(h, rec, &h->d_pencil_geo))) return rc;
+        }
         // layout conversion tables and scratch vector
         std::vector<int32_t> tp(op.tpos.begin(), op.tpos.end());
         if ((rc = upload(h, tp, &h->d_tpos)) || (rc = upload(h, op.tsign, &h->d_tsign))) return rc;

@@ -181,11 +181,34 @@ def test_pipelined_and_one_shot_kernels_agree_on_a_large_ragged_mesh():
 
 @pytest.mark.parametrize("variant", [0, 1, 2, 3, 4])
 def test_hex_p3_kernels_on_a_ragged_mesh_rk4(variant):
-    """Hexahedra p = 3 with RK4 (the half-plane kernel in variant 0): element count not
-    a multiple of the tile, negative and positive velocity components, against the oracle."""
+    """Hexahedra p = 3 with RK4: element count not a multiple of the tile, negative and
+    positive velocity components, against the oracle."""
     got, ref, solver = run_pair(desc([7, 5, 3]), 3, "advection", [-0.6, 0.8, -0.3], "RK4_4", 2e-3, 4,
                                 variant=variant)
     assert rel_err(got, ref) < RTOL
+
+
+@pytest.fixture(scope="module")
+def many_tiles_reference():
+    description = desc([23, 17, 13])
+    prob = Problem(mesh_from_description(description), 3, ADVECTION, a=[0.9, -0.5, 0.35])
+    u0 = prob.project(lambda x: sine_field(x)[:, None])
+    ref, ref_k = prob.step(u0, 1e-3, 2, "RK4_4", return_stages=True)
+    return description, u0, ref, ref_k, stage_rtol(prob)
+
+
+@pytest.mark.parametrize("variant", [0, 1])
+def test_hex_p3_many_tiles(variant, many_tiles_reference):
+    """More tiles than SMs, x-neighbours inside and outside each tile, periodic wrap in
+    every direction, a last tile that is only partly filled."""
+    description, u0, ref, ref_k, srtol = many_tiles_reference
+    solver = hpgem_b200.Advection(3, 3, [0.9, -0.5, 0.35], tableau="RK4_4").readMesh(description)
+    solver.handle.set_kernel_variant(variant)
+    solver.setTimeIntegrationVector(0, u0)
+    solver.computeTimeSteps(0.0, 1e-3, 2)
+    assert rel_err(solver.getTimeIntegrationVector(0), ref) < RTOL
+    for i, b in enumerate(ref_k):
+        assert rel_err(solver.getTimeIntegrationVector(i + 1), b) < srtol
 
 
 def test_axis_aligned_velocity_takes_average_flux():
