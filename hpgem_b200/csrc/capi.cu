@@ -14,9 +14,7 @@
 #include "../../include/hpgem_b200.h"
 #include "dg_kernels.cuh"
 #include "tensor_pipe.cuh"
-#include "tensor_plane.cuh"
-#include "tensor_reg.cuh"
-#include "tensor_pencil.cuh"
+#include "tensor_slice.cuh"
 #include "host/operators.h"
 #include "host/setup.h"
 
@@ -54,20 +52,17 @@ struct hgg_handle {
     double *d_ahat = nullptr, *d_tsigma = nullptr;
     int32_t *d_tnbr = nullptr;
     int8_t *d_tmode = nullptr;
-    double *d_pencil_geo = nullptr;   // per-element records of the pencil kernel (PencilShape::GR doubles)
     unsigned char *d_pgeo = nullptr;  // packed per-element geometry of the pipelined kernel
     int tile_elems = 1;               // elements per tile (common multiple of the tensor kernels' tiles)
-    int variant = 0;                  // 0: automatic, 1: one-shot, 2: pipelined pencil kernel
+    int variant = 0;                  // 0: automatic, 1: one-shot, 2: pipelined kernel
     bool tensor_layout = false;       // device vectors in tensor order (signs folded)
+    bool tiled = false;               // ... and in tiles of 32 elements, coefficient-major (slice kernel)
     double *d_scratch = nullptr;      // one vector, for layout conversion of set/get_state
     int32_t *d_tpos = nullptr;        // hpGEM index -> tensor position
     double *d_tsign = nullptr;
-    // half-plane kernel (hexahedra, p = 3)
-    bool plane_ok = false;
-    unsigned char *d_plane_geo = nullptr;
-    int64_t *d_plan = nullptr;
-    int32_t *d_plan_off = nullptr;
-    int plane_halo_slots = 0;
+    // slice kernel (hexahedra, p = 3): per-element records of SliceShape::GR doubles
+    bool slice_ok = false;
+    double *d_slice_geo = nullptr;
     int num_sms = 148;
     int *d_status = nullptr;
     bool store_last = true;
@@ -145,84 +140,45 @@ TensorConsts<P, DIM> tensor_consts(const HostOperators &op) {
     return tc;
 }
 
-// layout conversion kernels (hpGEM order <-> tensor order, signs folded)
+// layout conversion kernels (hpGEM order <-> tensor order, signs folded; tiled:
+// 32-element tiles, coefficient-major inside a tile)
+__device__ __forceinline__ int64_t device_index(int64_t e, int pos, int nb, bool tiled) {
+    return tiled ? (e >> 5) * ((int64_t)nb << 5) + (int64_t)pos * 32 + (e & 31) : e * nb + pos;
+}
 __global__ void to_tensor_order(const double *src, double *dst, const int32_t *tpos, const double *tsign,
-                                int nb, int64_t n) {
+                                int nb, int64_t n, bool tiled) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const int64_t e = i / nb;
         const int k = (int)(i - e * nb);
-        dst[e * nb + tpos[k]] = tsign[k] * src[i];
+        dst[device_index(e, tpos[k], nb, tiled)] = tsign[k] * src[i];
     }
 }
 __global__ void from_tensor_order(const double *src, double *dst, const int32_t *tpos, const double *tsign,
-                                  int nb, int64_t n) {
+                                  int nb, int64_t n, bool tiled) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const int64_t e = i / nb;
         const int k = (int)(i - e * nb);
-        dst[i] = tsign[k] * src[e * nb + tpos[k]];
+        dst[i] = tsign[k] * src[device_index(e, tpos[k], nb, tiled)];
     }
 }
 
-int launch_reg(hgg_handle *h, const StageIO &io) {
+int launch_slice(hgg_handle *h, const StageIO &io) {
     const HostOperators &op = h->op;
-    RegOps rops;
-    for (int i = 0; i < 16; ++i) rops.D[i] = op.D1[i];
+    SliceOps sops;
+    for (int i = 0; i < 16; ++i) sops.D[i] = op.D1[i];
     for (int sd = 0; sd < 2; ++sd)
-        for (int a = 0; a < 4; ++a) rops.L[sd][a] = op.lift[sd * 4 + a];
-    RegGeom geo{h->d_ahat, h->d_tnbr, h->d_tmode, h->d_tsigma};
-    if (h->variant == 4) {
-        const int64_t blocks = (op.nE + 127) / 128;
-        tensor_reg<<<(unsigned)blocks, 128, 0, h->stream>>>(io, geo, rops);
-    } else {
-        const int64_t blocks = (op.nE + PencilShape::TE - 1) / PencilShape::TE;
-        tensor_pencil<<<(unsigned)blocks, PencilShape::THREADS, 0, h->stream>>>(io, h->d_pencil_geo, rops);
-    }
-    return 0;
-}
-
-int launch_plane(hgg_handle *h, const StageIO &io) {
-    using S = PlaneShape;
-    const HostOperators &op = h->op;
-    PlaneArgs pa;
-    pa.geo = h->d_plane_geo;
-    pa.plan = h->d_plan;
-    pa.plan_off = h->d_plan_off;
-    pa.n_tiles = (op.nE + S::TE - 1) / S::TE;
-    // vectors to bring per tile: u, the stage inputs, then final-update vectors not already among them
-    pa.nv = 0;
-    pa.lv[pa.nv++] = io.u;
-    for (int j = 0; j < io.nin; ++j) pa.lv[pa.nv++] = io.kin[j];
-    for (int j = 0; j < (io.unew ? io.nfin : 0); ++j) {
-        int at = -1;
-        for (int v = 0; v < pa.nv; ++v)
-            if (pa.lv[v] == io.kfin[j]) at = v;
-        if (at < 0) {
-            at = pa.nv;
-            pa.lv[pa.nv++] = io.kfin[j];
-        }
-        pa.fin_idx[j] = at;
-    }
-    pa.nhv = 1 + io.nin;
-    pa.halo_slots = h->plane_halo_slots;
-    pa.halo_bytes = (uint32_t)((size_t)pa.halo_slots * (pa.nhv * 16 + 2) * 8);
-    pa.slot_bytes = (uint32_t)((size_t)pa.nv * S::TILE_VEC_BYTES + S::TILE_GEO_BYTES + pa.halo_bytes);
-    pa.trace_pos[0] = op.trace_pos[0];
-    pa.trace_pos[1] = op.trace_pos[1];
-    const size_t fixed = 256 + 2 * (size_t)S::TE * S::ES * 8;
-    const size_t budget = 227 * 1024;
-    int nbuf = 0;
-    for (int b = 6; b >= 2; --b)
-        if (fixed + (size_t)b * pa.slot_bytes <= budget) { nbuf = b; break; }
-    if (!nbuf) return fail(h, HGG_ERR_UNSUPPORTED, "half-plane kernel: tile does not fit in shared memory");
-    pa.nbuf = nbuf;
-    PlaneOps pops;
-    for (int i = 0; i < 16; ++i) pops.D[i] = op.D1[i];
-    for (int sd = 0; sd < 2; ++sd)
-        for (int a = 0; a < 4; ++a) pops.L[sd][a] = op.lift[sd * 4 + a];
-    const size_t smem = fixed + (size_t)nbuf * pa.slot_bytes;
-    cudaFuncSetAttribute(tensor_plane, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    const int64_t grid = std::min<int64_t>(pa.n_tiles, (int64_t)h->num_sms);
-    tensor_plane<<<(unsigned)grid, S::THREADS, smem, h->stream>>>(io, pa, pops);
+        for (int a = 0; a < 4; ++a) sops.L[sd][a] = op.lift[sd * 4 + a];
+    const int64_t blocks = (op.nE + SliceShape::TE - 1) / SliceShape::TE;
+    const dim3 grid((unsigned)blocks), block(SliceShape::THREADS);
+    const bool fin = io.unew != nullptr;
+    if (io.nin == 0 && (!fin || io.nfin == 0))
+        tensor_slice<0, 0><<<grid, block, 0, h->stream>>>(io, h->d_slice_geo, sops);
+    else if (io.nin == 1 && (!fin || io.nfin == 0))
+        tensor_slice<1, 0><<<grid, block, 0, h->stream>>>(io, h->d_slice_geo, sops);
+    else if (io.nin == 1 && fin && io.nfin == 3)
+        tensor_slice<1, 3><<<grid, block, 0, h->stream>>>(io, h->d_slice_geo, sops);
+    else
+        tensor_slice<-1, -1><<<grid, block, 0, h->stream>>>(io, h->d_slice_geo, sops);
     return 0;
 }
 
@@ -241,17 +197,8 @@ int launch_tensor(hgg_handle *h, const StageIO &io) {
     using TC = TensorConsts<P, DIM>;
     const HostOperators &op = h->op;
     TC tc = tensor_consts<P, DIM>(op);
-    if (h->variant == 1) {  // one-shot kernel
-        constexpr int EPB = (256 / TC::NB) > 0 ? (256 / TC::NB) : 1;
-        TensorGeom geo{h->d_ahat, h->d_tnbr, h->d_tmode, h->d_tsigma};
-        int64_t blocks = (op.nE + EPB - 1) / EPB;
-        tensor_stage<P, DIM, EPB><<<(unsigned)blocks, EPB * TC::NB, 0, h->stream>>>(io, geo, tc);
-        return 0;
-    }
     using S = PipeShape<P, DIM>;
     PipeArgs pa;
-    pa.geo = h->d_pgeo;
-    pa.n_tiles = (op.nE + S::TE - 1) / S::TE;
     pa.nv = 1 + io.nin + (io.unew ? io.nfin : 0);
     pa.slot_bytes = (uint32_t)((size_t)pa.nv * S::TILE_VEC_BYTES + S::TILE_GEO_BYTES);
     // two blocks per SM when a ring of >= 3 slots fits, else one block with up to 8 slots
@@ -264,7 +211,18 @@ int launch_tensor(hgg_handle *h, const StageIO &io) {
         for (int b = 8; b >= 2; --b)
             if (pipe_smem<P, DIM>(b, pa.nv) <= budget) { nbuf = b; break; }
     }
-    if (!nbuf) return fail(h, HGG_ERR_UNSUPPORTED, "pipelined kernel: tile does not fit in shared memory");
+    if (!nbuf && h->variant == 2)
+        return fail(h, HGG_ERR_UNSUPPORTED, "pipelined kernel: tile does not fit in shared memory");
+    // the one-shot kernel when asked for, or when a stage reads too many vectors for the ring
+    if (h->variant == 1 || !nbuf) {
+        constexpr int EPB = (256 / TC::NB) > 0 ? (256 / TC::NB) : 1;
+        TensorGeom geo{h->d_ahat, h->d_tnbr, h->d_tmode, h->d_tsigma};
+        int64_t blocks = (op.nE + EPB - 1) / EPB;
+        tensor_stage<P, DIM, EPB><<<(unsigned)blocks, EPB * TC::NB, 0, h->stream>>>(io, geo, tc);
+        return 0;
+    }
+    pa.geo = h->d_pgeo;
+    pa.n_tiles = (op.nE + S::TE - 1) / S::TE;
     pa.nbuf = nbuf;
     size_t smem = pipe_smem<P, DIM>(nbuf, pa.nv);
     cudaFuncSetAttribute(tensor_pipe<P, DIM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -319,10 +277,8 @@ int launch_dense(hgg_handle *h, const StageIO &io) {
 int launch_stage(hgg_handle *h, const StageIO &io) {
     const HostOperators &op = h->op;
     int rc;
-    if (op.tensor && h->plane_ok && (h->variant == 0 || h->variant == 4)) {
-        rc = launch_reg(h, io);
-    } else if (op.tensor && h->plane_ok && h->variant == 3 && io.nin <= 1) {
-        rc = launch_plane(h, io);
+    if (h->slice_ok) {
+        rc = launch_slice(h, io);
     } else if (op.tensor) {
         rc = op.dim == 2 ? launch_tensor_dim<2>(h, io)
                          : (op.dim == 3 ? launch_tensor_dim<3>(h, io)
@@ -415,8 +371,9 @@ int create_from_desc(const hgg_problem_desc *desc, hgg_handle *h) {
     h->N = op.nE * op.V * op.nB;
     h->tile_elems = op.tensor ? pipe_tile_elems(op.order, op.dim) : 1;
     h->tensor_layout = op.tensor;
-    h->plane_ok = op.tensor && op.dim == 3 && op.order == 3 && op.trace_pos[0] == 0 && op.trace_pos[1] == 1;
-    if (h->plane_ok) h->tile_elems = 32;  // PipeShape<3,3>::TE = 16 divides PlaneShape::TE = 32
+    h->slice_ok = op.tensor && op.dim == 3 && op.order == 3 && op.trace_pos[0] == 0 && op.trace_pos[1] == 1;
+    h->tiled = h->slice_ok;
+    if (h->slice_ok) h->tile_elems = SliceShape::TE;
     const int64_t n_pad = (op.nE + h->tile_elems - 1) / h->tile_elems * h->tile_elems;
     h->N_alloc = n_pad * op.V * op.nB;
 
@@ -456,10 +413,10 @@ int create_from_desc(const hgg_problem_desc *desc, hgg_handle *h) {
             for (int s2 = 0; s2 < ns; ++s2) mi[s2] = op.t_mode[e * ns + s2];
         }
         if ((rc = upload(h, pg, &h->d_pgeo))) return rc;
-        if (h->plane_ok) {
-            // pencil kernel records, padded to whole tiles: ahat[3], sigma[6] (double),
+        if (h->slice_ok) {
+            // slice kernel records, padded to whole tiles: ahat[3], sigma[6] (double),
             // nbr[6] (int32), mode[6] (int8), 2 bytes of padding
-            constexpr int GR = PencilShape::GR;
+            constexpr int GR = SliceShape::GR;
             std::vector<double> rec((size_t)n_pad * GR, 0.0);
             for (int64_t e = 0; e < op.nE; ++e) {
                 double *r = &rec[(size_t)e * GR];
@@ -472,58 +429,12 @@ int create_from_desc(const hgg_problem_desc *desc, hgg_handle *h) {
                     mi[s2] = op.t_mode[e * 6 + s2];
                 }
             }
-            if ((rc = upload(h, rec, &h->d_pencil_geo))) return rc;
+            if ((rc = upload(h, rec, &h->d_slice_geo))) return rc;
         }
         // layout conversion tables and scratch vector
         std::vector<int32_t> tp(op.tpos.begin(), op.tpos.end());
         if ((rc = upload(h, tp, &h->d_tpos)) || (rc = upload(h, op.tsign, &h->d_tsign))) return rc;
         if ((rc = alloc(h, sizeof(double) * h->N_alloc, (void **)&h->d_scratch))) return rc;
-        if (h->plane_ok) {
-            // records of the half-plane kernel and the halo gather plan, tiles of 32 elements
-            using PS = PlaneShape;
-            const int64_t n_tiles = n_pad / PS::TE;
-            std::vector<unsigned char> rec((size_t)n_pad * PS::GEO_BYTES, 0);
-            std::vector<int64_t> plan;
-            std::vector<int32_t> off(1, 0);
-            int max_slots = 1;
-            for (int64_t t = 0; t < n_tiles; ++t) {
-                int slots = 0;
-                for (int el = 0; el < PS::TE; ++el) {
-                    const int64_t e = t * PS::TE + el;
-                    if (e >= op.nE) break;
-                    unsigned char *r = &rec[(size_t)e * PS::GEO_BYTES];
-                    double *dd = reinterpret_cast<double *>(r);
-                    int8_t *mode = reinterpret_cast<int8_t *>(r + 72);
-                    int8_t *nloc = reinterpret_cast<int8_t *>(r + 78);
-                    int16_t *hslot = reinterpret_cast<int16_t *>(r + 84);
-                    for (int c = 0; c < 3; ++c) dd[c] = op.elem_geo[e * 3 + c];
-                    for (int s2 = 0; s2 < 6; ++s2) {
-                        dd[3 + s2] = op.t_sigma[e * 6 + s2];
-                        mode[s2] = op.t_mode[e * 6 + s2];
-                        nloc[s2] = -1;
-                        hslot[s2] = -1;
-                        if (mode[s2] < 2) continue;
-                        const int64_t n = op.t_nbr[e * 6 + s2];
-                        if (n >= t * PS::TE && n < (t + 1) * PS::TE) {
-                            nloc[s2] = (int8_t)(n - t * PS::TE);
-                        } else {
-                            if (slots >= 32767) return fail(h, HGG_ERR_UNSUPPORTED, "halo plan overflow");
-                            hslot[s2] = (int16_t)slots;
-                            const int slice = (s2 / 2) * 2 + (1 - s2 % 2);  // the neighbour's opposite face
-                            plan.push_back((int64_t)(uint32_t)n | ((int64_t)slice << 32) | ((int64_t)slots << 40));
-                            ++slots;
-                        }
-                    }
-                }
-                max_slots = std::max(max_slots, slots);
-                off.push_back((int32_t)plan.size());
-            }
-            if (plan.empty()) plan.push_back(0);
-            h->plane_halo_slots = max_slots;
-            if ((rc = upload(h, rec, &h->d_plane_geo)) || (rc = upload(h, plan, &h->d_plan)) ||
-                (rc = upload(h, off, &h->d_plan_off)))
-                return rc;
-        }
     } else {
         if ((rc = upload(h, op.vol, &h->d_vol)) || (rc = upload(h, op.pairs, &h->d_pairs)) ||
             (rc = upload(h, op.nbr, &h->d_nbr)) || (rc = upload(h, op.self_pair, &h->d_self)) ||
@@ -578,7 +489,7 @@ int hgg_set_state(hgg_handle *h, int32_t vec, const double *host) {
     if (h->tensor_layout) {
         HGG_CUDA(h, cudaMemcpyAsync(h->d_scratch, host, sizeof(double) * h->N, cudaMemcpyHostToDevice, h->stream));
         to_tensor_order<<<4 * h->num_sms, 256, 0, h->stream>>>(h->d_scratch, d, h->d_tpos, h->d_tsign,
-                                                               h->op.nB, h->N);
+                                                               h->op.nB, h->N, h->tiled);
         h->launches++;
         HGG_CUDA(h, cudaGetLastError());
     } else {
@@ -594,7 +505,7 @@ int hgg_get_state(hgg_handle *h, int32_t vec, double *host) {
     if (!d) return fail(h, HGG_ERR_INVALID, "vector id out of range");
     if (h->tensor_layout) {
         from_tensor_order<<<4 * h->num_sms, 256, 0, h->stream>>>(d, h->d_scratch, h->d_tpos, h->d_tsign,
-                                                                 h->op.nB, h->N);
+                                                                 h->op.nB, h->N, h->tiled);
         h->launches++;
         HGG_CUDA(h, cudaGetLastError());
         d = h->d_scratch;
@@ -681,7 +592,9 @@ int hgg_set_stream(hgg_handle *h, void *stream) {
 int64_t hgg_launch_count(const hgg_handle *h) { return h ? h->launches : -1; }
 
 int hgg_set_kernel_variant(hgg_handle *h, int32_t variant) {
-    if (!h || variant < 0 || variant > 4) return fail(h, HGG_ERR_INVALID, "variant must be 0..4");
+    if (!h || variant < 0 || variant > 2) return fail(h, HGG_ERR_INVALID, "variant must be 0..2");
+    if (variant != 0 && h->slice_ok)
+        return fail(h, HGG_ERR_UNSUPPORTED, "hexahedra of order 3 have one kernel organisation (the slice kernel)");
     if (variant != h->variant) {
         release_graphs(h);
         h->variant = variant;

@@ -1,0 +1,217 @@
+// Slice stage kernel for hexahedra of order p = 3 (tiled device layout).
+//
+// Device layout.  Vectors of a hexahedral p = 3 handle are stored in tiles of
+// 32 elements; inside a tile coefficient j of element e sits at
+//     (e / 32) * 2048 + j * 32 + e % 32,
+// with j the tensor position a + 4 b + 16 c (signs folded in).  A warp whose
+// lanes are the 32 elements of a tile therefore reads or writes any one
+// coefficient as 256 contiguous bytes, and so does a warp reading one
+// coefficient of 32 consecutive neighbours (the y and z neighbours of a tile
+// of a structured mesh are again whole tiles).
+//
+// Thread organisation.  One block of 128 threads per tile: lane = element,
+// warp c = the z-slice c of that element, so each thread owns the 16
+// coefficients (a, b, c), a, b = 0..3.  The x and y derivatives and the x and
+// y face traces of its outputs come from registers; only the z derivative and
+// the z faces need other slices, through a padded staged tile in shared
+// memory.  The L1 data path, which limits per-element-per-thread layouts on
+// this part, sees about a third of their shared and global wavefronts.
+//   phase 1  tile geometry records (coalesced copy into shared memory), the
+//            thread's 16 coefficients of u and of the stage vectors, stage
+//            input w staged in shared memory (element stride 65 doubles:
+//            lanes hit distinct banks);
+//   phase 2  face fluxes: x faces (entries (b, c)) and y faces (entries
+//            (a, c)) into registers, neighbour traces from the staged tile
+//            when the neighbour is in the tile, else from global memory; z
+//            faces (16 entries per side) are spread over the four warps and
+//            go to a padded trace tile;
+//   phase 3  the 16 outputs: x and y derivatives from registers, z derivative
+//            from the staged tile, lifts of the six face fluxes; kout and the
+//            final Runge-Kutta update are written coefficient by coefficient.
+#pragma once
+
+#include <cstdint>
+
+#include "dg_kernels.cuh"
+
+namespace hgg {
+
+struct SliceOps {
+    double D[16];    // M1^{-1} S1 (row-major, D[i][k])
+    double L[2][4];  // M1^{-1} psi(-1), M1^{-1} psi(+1)
+};
+
+struct SliceShape {
+    static constexpr int TE = 32, THREADS = 128;
+    static constexpr int TILE = TE * 64;  // doubles per tile of one vector
+    static constexpr int WS = 65;         // staged tile: element stride (doubles)
+    static constexpr int ZS = 33;         // z-face trace tile: element stride (doubles)
+    static constexpr int GR = 13;         // geometry record (doubles): ahat[3], sigma[6], nbr[6] int32, mode[6] int8
+};
+
+// index of coefficient j of element n in the tiled layout
+__device__ __forceinline__ int64_t tiled_index(int64_t n, int j) {
+    return (n >> 5) * SliceShape::TILE + j * 32 + (n & 31);
+}
+
+__device__ __forceinline__ double ldg_f64(const double *p) {
+    double v;
+    asm("ld.global.nc.f64 %0, [%1];" : "=d"(v) : "l"(p));
+    return v;
+}
+
+__device__ __forceinline__ double slice_flux(int md, double sg, double self, double nbr) {
+    return md == 1 ? sg * self : (md == 2 ? sg * nbr : (md == 3 ? 0.5 * sg * (self + nbr) : 0.0));
+}
+
+// NIN / NFIN: number of stage vectors in the stage input / in the final
+// update, fixed at compile time for the common Runge-Kutta stages (so every
+// load loop unrolls and all loads of a phase are in flight together), or -1
+// for a count read from io.
+template <int NIN, int NFIN>
+__global__ void __launch_bounds__(SliceShape::THREADS, 4)
+    tensor_slice(const StageIO io, const double *__restrict__ geo, const SliceOps op) {
+    constexpr int TE = SliceShape::TE, WS = SliceShape::WS, ZS = SliceShape::ZS, GR = SliceShape::GR;
+    constexpr int TILE = SliceShape::TILE;
+    constexpr int tp0 = 0, tp1 = 1;  // psi_0 only mode at -1, psi_1 only mode at +1
+    __shared__ double W[TE * WS];
+    __shared__ double TZ[TE * ZS];
+    __shared__ double G[TE * GR];
+
+    const int el = threadIdx.x & 31;
+    const int c = threadIdx.x >> 5;  // z-slice, uniform in the warp
+    const int64_t t0 = (int64_t)blockIdx.x * TE;
+    const int64_t e = t0 + el;
+    const bool active = e < io.n_elements;
+    // own coefficient j of this element: base + 32 j (padding lanes read their own zero slots)
+    const int64_t base = (int64_t)blockIdx.x * TILE + el;
+    const int nin = NIN >= 0 ? NIN : io.nin;
+    const int nfin = NFIN >= 0 ? NFIN : io.nfin;
+
+    // ---- phase 1: geometry records, own slice, stage input -------------------------
+    for (int i = threadIdx.x; i < TE * GR; i += SliceShape::THREADS) G[i] = ldg_f64(geo + t0 * GR + i);
+    double w[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) w[i] = ldg_f64(io.u + base + 32 * (i + 16 * c));
+#pragma unroll
+    for (int jj = 0; jj < nin; ++jj) {
+        const double cj = io.cin[jj];
+        const double *kj = io.kin[jj] + base;
+#pragma unroll
+        for (int i = 0; i < 16; ++i) w[i] += cj * ldg_f64(kj + 32 * (i + 16 * c));
+    }
+    double *wrow = W + el * WS;
+#pragma unroll
+    for (int i = 0; i < 16; ++i) wrow[i + 16 * c] = w[i];
+    __syncthreads();
+
+    // ---- phase 2: face fluxes -------------------------------------------------------
+    const double *g = G + el * GR;
+    const int32_t *gn = reinterpret_cast<const int32_t *>(g + 9);
+    const int8_t *gm = reinterpret_cast<const int8_t *>(g + 12);
+    int md[6];
+#pragma unroll
+    for (int s = 0; s < 6; ++s) {
+        md[s] = active ? (int)gm[s] : 0;
+        if (md[s] >= 2 && (gn[s] < 0 || gn[s] >= io.n_elements)) {
+            atomicOr(io.status, 1);
+            md[s] = 0;
+        }
+    }
+    const int zside = c >> 1, zs = 4 + zside, zm0 = 8 * (c & 1);
+    // neighbour traces, all requested before any is used: entries (b, c) of the x faces,
+    // (a, c) of the y faces, 8 of the 16 entries (a, b) of z face zs
+    auto nbr_pos = [&](int s, int q) {  // neighbour position of entry q of face s (this warp's part)
+        const int tpo = (s & 1) ? tp0 : tp1;
+        return s < 2 ? tpo + 4 * q + 16 * c : (s < 4 ? q + 4 * tpo + 16 * c : zm0 + q + 16 * tpo);
+    };
+    double NB[5][8];
+#pragma unroll
+    for (int f = 0; f < 5; ++f) {
+        const int s = f < 4 ? f : zs;
+        const int nq = f < 4 ? 4 : 8;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) NB[f][q] = 0.0;
+        const int32_t n = gn[s];
+        if (md[s] >= 2) {
+            if (n >= t0 && n < t0 + TE) {
+                const double *nrow = W + (int)(n - t0) * WS;
+#pragma unroll
+                for (int q = 0; q < nq; ++q) NB[f][q] = nrow[nbr_pos(s, q)];
+            } else {
+                const int64_t nbase = ((int64_t)n >> 5) * TILE + (n & 31);
+#pragma unroll
+                for (int q = 0; q < nq; ++q) NB[f][q] = ldg_f64(io.u + nbase + 32 * nbr_pos(s, q));
+#pragma unroll
+                for (int jj = 0; jj < nin; ++jj) {
+                    const double cj = io.cin[jj];
+#pragma unroll
+                    for (int q = 0; q < nq; ++q) NB[f][q] += cj * ldg_f64(io.kin[jj] + nbase + 32 * nbr_pos(s, q));
+                }
+            }
+        }
+    }
+    double FX[2][4], FY[2][4];
+#pragma unroll
+    for (int side = 0; side < 2; ++side) {
+        const int tps = side ? tp1 : tp0;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            FX[side][q] = slice_flux(md[side], g[3 + side], w[tps + 4 * q], NB[side][q]);
+            FY[side][q] = slice_flux(md[2 + side], g[5 + side], w[q + 4 * tps], NB[2 + side][q]);
+        }
+    }
+    {
+        const int tps = zside ? tp1 : tp0;
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+            TZ[el * ZS + 16 * zside + zm0 + q] = slice_flux(md[zs], g[3 + zs], wrow[zm0 + q + 16 * tps], NB[4][q]);
+    }
+    __syncthreads();
+    if (!active) return;
+
+    // ---- phase 3: the 16 outputs of the slice ---------------------------------------
+    double fu[16];
+    if (io.unew) {
+#pragma unroll
+        for (int i = 0; i < 16; ++i) fu[i] = ldg_f64(io.u + base + 32 * (i + 16 * c));
+#pragma unroll
+        for (int jj = 0; jj < nfin; ++jj) {
+            const double bj = io.bfin[jj];
+            const double *kj = io.kfin[jj] + base;
+#pragma unroll
+            for (int i = 0; i < 16; ++i) fu[i] += bj * ldg_f64(kj + 32 * (i + 16 * c));
+        }
+    }
+    const double ax = g[0], ay = g[1], az = g[2];
+    double Dc[4], Lc0, Lc1;
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+        Dc[k] = c == 0 ? op.D[k] : (c == 1 ? op.D[4 + k] : (c == 2 ? op.D[8 + k] : op.D[12 + k]));
+    Lc0 = c == 0 ? op.L[0][0] : (c == 1 ? op.L[0][1] : (c == 2 ? op.L[0][2] : op.L[0][3]));
+    Lc1 = c == 0 ? op.L[1][0] : (c == 1 ? op.L[1][1] : (c == 2 ? op.L[1][2] : op.L[1][3]));
+    const double *zrow = TZ + el * ZS;
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+#pragma unroll
+        for (int a = 0; a < 4; ++a) {
+            const int i = a + 4 * b;
+            double sx = 0.0, sy = 0.0, sz = 0.0;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                sx += op.D[a * 4 + k] * w[k + 4 * b];
+                sy += op.D[b * 4 + k] * w[a + 4 * k];
+                sz += Dc[k] * (k == c ? w[i] : wrow[i + 16 * k]);
+            }
+            double r = ax * sx + ay * sy + az * sz;
+            r -= op.L[0][a] * FX[0][b] + op.L[1][a] * FX[1][b];
+            r -= op.L[0][b] * FY[0][a] + op.L[1][b] * FY[1][a];
+            r -= Lc0 * zrow[i] + Lc1 * zrow[16 + i];
+            const int64_t off = base + 32 * (i + 16 * c);
+            if (io.kout) io.kout[off] = r;
+            if (io.unew) io.unew[off] = fu[i] + io.blast * r;
+        }
+    }
+}
+
+}  // namespace hgg

@@ -168,13 +168,11 @@ int hgg_set_store_last_stage(hgg_handle *h, int32_t enable);
 int hgg_set_stream(hgg_handle *h, void *stream);
 
 /* Selects the kernel organisation of the sum-factorised path: 0 (default)
- * automatic (for hexahedra of order 3 the warp-per-pencil kernel, otherwise
- * the pipelined pencil kernel), 1 one block per small group of elements,
- * 2 the pipelined pencil kernel, 3 the half-plane kernel (hexahedra of order
- * 3, stages whose input combines at most one stage vector), 4 one element
- * per thread in registers (hexahedra of order 3).  All compute the same
- * result; the choice exists for comparison and profiling.  Ignored by the
- * dense path. */
+ * automatic, 1 one block per small group of elements, 2 the pipelined kernel.
+ * Both compute the same result; the choice exists for comparison and
+ * profiling.  Hexahedra of order 3 keep their vectors in a tiled layout that
+ * only their slice kernel reads: any variant but 0 returns
+ * HGG_ERR_UNSUPPORTED there.  Ignored by the dense path. */
 int hgg_set_kernel_variant(hgg_handle *h, int32_t variant);
 
 /* Number of kernel launches the library issued on this handle so far. */

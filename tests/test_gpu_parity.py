@@ -9,12 +9,15 @@ Tolerances:
 * solution coefficients after N steps: 1e-12 relative (the FP64 target),
   widened only where the mass-solve rounding below, carried into the solution
   through dt once per stage and step, exceeds it (hexahedra at p = 5);
-* stage derivatives k_i = M^{-1} R: max(1e-12, cond(Mhat) * eps).  hpGEM
-  solves the element mass system by LU in every stage; its rounding error is
-  bounded by the condition number of the reference mass matrix times the unit
-  round-off (cond = 1.9e5 for hexahedra at p = 3, 1.6e7 at p = 5), while the
-  GPU path applies the inverse through exactly factorised reference operators.
-  In the solution the same error is damped by dt.
+* stage derivatives k_i = M^{-1} R: max(1e-12, 4 cond(Mhat) eps).  hpGEM
+  solves the element mass system by LU in every stage; the forward error of
+  that solve is the condition number of the reference mass matrix times a
+  small multiple of the unit round-off (cond = 1.9e5 for hexahedra at p = 3,
+  1.6e7 at p = 5), while the GPU path applies the inverse through exactly
+  factorised reference operators.  The factor 4 covers the maximum over the
+  1e5 coefficients of the larger meshes (1.4 cond eps observed for the
+  Dormand-Prince stages on 1287 hexahedra at p = 3).  In the solution the
+  same error is damped by dt.
 """
 import math
 
@@ -33,13 +36,17 @@ RTOL = 1e-12
 EPS = np.finfo(float).eps
 
 
-def stage_rtol(prob):
+def mass_cond_eps(prob):
     M = np.einsum("q,qi,qj->ij", prob.rule.weights, prob.phi, prob.phi)
-    return max(RTOL, np.linalg.cond(M) * EPS)
+    return np.linalg.cond(M) * EPS
+
+
+def stage_rtol(prob):
+    return max(RTOL, 4.0 * mass_cond_eps(prob))
 
 
 def solution_rtol(prob, dt, nsteps, stages=4):
-    return max(RTOL, stage_rtol(prob) * dt * nsteps * stages)
+    return max(RTOL, mass_cond_eps(prob) * dt * nsteps * stages)
 
 
 def desc(n, triangular=False, periodic=True):
@@ -76,6 +83,7 @@ def run_pair(description, p, physics, params, tableau, dt, nsteps, seed=0, stage
         ref, ref_k = prob.step(u0, dt, nsteps, tableau, return_stages=True)
         got_k = [solver.getTimeIntegrationVector(i + 1) for i in range(len(ref_k))]
         solver.stage_rtol = stage_rtol(prob)
+        solver.solution_rtol = solution_rtol(prob, dt, nsteps, len(ref_k))
         return got, ref, solver, got_k, ref_k
     ref = prob.step(u0, dt, nsteps, tableau)
     return got, ref, solver
@@ -92,14 +100,16 @@ def test_config1_quads_p2_rk4_100_steps():
     assert rel_err(got, ref) < RTOL
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4])
+@pytest.mark.parametrize("variant", [0, 1, 2])
 @pytest.mark.parametrize("p", [1, 2, 3, 4, 5])
 def test_hex_tensor_kernel(p, variant):
+    if p == 3 and variant != 0:
+        pytest.skip("hexahedra of order 3 have the slice kernel only")
     n = 4 if p <= 3 else 3
     got, ref, solver, gk, rk = run_pair(desc([n, n, n]), p, "advection", [1.0, 0.7, 0.3], "RK4_4",
                                         2e-3, 3, stages=True, variant=variant)
     assert solver.handle.kernel_kind == "tensor"
-    assert rel_err(got, ref) < max(RTOL, solver.stage_rtol * 2e-3 * 3 * 4)
+    assert rel_err(got, ref) < solver.solution_rtol
     for a, b in zip(gk, rk):
         assert rel_err(a, b) < solver.stage_rtol
 
@@ -162,14 +172,17 @@ def test_every_tableau(tableau):
     assert rel_err(got, ref) < RTOL
 
 
-def test_pipelined_and_one_shot_kernels_agree_on_a_large_ragged_mesh():
+@pytest.mark.parametrize("p", [2, 4])
+def test_pipelined_and_one_shot_kernels_agree_on_a_large_ragged_mesh(p):
     """Many tiles per block, a last tile that is only partly filled, every Dormand-Prince
     stage (more than one stage vector in the input): the two organisations of the
     sum-factorised kernel give the same numbers."""
     description = desc([13, 11, 9])
     res = []
-    for variant in (0, 1, 2, 3, 4):
-        s = hpgem_b200.Advection(3, 3, [-0.4, 0.9, 0.25], tableau="DormandPrince").readMesh(description)
+    # at p = 4 the last Dormand-Prince stage reads more vectors than the pipelined
+    # kernel's ring holds: variant 2 refuses it and the automatic choice takes variant 1
+    for variant in ((0, 1, 2) if p == 2 else (0, 1)):
+        s = hpgem_b200.Advection(3, p, [-0.4, 0.9, 0.25], tableau="DormandPrince").readMesh(description)
         s.handle.set_kernel_variant(variant)
         s.setInitialSolution(sine_field)
         s.computeTimeSteps(0.0, 1e-3, 5)
@@ -179,13 +192,30 @@ def test_pipelined_and_one_shot_kernels_agree_on_a_large_ragged_mesh():
             assert rel_err(a, b) < RTOL
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4])
-def test_hex_p3_kernels_on_a_ragged_mesh_rk4(variant):
+def test_hex_p3_slice_kernel_dormand_prince_ragged():
+    """Hexahedra p = 3, every Dormand-Prince stage (up to six stage vectors in the input
+    and five in the final update), 1287 elements (last tile partly filled), stage
+    vectors and solution against the oracle."""
+    got, ref, solver, gk, rk = run_pair(desc([13, 11, 9]), 3, "advection", [-0.4, 0.9, 0.25],
+                                        "DormandPrince", 1e-3, 2, stages=True)
+    assert rel_err(got, ref) < RTOL
+    for a, b in zip(gk, rk):
+        assert rel_err(a, b) < solver.stage_rtol
+
+
+def test_hex_p3_kernel_ragged_mesh_rk4():
     """Hexahedra p = 3 with RK4: element count not a multiple of the tile, negative and
     positive velocity components, against the oracle."""
-    got, ref, solver = run_pair(desc([7, 5, 3]), 3, "advection", [-0.6, 0.8, -0.3], "RK4_4", 2e-3, 4,
-                                variant=variant)
+    got, ref, solver = run_pair(desc([7, 5, 3]), 3, "advection", [-0.6, 0.8, -0.3], "RK4_4", 2e-3, 4)
     assert rel_err(got, ref) < RTOL
+
+
+def test_hex_p3_rejects_other_kernel_organisations():
+    s = hpgem_b200.Advection(3, 3, [1.0, 0.7, 0.3]).readMesh(desc([4, 4, 4]))
+    with pytest.raises(_native.NativeError) as ex:
+        s.handle.set_kernel_variant(1)
+    assert ex.value.code == -2  # HGG_ERR_UNSUPPORTED
+    s.handle.set_kernel_variant(0)
 
 
 @pytest.fixture(scope="module")
@@ -197,13 +227,11 @@ def many_tiles_reference():
     return description, u0, ref, ref_k, stage_rtol(prob)
 
 
-@pytest.mark.parametrize("variant", [0, 1])
-def test_hex_p3_many_tiles(variant, many_tiles_reference):
+def test_hex_p3_many_tiles(many_tiles_reference):
     """More tiles than SMs, x-neighbours inside and outside each tile, periodic wrap in
     every direction, a last tile that is only partly filled."""
     description, u0, ref, ref_k, srtol = many_tiles_reference
     solver = hpgem_b200.Advection(3, 3, [0.9, -0.5, 0.35], tableau="RK4_4").readMesh(description)
-    solver.handle.set_kernel_variant(variant)
     solver.setTimeIntegrationVector(0, u0)
     solver.computeTimeSteps(0.0, 1e-3, 2)
     assert rel_err(solver.getTimeIntegrationVector(0), ref) < RTOL
