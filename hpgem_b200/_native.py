@@ -23,7 +23,8 @@ EXPORTED = ["hgg_create", "hgg_destroy", "hgg_last_error", "hgg_set_state", "hgg
             "hgg_kernel_kind", "hgg_set_store_last_stage", "hgg_set_stream", "hgg_set_kernel_variant", "hgg_launch_count",
             "hgg_create_structured", "hgg_structured_descriptor", "hgg_free_descriptor",
             "hgg_quadrature_points", "hgg_num_quadrature_points",
-            "hgg_project", "hgg_num_error_points", "hgg_error_points", "hgg_l2_error"]
+            "hgg_project", "hgg_num_error_points", "hgg_error_points", "hgg_l2_error",
+            "hgg_time_derivative_static"]
 
 
 class ProblemDesc(ctypes.Structure):
@@ -74,6 +75,7 @@ def load():
         "hgg_get_state": (ctypes.c_int, [H, ctypes.c_int32, P]),
         "hgg_step": (ctypes.c_int, [H, ctypes.POINTER(ctypes.c_double), ctypes.c_double, ctypes.c_int32]),
         "hgg_time_derivative": (ctypes.c_int, [H, ctypes.c_int32, ctypes.c_int32]),
+        "hgg_time_derivative_static": (ctypes.c_int, [H, ctypes.c_void_p, ctypes.c_void_p]),
         "hgg_synchronize": (ctypes.c_int, [H]),
         "hgg_vector_length": (ctypes.c_int64, [H]),
         "hgg_kernel_kind": (ctypes.c_int, [H]),

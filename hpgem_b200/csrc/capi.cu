@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -600,6 +601,74 @@ int hgg_set_kernel_variant(hgg_handle *h, int32_t variant) {
         h->variant = variant;
     }
     return 0;
+}
+
+// ---- right-hand side without allocation ---------------------------------------
+// The sum-factorised handles keep their vectors in tensor order on the device,
+// so a right-hand side of caller-owned vectors in hpGEM order needs two
+// vectors of scratch (the input in device order, the output in device order).
+// This entry point takes them from one file-scope device array instead of the
+// allocator.  Every process that loads the library holds the array on every
+// GPU it uses until exit; all calls on a device share it.
+
+namespace {
+constexpr int64_t kStaticScratchDoubles = int64_t(1) << 22;  // 32 MiB
+constexpr int kMaxStaticDevices = 64;
+static __device__ __align__(256) double g_static_scratch[kStaticScratchDoubles];
+std::mutex g_static_mutex;
+double *g_static_ptr[kMaxStaticDevices] = {};
+}  // namespace
+
+int hgg_time_derivative_static(hgg_handle *h, const double *u, double *k) {
+    if (!h) return fail(h, HGG_ERR_INVALID, "null handle");
+    if (!u || !k || u == k) return fail(h, HGG_ERR_INVALID, "u and k must be distinct device vectors");
+    int dev = -1;
+    HGG_CUDA(h, cudaGetDevice(&dev));
+    if (dev != h->device) return fail(h, HGG_ERR_INVALID, "call with the handle's device current");
+    StageIO io{};
+    io.n_elements = h->op.nE;
+    io.status = h->d_status;
+    if (!h->tensor_layout) {  // the dense kernels read and write hpGEM order: no scratch
+        io.u = u;
+        io.kout = k;
+        int rc = launch_stage(h, io);
+        if (rc) return rc;
+        return check_status(h);
+    }
+    if (2 * h->N_alloc > kStaticScratchDoubles)
+        return fail(h, HGG_ERR_UNSUPPORTED,
+                    "problem needs " + std::to_string(2 * h->N_alloc) + " doubles of scratch; the static scratch holds " +
+                        std::to_string(kStaticScratchDoubles) + " (" + std::to_string(kStaticScratchDoubles / 2) +
+                        " per vector, padded to whole tiles)");
+    double *base = nullptr;
+    {
+        // first call on a device: look the array up, with that device current
+        std::lock_guard<std::mutex> lock(g_static_mutex);
+        if (dev < 0 || dev >= kMaxStaticDevices) return fail(h, HGG_ERR_UNSUPPORTED, "device ordinal too large");
+        if (!g_static_ptr[dev]) {
+            void *p = nullptr;
+            cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+            if (e != cudaSuccess)
+                return fail(h, HGG_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+            g_static_ptr[dev] = static_cast<double *>(p);
+        }
+        base = g_static_ptr[dev];
+    }
+    double *su = base, *sk = base + h->N_alloc;
+    // the padding of the last tile is read (and ignored) by the stage kernel: keep it zero
+    if (h->N_alloc > h->N)
+        HGG_CUDA(h, cudaMemsetAsync(su + h->N, 0, sizeof(double) * (h->N_alloc - h->N), h->stream));
+    to_tensor_order<<<4 * h->num_sms, 256, 0, h->stream>>>(u, su, h->d_tpos, h->d_tsign, h->op.nB, h->N, h->tiled);
+    h->launches++;
+    HGG_CUDA(h, cudaGetLastError());
+    io.u = su;
+    io.kout = sk;
+    int rc = launch_stage(h, io);
+    if (rc) return rc;
+    from_tensor_order<<<4 * h->num_sms, 256, 0, h->stream>>>(sk, k, h->d_tpos, h->d_tsign, h->op.nB, h->N, h->tiled);
+    h->launches++;
+    HGG_CUDA(h, cudaGetLastError());
+    return check_status(h);
 }
 
 // ---- stand-alone set-up ------------------------------------------------------

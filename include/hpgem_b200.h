@@ -175,6 +175,27 @@ int hgg_set_stream(hgg_handle *h, void *stream);
  * HGG_ERR_UNSUPPORTED there.  Ignored by the dense path. */
 int hgg_set_kernel_variant(hgg_handle *h, int32_t variant);
 
+/* Right-hand side k = M^{-1} R(u) of caller-owned DEVICE vectors u and k, both
+ * in hpGEM order (length hgg_vector_length), without any allocation: no
+ * cudaMalloc, cudaFree or allocating library call.  No counterpart in the
+ * reference: it exists for callers that cannot allocate device memory while
+ * they step (a serving loop that admits work by a fixed HBM budget, a host
+ * application whose memory manager owns the device, code running where an
+ * allocation's implicit device synchronisation would stall co-scheduled
+ * work).  The sum-factorised handles need two vectors of scratch; they come
+ * from one file-scope device array of 2^22 doubles (32 MiB) that every GPU
+ * using the library holds until the process exits, so the padded vector
+ * (hgg_vector_length rounded up to whole 32-element tiles) may hold at most
+ * 2^21 doubles, else HGG_ERR_UNSUPPORTED (32^3 hexahedra at p = 3 is the
+ * largest cube mesh of that order).  The first call on a device looks the
+ * array up (with the handle's device current, which every call requires);
+ * make that first call before any stream capture.  All calls on a device
+ * share the array and it keeps the last call's contents (the part that must
+ * read as zero is cleared each call): calls that overlap on the GPU, from
+ * different streams or handles, race.  Runs on the handle's stream and
+ * returns after it (like hgg_time_derivative, whose result it reproduces). */
+int hgg_time_derivative_static(hgg_handle *h, const double *u, double *k);
+
 /* Number of kernel launches the library issued on this handle so far. */
 int64_t hgg_launch_count(const hgg_handle *h);
 
