@@ -18,6 +18,13 @@ A "step" is one RK4 time step of the whole mesh (4 stage kernels).
 The five state vectors (134 MB each) exceed the 126 MB L2, so no flush is
 needed between steps.
 
+`forms` repeats the measurement in the FP32-mixed form (stage vectors and
+contractions in FP32; solution, geometry and the Runge-Kutta accumulation in
+FP64) and states for both forms the L2 error of the 200-step solution against
+the exact translated bump u0(x - a t) (periodic wrap; rule of order 2p+2), and
+for the mixed form its L2 distance and largest relative coefficient difference
+to the FP64 solution.
+
 --impl reference times the CPU oracle (the restated hpGEM loop: quadrature
 loops, per-element mass matrix rebuilt and LU-solved every stage) on all host
 cores as independent replica processes, each on a 2^3 sample of the same mesh
@@ -52,7 +59,11 @@ SOLVE_STEPS = 200
 # store is switched off here, with it the stage moves 48 B).  State: 104 B.
 # Plus per-stage geometry 4 * (G_e + (F/E) G_f) / nB = 4 * (80 + 3 * 48) / 64 = 14 B
 B_STATE = 16.0 + 24.0 + 24.0 + 40.0
-B_ALG = B_STATE + 4.0 * (8 * (3 * 3 + 1) + 3 * (8 * (3 + 1) + 16)) / 64.0
+B_GEO = 4.0 * (8 * (3 * 3 + 1) + 3 * (8 * (3 + 1) + 16)) / 64.0
+B_ALG = B_STATE + B_GEO
+# FP32-mixed form: stage vectors stored in FP32 (u and u^{n+1} stay FP64):
+# 12 + 16 + 16 + 28 = 72 B of state
+B_ALG_MIXED = (8.0 + 4) + (8 + 4 + 4) + (8 + 4 + 4) + (8 + 3 * 4 + 8) + B_GEO
 
 
 def description(n):
@@ -198,10 +209,16 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------------------
+def exact_translated(x, t):
+    """u0(x - a t) with the periodic wrap of the unit cube."""
+    return bump(np.mod(x - t * np.asarray(ADV), 1.0))
+
+
 def run_ours(args):
     import torch
 
     import hpgem_b200
+    from hpgem_b200 import _native
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -223,86 +240,117 @@ def run_ours(args):
         if dist is not None:
             dist.barrier()
 
-    solver = hpgem_b200.Advection(3, ORDER, ADV, tableau="RK4_4").readMesh(description(N_CELLS))
-    h = solver.handle
-    ndof = h.vector_length
-    solver.setInitialSolution(bump)
-    u0 = solver.getTimeIntegrationVector(0).reshape(-1).copy()
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        tt = torch.tensor([x], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        return float(tt.item())
+
     # a dedicated (non-default) stream: the library launches on it, the events are recorded on it
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
-    h.set_stream(stream.cuda_stream)
-    h.set_store_last_stage(False)
-    assert h.kernel_kind == "tensor"
 
-    # warm-up
-    t = h.step(0.0, DT, max(args.warmup, 3))
-    torch.cuda.synchronize()
+    def measure(precision, sample_clocks):
+        """K timed steps with the state resident, then the end-to-end solve (host in, host out)."""
+        solver = hpgem_b200.Advection(3, ORDER, ADV, tableau="RK4_4", precision=precision)
+        solver.readMesh(description(N_CELLS))
+        h = solver.handle
+        ndof = h.vector_length
+        solver.setInitialSolution(bump)
+        u0 = solver.getTimeIntegrationVector(0).reshape(-1).copy()
+        h.set_stream(stream.cuda_stream)
+        h.set_store_last_stage(False)
+        assert h.kernel_kind == "tensor"
+        t = h.step(0.0, DT, max(args.warmup, 3))
+        torch.cuda.synchronize()
+        sampler = ClockSampler(dev) if sample_clocks else None
+        if sampler:
+            sampler.start()
+            time.sleep(0.2)
+        launches0 = h.launch_count
+        barrier()
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        t = h.step(t, DT, args.steps)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        clocks = sampler.stop() if sampler else None
+        launches = h.launch_count - launches0
+        ms = max_over_ranks(ev0.elapsed_time(ev1))
+        # end to end: host initial coefficients in, host solution out, one 200-step solve each
+        host_in = torch.from_numpy(u0).pin_memory()
+        host_out = torch.empty_like(host_in).pin_memory()
+        reps = 2
+        h.step(0.0, DT, 1)
+        torch.cuda.synchronize()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            h.set_state_ptr(0, host_in.data_ptr())
+            h.step(0.0, DT, SOLVE_STEPS)
+            h.get_state_ptr(0, host_out.data_ptr())
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        e2e_ms = max_over_ranks(e0.elapsed_time(e1) / reps)
+        u_end = host_out.numpy().copy()
+        return dict(solver=solver, ndof=ndof, ms=ms, launches=launches, clocks=clocks,
+                    e2e_ms=e2e_ms, u_end=u_end)
 
-    sampler = ClockSampler(dev)
-    sampler.start()
-    time.sleep(0.2)
-    launches0 = h.launch_count
-    barrier()
-    torch.cuda.synchronize()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ev0.record(stream)
-    t = h.step(t, DT, args.steps)
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    barrier()
-    clocks = sampler.stop()
-    launches = h.launch_count - launches0
-    ms = ev0.elapsed_time(ev1)
-    if dist is not None:
-        tt = torch.tensor([ms], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
-    value = ndof * args.steps * world / (ms / 1e3)
+    f64 = measure(_native.PRECISION_FP64, True)
+    ndof = f64["ndof"]
+    value = ndof * args.steps * world / (f64["ms"] / 1e3)
+    e2e_value = ndof * SOLVE_STEPS * world / (f64["e2e_ms"] / 1e3)
+    f32 = measure(_native.PRECISION_FP32, False)
 
-    # end to end: host initial coefficients in, host solution out, one 200-step solve each
-    host_in = torch.from_numpy(u0).pin_memory()
-    host_out = torch.empty_like(host_in).pin_memory()
-    reps = 2
-    h.step(0.0, DT, 1)
-    torch.cuda.synchronize()
-    barrier()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(reps):
-        h.set_state_ptr(0, host_in.data_ptr())
-        h.step(0.0, DT, SOLVE_STEPS)
-        h.get_state_ptr(0, host_out.data_ptr())
-    e1.record(stream)
-    torch.cuda.synchronize()
-    barrier()
-    e2e_ms = e0.elapsed_time(e1) / reps
-    if dist is not None:
-        tt = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_ms = float(tt.item())
-    e2e_value = ndof * SOLVE_STEPS * world / (e2e_ms / 1e3)
-    finite = bool(np.isfinite(host_out.numpy()).all())
+    # errors of the 200-step solutions (rank 0; every rank runs the same replica)
+    forms = {}
+    if rank == 0:
+        s64 = f64["solver"]
+        T = SOLVE_STEPS * DT
+        err64 = s64.computeTotalError(exact_translated, T)
+        s64.setTimeIntegrationVector(0, f32["u_end"])
+        err32 = s64.computeTotalError(exact_translated, T)
+        d = s64.l2Distance(f32["u_end"], f64["u_end"])
+        rel = float(np.abs(f32["u_end"] - f64["u_end"]).max() / np.abs(f64["u_end"]).max())
+        for name, r, extra in (("fp64", f64, {"l2_error_vs_exact": err64}),
+                               ("fp32_mixed", f32, {"l2_error_vs_exact": err32, "l2_distance_to_fp64": d,
+                                                    "max_rel_coef_diff_vs_fp64": rel})):
+            forms[name] = dict({"value": ndof * args.steps * world / (r["ms"] / 1e3),
+                                "ms_per_step": r["ms"] / args.steps,
+                                "e2e_value": ndof * SOLVE_STEPS * world / (r["e2e_ms"] / 1e3),
+                                "solve_steps": SOLVE_STEPS}, **extra)
+        forms["fp32_mixed"]["stage_vector_bytes"] = 4
+        forms["fp32_mixed"]["algorithmic_bytes_per_dof_update"] = B_ALG_MIXED
+        forms["fp32_mixed"]["roofline_frac"] = (B_ALG_MIXED * forms["fp32_mixed"]["value"] / world / 1e9
+                                                / measured_peak_hbm()[0])
+        forms["note"] = ("errors of the 200-step solve; the FP64 GPU form equals the oracle to 1e-12 on "
+                         "every parity case, so it is the reference at this size")
 
     peak, peak_kind = measured_peak_hbm()
-    step_s = (ms / 1e3) / args.steps
+    step_s = (f64["ms"] / 1e3) / args.steps
     achieved = B_ALG * ndof / step_s / 1e9
     tr = traffic_per_dof_step()
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "warmup": args.warmup, "ms_per_step": f64["ms"] / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": dict(config(), parallelism="replicas%d" % world),
-            "clocks": clocks,
+            "clocks": f64["clocks"],
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": ndof * 8,
                     "d2h_bytes_per_step": ndof * 8, "step": "one %d-step solve" % SOLVE_STEPS,
-                    "ms_per_step": e2e_ms, "finite": finite},
-            "gpu_launches": int(launches),
+                    "ms_per_step": f64["e2e_ms"], "finite": bool(np.isfinite(f64["u_end"]).all())},
+            "gpu_launches": int(f64["launches"]),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
                          "kernel": "tensor_slice (4 launches per step, back to back in one graph)",
                          "algorithmic_bytes_per_dof_update": B_ALG,
                          "traffic": (tr * ndof if tr else None),
-                         "traffic_unit": "bytes per RK4 step (4 launches)"}}
+                         "traffic_unit": "bytes per RK4 step (4 launches)"},
+            "forms": forms}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, sample = cpu_sample_rate()
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",

@@ -44,7 +44,8 @@ struct hgg_handle {
     int64_t N_alloc = 0;           // doubles allocated per vector (whole tiles)
     double *sol[2] = {nullptr, nullptr};
     int cur = 0;                   // which sol[] holds the solution
-    std::vector<double *> k;       // S stage vectors
+    std::vector<void *> k;         // S stage vectors (double, or float in the FP32-mixed form)
+    bool mixed = false;            // FP32-mixed form: float stage vectors and contractions
     std::vector<DevBuf> bufs;      // every device allocation
     // device operator / geometry arrays
     double *d_vol = nullptr, *d_pairs = nullptr, *d_elem_geo = nullptr, *d_face_geo = nullptr;
@@ -146,24 +147,36 @@ TensorConsts<P, DIM> tensor_consts(const HostOperators &op) {
 __device__ __forceinline__ int64_t device_index(int64_t e, int pos, int nb, bool tiled) {
     return tiled ? (e >> 5) * ((int64_t)nb << 5) + (int64_t)pos * 32 + (e & 31) : e * nb + pos;
 }
-__global__ void to_tensor_order(const double *src, double *dst, const int32_t *tpos, const double *tsign,
+template <typename TD>
+__global__ void to_tensor_order(const double *src, TD *dst, const int32_t *tpos, const double *tsign,
                                 int nb, int64_t n, bool tiled) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const int64_t e = i / nb;
         const int k = (int)(i - e * nb);
-        dst[device_index(e, tpos[k], nb, tiled)] = tsign[k] * src[i];
+        dst[device_index(e, tpos[k], nb, tiled)] = (TD)(tsign[k] * src[i]);
     }
 }
-__global__ void from_tensor_order(const double *src, double *dst, const int32_t *tpos, const double *tsign,
+template <typename TS>
+__global__ void from_tensor_order(const TS *src, double *dst, const int32_t *tpos, const double *tsign,
                                   int nb, int64_t n, bool tiled) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const int64_t e = i / nb;
         const int k = (int)(i - e * nb);
-        dst[i] = tsign[k] * src[device_index(e, tpos[k], nb, tiled)];
+        dst[i] = tsign[k] * (double)src[device_index(e, tpos[k], nb, tiled)];
     }
 }
+// plain precision conversion of a vector (FP32-mixed stage vectors without layout change)
+__global__ void convert_vector(const double *src, float *dst, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        dst[i] = (float)src[i];
+}
+__global__ void convert_vector(const float *src, double *dst, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        dst[i] = (double)src[i];
+}
 
-int launch_slice(hgg_handle *h, const StageIO &io) {
+template <typename KT>
+int launch_slice(hgg_handle *h, const StageIOT<KT> &io) {
     const HostOperators &op = h->op;
     SliceOps sops;
     for (int i = 0; i < 16; ++i) sops.D[i] = op.D1[i];
@@ -173,13 +186,13 @@ int launch_slice(hgg_handle *h, const StageIO &io) {
     const dim3 grid((unsigned)blocks), block(SliceShape::THREADS);
     const bool fin = io.unew != nullptr;
     if (io.nin == 0 && (!fin || io.nfin == 0))
-        tensor_slice<0, 0><<<grid, block, 0, h->stream>>>(io, h->d_slice_geo, sops);
+        tensor_slice<KT, 0, 0><<<grid, block, 0, h->stream>>>(io, h->d_slice_geo, sops);
     else if (io.nin == 1 && (!fin || io.nfin == 0))
-        tensor_slice<1, 0><<<grid, block, 0, h->stream>>>(io, h->d_slice_geo, sops);
+        tensor_slice<KT, 1, 0><<<grid, block, 0, h->stream>>>(io, h->d_slice_geo, sops);
     else if (io.nin == 1 && fin && io.nfin == 3)
-        tensor_slice<1, 3><<<grid, block, 0, h->stream>>>(io, h->d_slice_geo, sops);
+        tensor_slice<KT, 1, 3><<<grid, block, 0, h->stream>>>(io, h->d_slice_geo, sops);
     else
-        tensor_slice<-1, -1><<<grid, block, 0, h->stream>>>(io, h->d_slice_geo, sops);
+        tensor_slice<KT, -1, -1><<<grid, block, 0, h->stream>>>(io, h->d_slice_geo, sops);
     return 0;
 }
 
@@ -279,7 +292,7 @@ int launch_stage(hgg_handle *h, const StageIO &io) {
     const HostOperators &op = h->op;
     int rc;
     if (h->slice_ok) {
-        rc = launch_slice(h, io);
+        rc = launch_slice<double>(h, io);
     } else if (op.tensor) {
         rc = op.dim == 2 ? launch_tensor_dim<2>(h, io)
                          : (op.dim == 3 ? launch_tensor_dim<3>(h, io)
@@ -302,38 +315,56 @@ int launch_stage(hgg_handle *h, const StageIO &io) {
     return 0;
 }
 
-double *vector_ptr(hgg_handle *h, int vec) {
+// FP32-mixed form: the stage kernels that have it
+int launch_stage(hgg_handle *h, const StageIOT<float> &io) {
+    int rc;
+    if (h->slice_ok) rc = launch_slice(h, io);
+    else return fail(h, HGG_ERR_UNSUPPORTED, "the FP32-mixed form has no kernel for this shape and order");
+    if (rc) return rc;
+    h->launches++;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(h, HGG_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+    return 0;
+}
+
+// whether the mixed form has a kernel for this handle's shape and order
+bool mixed_supported(const hgg_handle *h) { return h->slice_ok; }
+
+void *vector_ptr(hgg_handle *h, int vec) {
     if (vec == 0) return h->sol[h->cur];
     if (vec >= 1 && vec <= h->S) return h->k[vec - 1];
     return nullptr;
 }
+bool vector_is_float(const hgg_handle *h, int vec) { return h->mixed && vec >= 1; }
 
 // One Runge-Kutta step from sol[from] into sol[1 - from] (stages as in
 // HpgemAPISimplified_Impl.h:788-820; zero tableau entries are skipped).
-int enqueue_step(hgg_handle *h, int from, double dt) {
+template <typename KT>
+int enqueue_step_t(hgg_handle *h, int from, double dt) {
     const int S = h->S;
     const double *u = h->sol[from];
+    auto kv = [&](int j) { return static_cast<KT *>(h->k[j]); };
     for (int i = 0; i < S; ++i) {
-        StageIO io{};
+        StageIOT<KT> io{};
         io.u = u;
         io.n_elements = h->op.nE;
         io.status = h->d_status;
         for (int j = 0; j < i; ++j) {
             double c = dt * h->rk_a[i * S + j];
             if (c != 0.0) {
-                io.kin[io.nin] = h->k[j];
+                io.kin[io.nin] = kv(j);
                 io.cin[io.nin] = c;
                 io.nin++;
             }
         }
         const bool last = i == S - 1;
-        io.kout = (!last || h->store_last) ? h->k[i] : nullptr;
+        io.kout = (!last || h->store_last) ? kv(i) : nullptr;
         if (last) {
             io.unew = h->sol[1 - from];
             for (int j = 0; j < S - 1; ++j) {
                 double b = dt * h->rk_b[j];
                 if (b != 0.0) {
-                    io.kfin[io.nfin] = h->k[j];
+                    io.kfin[io.nfin] = kv(j);
                     io.bfin[io.nfin] = b;
                     io.nfin++;
                 }
@@ -344,6 +375,10 @@ int enqueue_step(hgg_handle *h, int from, double dt) {
         if (rc) return rc;
     }
     return 0;
+}
+
+int enqueue_step(hgg_handle *h, int from, double dt) {
+    return h->mixed ? enqueue_step_t<float>(h, from, dt) : enqueue_step_t<double>(h, from, dt);
 }
 
 int check_status(hgg_handle *h) {
@@ -366,8 +401,9 @@ int create_from_desc(const hgg_problem_desc *desc, hgg_handle *h) {
     h->rk_a.assign(desc->rk_a, desc->rk_a + h->S * h->S);
     h->rk_b.assign(desc->rk_b, desc->rk_b + h->S);
     h->rk_c = desc->rk_c ? std::vector<double>(desc->rk_c, desc->rk_c + h->S) : std::vector<double>(h->S, 0.0);
-    if (desc->precision != HGG_PRECISION_FP64)
-        return fail(h, HGG_ERR_UNSUPPORTED, "only the FP64 precision form is available in this build");
+    if (desc->precision != HGG_PRECISION_FP64 && desc->precision != HGG_PRECISION_FP32)
+        return fail(h, HGG_ERR_INVALID, "precision must be HGG_PRECISION_FP64 or HGG_PRECISION_FP32");
+    h->mixed = desc->precision == HGG_PRECISION_FP32;
     const HostOperators &op = h->op;
     h->N = op.nE * op.V * op.nB;
     h->tile_elems = op.tensor ? pipe_tile_elems(op.order, op.dim) : 1;
@@ -375,6 +411,8 @@ int create_from_desc(const hgg_problem_desc *desc, hgg_handle *h) {
     h->slice_ok = op.tensor && op.dim == 3 && op.order == 3 && op.trace_pos[0] == 0 && op.trace_pos[1] == 1;
     h->tiled = h->slice_ok;
     if (h->slice_ok) h->tile_elems = SliceShape::TE;
+    if (h->mixed && !mixed_supported(h))
+        return fail(h, HGG_ERR_UNSUPPORTED, "the FP32-mixed form has no kernel for this shape and order");
     const int64_t n_pad = (op.nE + h->tile_elems - 1) / h->tile_elems * h->tile_elems;
     h->N_alloc = n_pad * op.V * op.nB;
 
@@ -390,9 +428,10 @@ int create_from_desc(const hgg_problem_desc *desc, hgg_handle *h) {
         if ((rc = alloc(h, sizeof(double) * h->N_alloc, (void **)&h->sol[i]))) return rc;
     h->k.resize(h->S);
     for (int i = 0; i < h->S; ++i)
-        if ((rc = alloc(h, sizeof(double) * h->N_alloc, (void **)&h->k[i]))) return rc;
+        if ((rc = alloc(h, (h->mixed ? sizeof(float) : sizeof(double)) * h->N_alloc, &h->k[i]))) return rc;
     for (int i = 0; i < 2; ++i) HGG_CUDA(h, cudaMemsetAsync(h->sol[i], 0, sizeof(double) * h->N_alloc, h->stream));
-    for (int i = 0; i < h->S; ++i) HGG_CUDA(h, cudaMemsetAsync(h->k[i], 0, sizeof(double) * h->N_alloc, h->stream));
+    for (int i = 0; i < h->S; ++i)
+        HGG_CUDA(h, cudaMemsetAsync(h->k[i], 0, (h->mixed ? sizeof(float) : sizeof(double)) * h->N_alloc, h->stream));
     if ((rc = alloc(h, sizeof(int), (void **)&h->d_status))) return rc;
     HGG_CUDA(h, cudaMemsetAsync(h->d_status, 0, sizeof(int), h->stream));
     if (op.tensor) {
@@ -437,6 +476,7 @@ int create_from_desc(const hgg_problem_desc *desc, hgg_handle *h) {
         if ((rc = upload(h, tp, &h->d_tpos)) || (rc = upload(h, op.tsign, &h->d_tsign))) return rc;
         if ((rc = alloc(h, sizeof(double) * h->N_alloc, (void **)&h->d_scratch))) return rc;
     } else {
+        if (h->mixed && (rc = alloc(h, sizeof(double) * h->N_alloc, (void **)&h->d_scratch))) return rc;
         if ((rc = upload(h, op.vol, &h->d_vol)) || (rc = upload(h, op.pairs, &h->d_pairs)) ||
             (rc = upload(h, op.nbr, &h->d_nbr)) || (rc = upload(h, op.self_pair, &h->d_self)) ||
             (rc = upload(h, op.nbr_pair, &h->d_nbrp)) || (rc = upload(h, op.mode, &h->d_mode)) ||
@@ -485,12 +525,20 @@ const char *hgg_last_error(const hgg_handle *h) { return h ? h->err.c_str() : g_
 
 int hgg_set_state(hgg_handle *h, int32_t vec, const double *host) {
     if (!h || !host) return fail(h, HGG_ERR_INVALID, "null argument");
-    double *d = vector_ptr(h, vec);
+    void *d = vector_ptr(h, vec);
     if (!d) return fail(h, HGG_ERR_INVALID, "vector id out of range");
-    if (h->tensor_layout) {
+    const bool f = vector_is_float(h, vec);
+    const unsigned grid = 4 * h->num_sms;
+    if (h->tensor_layout || f) {
         HGG_CUDA(h, cudaMemcpyAsync(h->d_scratch, host, sizeof(double) * h->N, cudaMemcpyHostToDevice, h->stream));
-        to_tensor_order<<<4 * h->num_sms, 256, 0, h->stream>>>(h->d_scratch, d, h->d_tpos, h->d_tsign,
-                                                               h->op.nB, h->N, h->tiled);
+        if (h->tensor_layout && f)
+            to_tensor_order<float><<<grid, 256, 0, h->stream>>>(h->d_scratch, static_cast<float *>(d), h->d_tpos,
+                                                                 h->d_tsign, h->op.nB, h->N, h->tiled);
+        else if (h->tensor_layout)
+            to_tensor_order<double><<<grid, 256, 0, h->stream>>>(h->d_scratch, static_cast<double *>(d), h->d_tpos,
+                                                                  h->d_tsign, h->op.nB, h->N, h->tiled);
+        else
+            convert_vector<<<grid, 256, 0, h->stream>>>(h->d_scratch, static_cast<float *>(d), h->N);
         h->launches++;
         HGG_CUDA(h, cudaGetLastError());
     } else {
@@ -502,16 +550,25 @@ int hgg_set_state(hgg_handle *h, int32_t vec, const double *host) {
 
 int hgg_get_state(hgg_handle *h, int32_t vec, double *host) {
     if (!h || !host) return fail(h, HGG_ERR_INVALID, "null argument");
-    double *d = vector_ptr(h, vec);
+    void *d = vector_ptr(h, vec);
     if (!d) return fail(h, HGG_ERR_INVALID, "vector id out of range");
-    if (h->tensor_layout) {
-        from_tensor_order<<<4 * h->num_sms, 256, 0, h->stream>>>(d, h->d_scratch, h->d_tpos, h->d_tsign,
-                                                                 h->op.nB, h->N, h->tiled);
+    const bool f = vector_is_float(h, vec);
+    const unsigned grid = 4 * h->num_sms;
+    const double *src = static_cast<const double *>(d);
+    if (h->tensor_layout || f) {
+        if (h->tensor_layout && f)
+            from_tensor_order<float><<<grid, 256, 0, h->stream>>>(static_cast<const float *>(d), h->d_scratch,
+                                                                   h->d_tpos, h->d_tsign, h->op.nB, h->N, h->tiled);
+        else if (h->tensor_layout)
+            from_tensor_order<double><<<grid, 256, 0, h->stream>>>(static_cast<const double *>(d), h->d_scratch,
+                                                                    h->d_tpos, h->d_tsign, h->op.nB, h->N, h->tiled);
+        else
+            convert_vector<<<grid, 256, 0, h->stream>>>(static_cast<const float *>(d), h->d_scratch, h->N);
         h->launches++;
         HGG_CUDA(h, cudaGetLastError());
-        d = h->d_scratch;
+        src = h->d_scratch;
     }
-    HGG_CUDA(h, cudaMemcpyAsync(host, d, sizeof(double) * h->N, cudaMemcpyDeviceToHost, h->stream));
+    HGG_CUDA(h, cudaMemcpyAsync(host, src, sizeof(double) * h->N, cudaMemcpyDeviceToHost, h->stream));
     HGG_CUDA(h, cudaStreamSynchronize(h->stream));
     return 0;
 }
@@ -551,14 +608,27 @@ int hgg_step(hgg_handle *h, double *time, double dt, int32_t nsteps) {
 
 int hgg_time_derivative(hgg_handle *h, int32_t in_vec, int32_t out_vec) {
     if (!h) return fail(h, HGG_ERR_INVALID, "null handle");
-    double *in = vector_ptr(h, in_vec), *outp = vector_ptr(h, out_vec);
+    void *in = vector_ptr(h, in_vec), *outp = vector_ptr(h, out_vec);
     if (!in || !outp || in == outp) return fail(h, HGG_ERR_INVALID, "bad vector ids");
-    StageIO io{};
-    io.u = in;
-    io.kout = outp;
-    io.n_elements = h->op.nE;
-    io.status = h->d_status;
-    int rc = launch_stage(h, io);
+    int rc;
+    if (h->mixed) {
+        // FP32-mixed form: FP64 input (the solution), FP32 stage vector output
+        if (vector_is_float(h, in_vec) || !vector_is_float(h, out_vec))
+            return fail(h, HGG_ERR_INVALID, "the FP32-mixed form maps the solution (vector 0) to a stage vector");
+        StageIOT<float> io{};
+        io.u = static_cast<const double *>(in);
+        io.kout = static_cast<float *>(outp);
+        io.n_elements = h->op.nE;
+        io.status = h->d_status;
+        rc = launch_stage(h, io);
+    } else {
+        StageIO io{};
+        io.u = static_cast<const double *>(in);
+        io.kout = static_cast<double *>(outp);
+        io.n_elements = h->op.nE;
+        io.status = h->d_status;
+        rc = launch_stage(h, io);
+    }
     if (rc) return rc;
     return check_status(h);
 }
@@ -625,6 +695,7 @@ int hgg_time_derivative_static(hgg_handle *h, const double *u, double *k) {
     int dev = -1;
     HGG_CUDA(h, cudaGetDevice(&dev));
     if (dev != h->device) return fail(h, HGG_ERR_INVALID, "call with the handle's device current");
+    if (h->mixed) return fail(h, HGG_ERR_UNSUPPORTED, "the FP32-mixed form has no static-scratch right-hand side");
     StageIO io{};
     io.n_elements = h->op.nE;
     io.status = h->d_status;
@@ -658,14 +729,16 @@ int hgg_time_derivative_static(hgg_handle *h, const double *u, double *k) {
     // the padding of the last tile is read (and ignored) by the stage kernel: keep it zero
     if (h->N_alloc > h->N)
         HGG_CUDA(h, cudaMemsetAsync(su + h->N, 0, sizeof(double) * (h->N_alloc - h->N), h->stream));
-    to_tensor_order<<<4 * h->num_sms, 256, 0, h->stream>>>(u, su, h->d_tpos, h->d_tsign, h->op.nB, h->N, h->tiled);
+    to_tensor_order<double><<<4 * h->num_sms, 256, 0, h->stream>>>(u, su, h->d_tpos, h->d_tsign, h->op.nB, h->N,
+                                                                    h->tiled);
     h->launches++;
     HGG_CUDA(h, cudaGetLastError());
     io.u = su;
     io.kout = sk;
     int rc = launch_stage(h, io);
     if (rc) return rc;
-    from_tensor_order<<<4 * h->num_sms, 256, 0, h->stream>>>(sk, k, h->d_tpos, h->d_tsign, h->op.nB, h->N, h->tiled);
+    from_tensor_order<double><<<4 * h->num_sms, 256, 0, h->stream>>>(sk, k, h->d_tpos, h->d_tsign, h->op.nB, h->N,
+                                                                      h->tiled);
     h->launches++;
     HGG_CUDA(h, cudaGetLastError());
     return check_status(h);

@@ -25,20 +25,25 @@ namespace hgg {
 constexpr int kMaxStages = 8;
 
 // Linear combination inputs and the fused final update of one stage.
-struct StageIO {
+// Inputs and outputs of one stage launch.  KT is the storage type of the
+// stage vectors: double in the FP64 form, float in the FP32-mixed form (the
+// solution and the Runge-Kutta accumulation stay FP64 in both).
+template <typename KT>
+struct StageIOT {
     const double *u;                 // current solution
-    const double *kin[kMaxStages];   // stage vectors entering the stage input
+    const KT *kin[kMaxStages];       // stage vectors entering the stage input
     double cin[kMaxStages];          // their coefficients dt * a_ij
     int nin;
-    double *kout;                    // this stage's derivative (nullptr: not stored)
+    KT *kout;                        // this stage's derivative (nullptr: not stored)
     double *unew;                    // final stage: new solution (nullptr otherwise)
-    const double *kfin[kMaxStages];  // earlier stage vectors of the final update
+    const KT *kfin[kMaxStages];      // earlier stage vectors of the final update
     double bfin[kMaxStages];         // their weights dt * b_j
     int nfin;
     double blast;                    // dt * b_S for the derivative computed in this stage
     int64_t n_elements;
     int *status;                     // device status word, bit 0: bad neighbour index
 };
+using StageIO = StageIOT<double>;
 
 __device__ __forceinline__ double stage_input(const StageIO &io, int64_t idx) {
     double w = io.u[idx];

@@ -28,6 +28,12 @@
 //   phase 3  the 16 outputs: x and y derivatives from registers, z derivative
 //            from the staged tile, lifts of the six face fluxes; kout and the
 //            final Runge-Kutta update are written coefficient by coefficient.
+//
+// Precision.  KT is the type of the stage vectors and of the contractions:
+// double (FP64 form) or float (FP32-mixed form: stage vectors stored in FP32,
+// stage input formed in FP64 from the FP64 solution and rounded once, the
+// derivative, lift and flux arithmetic in FP32, the geometry computed and
+// stored in FP64, the final update u + dt sum b_j k_j accumulated in FP64).
 #pragma once
 
 #include <cstdint>
@@ -60,22 +66,32 @@ __device__ __forceinline__ double ldg_f64(const double *p) {
     return v;
 }
 
-__device__ __forceinline__ double slice_flux(int md, double sg, double self, double nbr) {
-    return md == 1 ? sg * self : (md == 2 ? sg * nbr : (md == 3 ? 0.5 * sg * (self + nbr) : 0.0));
+__device__ __forceinline__ float ldg_f32(const float *p) {
+    float v;
+    asm("ld.global.nc.f32 %0, [%1];" : "=f"(v) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ double ldg_k(const double *p) { return ldg_f64(p); }
+__device__ __forceinline__ double ldg_k(const float *p) { return (double)ldg_f32(p); }
+
+template <typename CT>
+__device__ __forceinline__ CT slice_flux(int md, CT sg, CT self, CT nbr) {
+    return md == 1 ? sg * self : (md == 2 ? sg * nbr : (md == 3 ? CT(0.5) * sg * (self + nbr) : CT(0)));
 }
 
 // NIN / NFIN: number of stage vectors in the stage input / in the final
 // update, fixed at compile time for the common Runge-Kutta stages (so every
 // load loop unrolls and all loads of a phase are in flight together), or -1
 // for a count read from io.
-template <int NIN, int NFIN>
-__global__ void __launch_bounds__(SliceShape::THREADS, 4)
-    tensor_slice(const StageIO io, const double *__restrict__ geo, const SliceOps op) {
+template <typename KT, int NIN, int NFIN>
+__global__ void __launch_bounds__(SliceShape::THREADS, sizeof(KT) == 4 ? 5 : 4)
+    tensor_slice(const StageIOT<KT> io, const double *__restrict__ geo, const SliceOps op) {
+    using CT = KT;  // contraction type
     constexpr int TE = SliceShape::TE, WS = SliceShape::WS, ZS = SliceShape::ZS, GR = SliceShape::GR;
     constexpr int TILE = SliceShape::TILE;
     constexpr int tp0 = 0, tp1 = 1;  // psi_0 only mode at -1, psi_1 only mode at +1
-    __shared__ double W[TE * WS];
-    __shared__ double TZ[TE * ZS];
+    __shared__ CT W[TE * WS];
+    __shared__ CT TZ[TE * ZS];
     __shared__ double G[TE * GR];
 
     const int el = threadIdx.x & 31;
@@ -90,17 +106,22 @@ __global__ void __launch_bounds__(SliceShape::THREADS, 4)
 
     // ---- phase 1: geometry records, own slice, stage input -------------------------
     for (int i = threadIdx.x; i < TE * GR; i += SliceShape::THREADS) G[i] = ldg_f64(geo + t0 * GR + i);
-    double w[16];
+    CT w[16];
+    {
+        double wd[16];
 #pragma unroll
-    for (int i = 0; i < 16; ++i) w[i] = ldg_f64(io.u + base + 32 * (i + 16 * c));
+        for (int i = 0; i < 16; ++i) wd[i] = ldg_f64(io.u + base + 32 * (i + 16 * c));
 #pragma unroll
-    for (int jj = 0; jj < nin; ++jj) {
-        const double cj = io.cin[jj];
-        const double *kj = io.kin[jj] + base;
+        for (int jj = 0; jj < nin; ++jj) {
+            const double cj = io.cin[jj];
+            const KT *kj = io.kin[jj] + base;
 #pragma unroll
-        for (int i = 0; i < 16; ++i) w[i] += cj * ldg_f64(kj + 32 * (i + 16 * c));
+            for (int i = 0; i < 16; ++i) wd[i] += cj * ldg_k(kj + 32 * (i + 16 * c));
+        }
+#pragma unroll
+        for (int i = 0; i < 16; ++i) w[i] = (CT)wd[i];
     }
-    double *wrow = W + el * WS;
+    CT *wrow = W + el * WS;
 #pragma unroll
     for (int i = 0; i < 16; ++i) wrow[i + 16 * c] = w[i];
     __syncthreads();
@@ -125,47 +146,52 @@ __global__ void __launch_bounds__(SliceShape::THREADS, 4)
         const int tpo = (s & 1) ? tp0 : tp1;
         return s < 2 ? tpo + 4 * q + 16 * c : (s < 4 ? q + 4 * tpo + 16 * c : zm0 + q + 16 * tpo);
     };
-    double NB[5][8];
+    CT NB[5][8];
 #pragma unroll
     for (int f = 0; f < 5; ++f) {
         const int s = f < 4 ? f : zs;
         const int nq = f < 4 ? 4 : 8;
 #pragma unroll
-        for (int q = 0; q < 8; ++q) NB[f][q] = 0.0;
+        for (int q = 0; q < 8; ++q) NB[f][q] = CT(0);
         const int32_t n = gn[s];
         if (md[s] >= 2) {
             if (n >= t0 && n < t0 + TE) {
-                const double *nrow = W + (int)(n - t0) * WS;
+                const CT *nrow = W + (int)(n - t0) * WS;
 #pragma unroll
                 for (int q = 0; q < nq; ++q) NB[f][q] = nrow[nbr_pos(s, q)];
             } else {
                 const int64_t nbase = ((int64_t)n >> 5) * TILE + (n & 31);
+                double v[8];
 #pragma unroll
-                for (int q = 0; q < nq; ++q) NB[f][q] = ldg_f64(io.u + nbase + 32 * nbr_pos(s, q));
+                for (int q = 0; q < nq; ++q) v[q] = ldg_f64(io.u + nbase + 32 * nbr_pos(s, q));
 #pragma unroll
                 for (int jj = 0; jj < nin; ++jj) {
                     const double cj = io.cin[jj];
 #pragma unroll
-                    for (int q = 0; q < nq; ++q) NB[f][q] += cj * ldg_f64(io.kin[jj] + nbase + 32 * nbr_pos(s, q));
+                    for (int q = 0; q < nq; ++q) v[q] += cj * ldg_k(io.kin[jj] + nbase + 32 * nbr_pos(s, q));
                 }
+#pragma unroll
+                for (int q = 0; q < nq; ++q) NB[f][q] = (CT)v[q];
             }
         }
     }
-    double FX[2][4], FY[2][4];
+    CT FX[2][4], FY[2][4];
 #pragma unroll
     for (int side = 0; side < 2; ++side) {
         const int tps = side ? tp1 : tp0;
+        const CT sgx = (CT)g[3 + side], sgy = (CT)g[5 + side];
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-            FX[side][q] = slice_flux(md[side], g[3 + side], w[tps + 4 * q], NB[side][q]);
-            FY[side][q] = slice_flux(md[2 + side], g[5 + side], w[q + 4 * tps], NB[2 + side][q]);
+            FX[side][q] = slice_flux<CT>(md[side], sgx, w[tps + 4 * q], NB[side][q]);
+            FY[side][q] = slice_flux<CT>(md[2 + side], sgy, w[q + 4 * tps], NB[2 + side][q]);
         }
     }
     {
         const int tps = zside ? tp1 : tp0;
+        const CT sgz = (CT)g[3 + zs];
 #pragma unroll
         for (int q = 0; q < 8; ++q)
-            TZ[el * ZS + 16 * zside + zm0 + q] = slice_flux(md[zs], g[3 + zs], wrow[zm0 + q + 16 * tps], NB[4][q]);
+            TZ[el * ZS + 16 * zside + zm0 + q] = slice_flux<CT>(md[zs], sgz, wrow[zm0 + q + 16 * tps], NB[4][q]);
     }
     __syncthreads();
     if (!active) return;
@@ -178,38 +204,44 @@ __global__ void __launch_bounds__(SliceShape::THREADS, 4)
 #pragma unroll
         for (int jj = 0; jj < nfin; ++jj) {
             const double bj = io.bfin[jj];
-            const double *kj = io.kfin[jj] + base;
+            const KT *kj = io.kfin[jj] + base;
 #pragma unroll
-            for (int i = 0; i < 16; ++i) fu[i] += bj * ldg_f64(kj + 32 * (i + 16 * c));
+            for (int i = 0; i < 16; ++i) fu[i] += bj * ldg_k(kj + 32 * (i + 16 * c));
         }
     }
-    const double ax = g[0], ay = g[1], az = g[2];
-    double Dc[4], Lc0, Lc1;
+    const CT ax = (CT)g[0], ay = (CT)g[1], az = (CT)g[2];
+    CT D[16], L0[4], L1[4], Dc[4], Lc0, Lc1;
 #pragma unroll
-    for (int k = 0; k < 4; ++k)
-        Dc[k] = c == 0 ? op.D[k] : (c == 1 ? op.D[4 + k] : (c == 2 ? op.D[8 + k] : op.D[12 + k]));
-    Lc0 = c == 0 ? op.L[0][0] : (c == 1 ? op.L[0][1] : (c == 2 ? op.L[0][2] : op.L[0][3]));
-    Lc1 = c == 0 ? op.L[1][0] : (c == 1 ? op.L[1][1] : (c == 2 ? op.L[1][2] : op.L[1][3]));
-    const double *zrow = TZ + el * ZS;
+    for (int k = 0; k < 16; ++k) D[k] = (CT)op.D[k];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        L0[k] = (CT)op.L[0][k];
+        L1[k] = (CT)op.L[1][k];
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) Dc[k] = c == 0 ? D[k] : (c == 1 ? D[4 + k] : (c == 2 ? D[8 + k] : D[12 + k]));
+    Lc0 = c == 0 ? L0[0] : (c == 1 ? L0[1] : (c == 2 ? L0[2] : L0[3]));
+    Lc1 = c == 0 ? L1[0] : (c == 1 ? L1[1] : (c == 2 ? L1[2] : L1[3]));
+    const CT *zrow = TZ + el * ZS;
 #pragma unroll
     for (int b = 0; b < 4; ++b) {
 #pragma unroll
         for (int a = 0; a < 4; ++a) {
             const int i = a + 4 * b;
-            double sx = 0.0, sy = 0.0, sz = 0.0;
+            CT sx = CT(0), sy = CT(0), sz = CT(0);
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
-                sx += op.D[a * 4 + k] * w[k + 4 * b];
-                sy += op.D[b * 4 + k] * w[a + 4 * k];
+                sx += D[a * 4 + k] * w[k + 4 * b];
+                sy += D[b * 4 + k] * w[a + 4 * k];
                 sz += Dc[k] * (k == c ? w[i] : wrow[i + 16 * k]);
             }
-            double r = ax * sx + ay * sy + az * sz;
-            r -= op.L[0][a] * FX[0][b] + op.L[1][a] * FX[1][b];
-            r -= op.L[0][b] * FY[0][a] + op.L[1][b] * FY[1][a];
+            CT r = ax * sx + ay * sy + az * sz;
+            r -= L0[a] * FX[0][b] + L1[a] * FX[1][b];
+            r -= L0[b] * FY[0][a] + L1[b] * FY[1][a];
             r -= Lc0 * zrow[i] + Lc1 * zrow[16 + i];
             const int64_t off = base + 32 * (i + 16 * c);
             if (io.kout) io.kout[off] = r;
-            if (io.unew) io.unew[off] = fu[i] + io.blast * r;
+            if (io.unew) io.unew[off] = fu[i] + io.blast * (double)r;
         }
     }
 }

@@ -1,9 +1,11 @@
-"""Reads the host-built hgg_problem_desc of a structured mesh into numpy arrays."""
+"""Reads the host-built hgg_problem_desc of a structured mesh into numpy arrays
+(hgg_structured_descriptor: the tabulations, geometry and face table the
+library builds from a Preprocessor structured description)."""
 import ctypes
 
 import numpy as np
 
-from hpgem_b200 import _native
+from . import _native
 
 
 def _arr(ptr, shape, dtype):

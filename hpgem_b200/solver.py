@@ -171,6 +171,8 @@ class HpgemAPISimplified:
         """Creates the device problem from a Preprocessor 'structured' description."""
         self.handle = Handle.structured(description, self.polynomialOrder, self._physics_code,
                                         self.params, self.tableau, self.precision)
+        self._description = description
+        self._mass = None
         self.n_basis = _basis_count(self.dim, description, self.polynomialOrder)
         self.n_elements = self.handle.vector_length // (self.numberOfVariables * self.n_basis)
         return self
@@ -213,6 +215,21 @@ class HpgemAPISimplified:
 
     def setTimeIntegrationVector(self, vec, values):
         self.handle.set_state(vec, values)
+
+    def l2Distance(self, a, b):
+        """L2 norm of the difference of two coefficient vectors (hpGEM order) of this
+        mesh: sqrt(sum_e |J_e| d_e^T Mhat d_e), exact on affine elements (the element
+        rule of order 2p+1 integrates the degree-2p mass integrand exactly)."""
+        if getattr(self, "_mass", None) is None:
+            from .descriptor import structured_descriptor
+            D = structured_descriptor(self._description, self.polynomialOrder, self._physics_code,
+                                      self.params, self.tableau)
+            phi = D["basis_values"]
+            self._mass = np.einsum("q,qi,qj->ij", D["quad_weights"], phi, phi)
+            self._absdet = np.abs(np.linalg.det(D["jacobians"]))
+        nE, V, nB = self.n_elements, self.numberOfVariables, self.n_basis
+        d = (np.asarray(a, dtype=float) - np.asarray(b, dtype=float)).reshape(nE, V, nB)
+        return float(np.sqrt(np.einsum("evi,ij,evj,e->", d, self._mass, d, self._absdet)))
 
     def computeTotalError(self, exact, time, vec=0):
         """L2 error against exact(x[n, dim], t) -> [n] or [n, V], rule of order 2p+2."""

@@ -13,7 +13,7 @@ from oracle.mesh import mesh_from_description
 
 import hpgem_b200
 from hpgem_b200 import _native
-from descriptor_util import structured_descriptor
+from hpgem_b200.descriptor import structured_descriptor
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
@@ -98,6 +98,25 @@ def test_create_reports_a_missing_device_or_succeeds():
         lib.hgg_destroy(h)
     else:
         assert rc == -6 and b"device" in lib.hgg_last_error(None)
+
+
+def test_precision_forms_are_checked_before_the_device():
+    """An unknown precision is invalid; the FP32-mixed form exists only where a kernel
+    has it (hexahedra of order 3), which create decides before looking for a device."""
+    lib = _native.load()
+    h = ctypes.c_void_p()
+    a = (ctypes.c_double * 2)(1.0, 0.5)
+    quads = b"structured 1 2\n4 4\n0 0\n1 1\nrectangular\ntrue true\n"
+    assert lib.hgg_create_structured(quads, 2, 0, a, b"RK4_4", 7, ctypes.byref(h)) == -1
+    assert lib.hgg_create_structured(quads, 2, 0, a, b"RK4_4", _native.PRECISION_FP32, ctypes.byref(h)) == -2
+    assert b"FP32-mixed" in lib.hgg_last_error(None)
+    a3 = (ctypes.c_double * 3)(1.0, 0.7, 0.3)
+    cubes = b"structured 1 3\n4 4 4\n0 0 0\n1 1 1\nrectangular\ntrue true true\n"
+    rc = lib.hgg_create_structured(cubes, 3, 0, a3, b"RK4_4", _native.PRECISION_FP32, ctypes.byref(h))
+    if rc == 0:
+        lib.hgg_destroy(h)
+    else:
+        assert rc == -6
 
 
 def test_solve_step_count_rule():
