@@ -6,8 +6,9 @@ include/hpgem_b200.h): CUDA kernels for sm_100a plus the C++ host set-up.
 Build it with ``python -m hpgem_b200.build``.
 """
 from ._native import NativeError, ProblemDesc, load  # noqa: F401
+from .batch import Batch  # noqa: F401
 from .solver import (AcousticWave, Advection, Handle, HpgemAPISimplified,  # noqa: F401
                      structured_description)
 
-__all__ = ["AcousticWave", "Advection", "Handle", "HpgemAPISimplified", "NativeError",
+__all__ = ["AcousticWave", "Advection", "Batch", "Handle", "HpgemAPISimplified", "NativeError",
            "ProblemDesc", "load", "structured_description"]

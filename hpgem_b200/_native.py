@@ -24,7 +24,10 @@ EXPORTED = ["hgg_create", "hgg_destroy", "hgg_last_error", "hgg_set_state", "hgg
             "hgg_create_structured", "hgg_structured_descriptor", "hgg_free_descriptor",
             "hgg_quadrature_points", "hgg_num_quadrature_points",
             "hgg_project", "hgg_num_error_points", "hgg_error_points", "hgg_l2_error",
-            "hgg_time_derivative_static"]
+            "hgg_time_derivative_static",
+            "hgg_batch_create", "hgg_batch_destroy", "hgg_batch_last_error", "hgg_batch_add",
+            "hgg_batch_remove", "hgg_batch_step", "hgg_batch_synchronize", "hgg_batch_remaining",
+            "hgg_batch_set_autotune", "hgg_batch_launch_count", "hgg_batch_num_classes"]
 
 
 class ProblemDesc(ctypes.Structure):
@@ -67,6 +70,7 @@ def load():
     lib = ctypes.CDLL(LIB_PATH)
     H = ctypes.c_void_p
     P = ctypes.c_void_p
+    B = ctypes.c_void_p
     sig = {
         "hgg_create": (ctypes.c_int, [ctypes.POINTER(ProblemDesc), ctypes.POINTER(H)]),
         "hgg_destroy": (ctypes.c_int, [H]),
@@ -76,6 +80,17 @@ def load():
         "hgg_step": (ctypes.c_int, [H, ctypes.POINTER(ctypes.c_double), ctypes.c_double, ctypes.c_int32]),
         "hgg_time_derivative": (ctypes.c_int, [H, ctypes.c_int32, ctypes.c_int32]),
         "hgg_time_derivative_static": (ctypes.c_int, [H, ctypes.c_void_p, ctypes.c_void_p]),
+        "hgg_batch_create": (ctypes.c_int, [ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p)]),
+        "hgg_batch_destroy": (ctypes.c_int, [B]),
+        "hgg_batch_last_error": (ctypes.c_char_p, [B]),
+        "hgg_batch_add": (ctypes.c_int, [B, H, ctypes.c_double, ctypes.c_int32, ctypes.POINTER(ctypes.c_int32)]),
+        "hgg_batch_remove": (ctypes.c_int, [B, ctypes.c_int32]),
+        "hgg_batch_step": (ctypes.c_int, [B, ctypes.c_int32]),
+        "hgg_batch_synchronize": (ctypes.c_int, [B]),
+        "hgg_batch_remaining": (ctypes.c_int32, [B, ctypes.c_int32]),
+        "hgg_batch_set_autotune": (ctypes.c_int, [B, ctypes.c_int32]),
+        "hgg_batch_launch_count": (ctypes.c_int64, [B]),
+        "hgg_batch_num_classes": (ctypes.c_int32, [B]),
         "hgg_synchronize": (ctypes.c_int, [H]),
         "hgg_vector_length": (ctypes.c_int64, [H]),
         "hgg_kernel_kind": (ctypes.c_int, [H]),
@@ -107,5 +122,12 @@ def load():
 def check(code, handle=None):
     if code != 0:
         msg = load().hgg_last_error(handle)
+        raise NativeError(code, msg.decode() if msg else "")
+    return code
+
+
+def check_batch(code, batch=None):
+    if code != 0:
+        msg = load().hgg_batch_last_error(batch)
         raise NativeError(code, msg.decode() if msg else "")
     return code

@@ -1,0 +1,711 @@
+// Grouped execution of many independent problems (hgg_batch_*).
+//
+// Every problem keeps its own handle: its vectors and geometry stay resident
+// where hgg_create put them.  A batch groups its problems by kernel class
+// (kernel organisation, shape, order, physics, precision, tableau).  One RK
+// stage of a class is ONE persistent launch: its CTAs walk the virtual blocks
+// of all member problems (a prefix table of per-problem block counts, binary
+// searched per virtual block) and run the same per-block code as the
+// single-problem kernels, with that problem's stage inputs (its own dt and its
+// own current buffer).  Per problem the device holds the buffer parity (which
+// of its two solution buffers is current) and the steps still to take; a
+// small kernel at the end of every step flips the parity and counts down, so a
+// problem stops at exactly its own step count while the others go on.  The
+// classes of one step are captured into one CUDA graph as parallel branches
+// (fork/join on per-class streams) and the graph is replayed for every step;
+// adding or removing a problem rewrites the tables and recaptures.
+//
+// Kernel tile shapes are chosen per class by a small autotuner: candidate
+// launch shapes are timed on the class's own members with a stage-1 launch
+// (which writes only the first stage vector, scratch between steps), and the
+// fastest is cached per (class, size bucket) for the life of the process.
+#pragma once
+
+#include <map>
+#include <mutex>
+#include <tuple>
+
+namespace hgg {
+
+struct DenseItem {
+    StageIO io[2];  // [parity]: from sol[base] / from sol[1 - base]
+    DenseGeom g;
+    int64_t block0;  // first virtual block
+    int slot;
+};
+struct TensorItem {
+    StageIO io[2];
+    TensorGeom geo;
+    int64_t block0;
+    int slot;
+};
+template <typename KT>
+struct SliceItem {
+    StageIOT<KT> io[2];
+    const double *geo;
+    int64_t block0;
+    int slot;
+};
+
+// item whose virtual blocks contain vb (items sorted by block0, block0[0] = 0)
+template <typename Item>
+__device__ __forceinline__ int find_item(const Item *items, int n, int64_t vb) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (items[mid].block0 <= vb) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+template <int DIM, int NFL, int WAVE>
+__global__ void __launch_bounds__(256)
+    grouped_dense(const DenseItem *items, const int *n_items, const int64_t *total, const int *parity,
+                  const int *remaining) {
+    const int n = *n_items;
+    const int64_t nb = *total;
+    for (int64_t vb = blockIdx.x; vb < nb; vb += gridDim.x) {
+        const int i = find_item(items, n, vb);
+        const int slot = items[i].slot;
+        __syncthreads();  // shared memory of the previous virtual block is free
+        if (remaining[slot] <= 0) continue;
+        dense_stage_body<DIM, NFL, WAVE>(items[i].io[parity[slot]], items[i].g, vb - items[i].block0);
+    }
+}
+
+template <int P, int DIM, int EPB>
+__global__ void __launch_bounds__(EPB *TensorConsts<P, DIM>::NB)
+    grouped_tensor(const TensorItem *items, const int *n_items, const int64_t *total, const int *parity,
+                   const int *remaining, const TensorConsts<P, DIM> tc) {
+    const int n = *n_items;
+    const int64_t nb = *total;
+    for (int64_t vb = blockIdx.x; vb < nb; vb += gridDim.x) {
+        const int i = find_item(items, n, vb);
+        const int slot = items[i].slot;
+        __syncthreads();
+        if (remaining[slot] <= 0) continue;
+        tensor_stage_body<P, DIM, EPB>(items[i].io[parity[slot]], items[i].geo, tc, vb - items[i].block0);
+    }
+}
+
+template <typename KT, int NIN, int NFIN>
+__global__ void __launch_bounds__(SliceShape::THREADS, sizeof(KT) == 4 ? 5 : 4)
+    grouped_slice(const SliceItem<KT> *items, const int *n_items, const int64_t *total, const int *parity,
+                  const int *remaining, const SliceOps op) {
+    const int n = *n_items;
+    const int64_t nb = *total;
+    for (int64_t vb = blockIdx.x; vb < nb; vb += gridDim.x) {
+        const int i = find_item(items, n, vb);
+        const int slot = items[i].slot;
+        __syncthreads();
+        if (remaining[slot] <= 0) continue;
+        tensor_slice_body<KT, NIN, NFIN>(items[i].io[parity[slot]], items[i].geo, op, vb - items[i].block0);
+    }
+}
+
+// end of one step of every member: flip the current buffer, count the step
+__global__ void batch_advance(int *parity, int *remaining, int cap) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < cap && remaining[i] > 0) {
+        parity[i] ^= 1;
+        remaining[i] -= 1;
+    }
+}
+
+}  // namespace hgg
+
+namespace {
+
+enum BatchKind { KIND_DENSE = 0, KIND_TENSOR = 1, KIND_SLICE = 2 };
+
+struct BatchClass {
+    // key
+    int kind = 0, shape = 0, order = 0, dim = 0, physics = 0, S = 0;
+    bool mixed = false;
+    std::vector<double> rk_a, rk_b;
+    // members and launch shape
+    std::vector<int> slots;
+    int epb = 1;          // dense: elements per block
+    int ctas_per_sm = 2;  // persistent CTAs per SM
+    bool tuned = false;
+    int tuned_bucket = -1;
+    // device tables: items [S][cap] (one array per stage), count and block total
+    std::vector<void *> d_items;
+    size_t item_bytes = 0;
+    int *d_n = nullptr;
+    int64_t *d_total = nullptr;
+    int64_t total_blocks = 0;
+    int64_t total_elements = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done = nullptr;
+};
+
+struct TuneKey {
+    int kind, shape, order, physics, mixed, bucket;
+    bool operator<(const TuneKey &o) const {
+        return std::tie(kind, shape, order, physics, mixed, bucket) <
+               std::tie(o.kind, o.shape, o.order, o.physics, o.mixed, o.bucket);
+    }
+};
+struct TuneChoice {
+    int epb, ctas_per_sm;
+    float ms;
+};
+std::mutex g_tune_mutex;
+std::map<TuneKey, TuneChoice> g_tune_cache;
+
+thread_local std::string g_batch_create_error = "no error";
+
+}  // namespace
+
+struct hgg_batch {
+    int device = 0;
+    int cap = 0;
+    int num_sms = 148;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t fork = nullptr;
+    std::vector<hgg_handle *> handles;  // by slot, nullptr when free
+    std::vector<double> dt;
+    std::vector<int> base;               // the handle's current buffer when it was added
+    std::vector<int> cls;                // class index of each slot
+    std::vector<int> remaining_host;     // as last read back
+    std::vector<int> parity_host;
+    int *d_parity = nullptr, *d_remaining = nullptr, *d_status = nullptr;
+    std::vector<BatchClass> classes;
+    cudaGraphExec_t graph = nullptr;
+    bool dirty = true;
+    bool autotune = true;
+    int64_t launches = 0;
+    std::string err = "no error";
+};
+
+namespace {
+
+int bfail(hgg_batch *b, int code, const std::string &msg) {
+    if (b) b->err = msg;
+    else g_batch_create_error = msg;
+    return code;
+}
+
+#define HGG_BCUDA(b, call)                                                                    \
+    do {                                                                                      \
+        cudaError_t _e = (call);                                                              \
+        if (_e != cudaSuccess)                                                                \
+            return bfail(b, HGG_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(_e)); \
+    } while (0)
+
+int batch_kind(const hgg_handle *h) {
+    if (h->slice_ok) return KIND_SLICE;
+    if (h->op.tensor) return KIND_TENSOR;
+    return KIND_DENSE;
+}
+
+bool same_class(const BatchClass &c, const hgg_handle *h) {
+    return c.kind == batch_kind(h) && c.shape == h->op.shape && c.order == h->op.order && c.dim == h->op.dim &&
+           c.physics == h->op.physics && c.mixed == h->mixed && c.S == h->S && c.rk_a == h->rk_a &&
+           c.rk_b == h->rk_b;
+}
+
+int dense_R(const hgg_handle *h) { return h->op.V * h->op.nB; }
+
+int tensor_epb(int order, int dim) {
+    const int np = order + 1, nb = dim == 2 ? np * np : np * np * np;
+    return std::max(1, 256 / nb);
+}
+
+int64_t item_blocks(const BatchClass &c, const hgg_handle *h) {
+    const int64_t nE = h->op.nE;
+    if (c.kind == KIND_SLICE) return (nE + SliceShape::TE - 1) / SliceShape::TE;
+    if (c.kind == KIND_TENSOR) {
+        const int epb = tensor_epb(c.order, c.dim);
+        return (nE + epb - 1) / epb;
+    }
+    return (nE + c.epb - 1) / c.epb;
+}
+
+size_t class_item_bytes(const BatchClass &c) {
+    if (c.kind == KIND_DENSE) return sizeof(DenseItem);
+    if (c.kind == KIND_TENSOR) return sizeof(TensorItem);
+    return c.mixed ? sizeof(SliceItem<float>) : sizeof(SliceItem<double>);
+}
+
+DenseGeom dense_geom(const hgg_handle *h, int epb) {
+    const HostOperators &op = h->op;
+    return DenseGeom{h->d_vol, h->d_pairs, h->d_nbr, h->d_self, h->d_nbrp, h->d_mode,
+                     h->d_elem_geo, h->d_face_geo, 1.0 / op.c_inv, op.nB, epb};
+}
+
+// host copy of the items of one stage of a class
+template <typename KT>
+void fill_items(const hgg_batch *b, const BatchClass &c, int stage, std::vector<unsigned char> &buf) {
+    buf.assign(c.item_bytes * c.slots.size(), 0);
+    int64_t block0 = 0;
+    for (size_t m = 0; m < c.slots.size(); ++m) {
+        const int slot = c.slots[m];
+        const hgg_handle *h = b->handles[slot];
+        const int base = b->base[slot];
+        unsigned char *dst = buf.data() + m * c.item_bytes;
+        if (c.kind == KIND_DENSE) {
+            DenseItem it{};
+            for (int par = 0; par < 2; ++par)
+                it.io[par] = make_stage_io<double>(h, par ? 1 - base : base, b->dt[slot], stage, b->d_status);
+            it.g = dense_geom(h, c.epb);
+            it.block0 = block0;
+            it.slot = slot;
+            std::memcpy(dst, &it, sizeof(it));
+        } else if (c.kind == KIND_TENSOR) {
+            TensorItem it{};
+            for (int par = 0; par < 2; ++par)
+                it.io[par] = make_stage_io<double>(h, par ? 1 - base : base, b->dt[slot], stage, b->d_status);
+            it.geo = TensorGeom{h->d_ahat, h->d_tnbr, h->d_tmode, h->d_tsigma};
+            it.block0 = block0;
+            it.slot = slot;
+            std::memcpy(dst, &it, sizeof(it));
+        } else {
+            SliceItem<KT> it{};
+            for (int par = 0; par < 2; ++par)
+                it.io[par] = make_stage_io<KT>(h, par ? 1 - base : base, b->dt[slot], stage, b->d_status);
+            it.geo = h->d_slice_geo;
+            it.block0 = block0;
+            it.slot = slot;
+            std::memcpy(dst, &it, sizeof(it));
+        }
+        block0 += item_blocks(c, h);
+    }
+}
+
+int upload_class(hgg_batch *b, BatchClass &c) {
+    c.total_blocks = 0;
+    c.total_elements = 0;
+    for (int slot : c.slots) {
+        c.total_blocks += item_blocks(c, b->handles[slot]);
+        c.total_elements += b->handles[slot]->op.nE;
+    }
+    std::vector<unsigned char> buf;
+    for (int st = 0; st < c.S; ++st) {
+        if (c.mixed) fill_items<float>(b, c, st, buf);
+        else fill_items<double>(b, c, st, buf);
+        if (!buf.empty())
+            HGG_BCUDA(b, cudaMemcpyAsync(c.d_items[st], buf.data(), buf.size(), cudaMemcpyHostToDevice, b->stream));
+    }
+    const int n = (int)c.slots.size();
+    HGG_BCUDA(b, cudaMemcpyAsync(c.d_n, &n, sizeof(int), cudaMemcpyHostToDevice, b->stream));
+    HGG_BCUDA(b, cudaMemcpyAsync(c.d_total, &c.total_blocks, sizeof(int64_t), cudaMemcpyHostToDevice, b->stream));
+    // the host buffers above are reused: wait for the copies
+    HGG_BCUDA(b, cudaStreamSynchronize(b->stream));
+    return 0;
+}
+
+template <int DIM, int NFL, int WAVE>
+void launch_grouped_dense(const hgg_batch *b, const BatchClass &c, int st, unsigned grid, cudaStream_t s) {
+    const int R = (WAVE ? DIM + 1 : 1) * b->handles[c.slots[0]]->op.nB;
+    const int threads = ((c.epb * R + 31) / 32) * 32;
+    const size_t smem = sizeof(double) * (size_t)c.epb * R * (1 + NFL);
+    if (smem > 48 * 1024)
+        cudaFuncSetAttribute(grouped_dense<DIM, NFL, WAVE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    grouped_dense<DIM, NFL, WAVE><<<grid, threads, smem, s>>>(static_cast<const DenseItem *>(c.d_items[st]), c.d_n,
+                                                             c.d_total, b->d_parity, b->d_remaining);
+}
+
+template <int P, int DIM>
+void launch_grouped_tensor(const hgg_batch *b, const BatchClass &c, int st, unsigned grid, cudaStream_t s) {
+    constexpr int NB = TensorConsts<P, DIM>::NB;
+    constexpr int EPB = (256 / NB) > 0 ? (256 / NB) : 1;
+    const TensorConsts<P, DIM> tc = tensor_consts<P, DIM>(b->handles[c.slots[0]]->op);
+    grouped_tensor<P, DIM, EPB><<<grid, EPB * NB, 0, s>>>(static_cast<const TensorItem *>(c.d_items[st]), c.d_n,
+                                                         c.d_total, b->d_parity, b->d_remaining, tc);
+}
+
+template <typename KT>
+void launch_grouped_slice(const hgg_batch *b, const BatchClass &c, int st, unsigned grid, cudaStream_t s) {
+    const hgg_handle *h = b->handles[c.slots[0]];
+    SliceOps sops;
+    for (int i = 0; i < 16; ++i) sops.D[i] = h->op.D1[i];
+    for (int sd = 0; sd < 2; ++sd)
+        for (int a = 0; a < 4; ++a) sops.L[sd][a] = h->op.lift[sd * 4 + a];
+    // the stage's shape is the same for every member (same tableau): take it from the first
+    const StageIOT<KT> io = make_stage_io<KT>(h, 0, 1.0, st, nullptr);
+    const bool fin = io.unew != nullptr;
+    const auto *items = static_cast<const SliceItem<KT> *>(c.d_items[st]);
+    const dim3 g(grid), blk(SliceShape::THREADS);
+    if (io.nin == 0 && (!fin || io.nfin == 0))
+        grouped_slice<KT, 0, 0><<<g, blk, 0, s>>>(items, c.d_n, c.d_total, b->d_parity, b->d_remaining, sops);
+    else if (io.nin == 1 && (!fin || io.nfin == 0))
+        grouped_slice<KT, 1, 0><<<g, blk, 0, s>>>(items, c.d_n, c.d_total, b->d_parity, b->d_remaining, sops);
+    else if (io.nin == 1 && fin && io.nfin == 3)
+        grouped_slice<KT, 1, 3><<<g, blk, 0, s>>>(items, c.d_n, c.d_total, b->d_parity, b->d_remaining, sops);
+    else
+        grouped_slice<KT, -1, -1><<<g, blk, 0, s>>>(items, c.d_n, c.d_total, b->d_parity, b->d_remaining, sops);
+}
+
+// one stage of one class
+void launch_class_stage(hgg_batch *b, const BatchClass &c, int st, cudaStream_t s) {
+    const unsigned grid = (unsigned)std::max<int64_t>(
+        1, std::min<int64_t>(c.total_blocks, (int64_t)c.ctas_per_sm * b->num_sms));
+    if (c.kind == KIND_SLICE) {
+        if (c.mixed) launch_grouped_slice<float>(b, c, st, grid, s);
+        else launch_grouped_slice<double>(b, c, st, grid, s);
+    } else if (c.kind == KIND_TENSOR) {
+#define HGG_GT(P)                                                  \
+    case P:                                                        \
+        if (c.dim == 2) launch_grouped_tensor<P, 2>(b, c, st, grid, s); \
+        else launch_grouped_tensor<P, 3>(b, c, st, grid, s);            \
+        break;
+        switch (c.order) { HGG_GT(1) HGG_GT(2) HGG_GT(3) HGG_GT(4) HGG_GT(5) }
+#undef HGG_GT
+    } else {
+        const bool wave = c.physics == HGG_PHYSICS_WAVE;
+        switch (c.shape) {
+            case HGG_SHAPE_LINE: wave ? launch_grouped_dense<1, 2, 1>(b, c, st, grid, s) : launch_grouped_dense<1, 2, 0>(b, c, st, grid, s); break;
+            case HGG_SHAPE_TRIANGLE: wave ? launch_grouped_dense<2, 3, 1>(b, c, st, grid, s) : launch_grouped_dense<2, 3, 0>(b, c, st, grid, s); break;
+            case HGG_SHAPE_SQUARE: wave ? launch_grouped_dense<2, 4, 1>(b, c, st, grid, s) : launch_grouped_dense<2, 4, 0>(b, c, st, grid, s); break;
+            case HGG_SHAPE_TETRAHEDRON: wave ? launch_grouped_dense<3, 4, 1>(b, c, st, grid, s) : launch_grouped_dense<3, 4, 0>(b, c, st, grid, s); break;
+            case HGG_SHAPE_CUBE: wave ? launch_grouped_dense<3, 6, 1>(b, c, st, grid, s) : launch_grouped_dense<3, 6, 0>(b, c, st, grid, s); break;
+        }
+    }
+    b->launches++;
+}
+
+int size_bucket(int64_t elements) {
+    int k = 0;
+    while (elements > 1 && k < 40) {
+        elements >>= 1;
+        ++k;
+    }
+    return k;
+}
+
+// Time the candidate launch shapes of a class on its members (stage 1, which
+// writes only the first stage vector) and keep the fastest.
+int tune_class(hgg_batch *b, BatchClass &c) {
+    const TuneKey key{c.kind, c.shape, c.order, c.physics, (int)c.mixed, size_bucket(c.total_elements)};
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) {
+            const bool same_epb = c.epb == it->second.epb;
+            c.epb = it->second.epb;
+            c.ctas_per_sm = it->second.ctas_per_sm;
+            c.tuned = true;
+            c.tuned_bucket = key.bucket;
+            if (!same_epb) return upload_class(b, c);  // dense block counts depend on epb
+            return 0;
+        }
+    }
+    std::vector<std::pair<int, int>> cands;  // (epb, ctas_per_sm)
+    const int ctas[] = {1, 2, 4, 8};
+    if (c.kind == KIND_DENSE) {
+        const int R = dense_R(b->handles[c.slots[0]]);
+        const int nfl = c.shape == HGG_SHAPE_LINE ? 2 : (c.shape == HGG_SHAPE_TRIANGLE ? 3
+                        : (c.shape == HGG_SHAPE_SQUARE || c.shape == HGG_SHAPE_TETRAHEDRON ? 4 : 6));
+        for (int epb : {1, 2, 4, 8, 16, 32}) {
+            if (epb * R > 256 || sizeof(double) * (size_t)epb * R * (1 + nfl) > 200 * 1024) continue;
+            for (int cs : ctas) cands.push_back({epb, cs});
+        }
+    } else {
+        for (int cs : ctas) cands.push_back({c.epb, cs});
+    }
+    if (cands.empty()) return bfail(b, HGG_ERR_UNSUPPORTED, "batch: no launch shape fits this class");
+    // the remaining counters must read positive for every member while timing
+    cudaEvent_t e0, e1;
+    HGG_BCUDA(b, cudaEventCreate(&e0));
+    HGG_BCUDA(b, cudaEventCreate(&e1));
+    TuneChoice best{c.epb, c.ctas_per_sm, 1e30f};
+    for (auto [epb, cs] : cands) {
+        if (epb != c.epb) {
+            c.epb = epb;
+            int rc = upload_class(b, c);
+            if (rc) return rc;
+        }
+        c.ctas_per_sm = cs;
+        float tmin = 1e30f;
+        for (int rep = 0; rep < 3; ++rep) {
+            cudaEventRecord(e0, b->stream);
+            launch_class_stage(b, c, 0, b->stream);
+            cudaEventRecord(e1, b->stream);
+            HGG_BCUDA(b, cudaEventSynchronize(e1));
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            tmin = std::min(tmin, ms);
+        }
+        HGG_BCUDA(b, cudaGetLastError());
+        if (tmin < best.ms) best = TuneChoice{epb, cs, tmin};
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (c.epb != best.epb) {
+        c.epb = best.epb;
+        int rc = upload_class(b, c);
+        if (rc) return rc;
+    }
+    c.ctas_per_sm = best.ctas_per_sm;
+    c.tuned = true;
+    c.tuned_bucket = key.bucket;
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    g_tune_cache[key] = best;
+    return 0;
+}
+
+// read parity and remaining counters back (after the stream is idle)
+int read_counters(hgg_batch *b) {
+    HGG_BCUDA(b, cudaMemcpyAsync(b->parity_host.data(), b->d_parity, sizeof(int) * b->cap, cudaMemcpyDeviceToHost,
+                                 b->stream));
+    HGG_BCUDA(b, cudaMemcpyAsync(b->remaining_host.data(), b->d_remaining, sizeof(int) * b->cap,
+                                 cudaMemcpyDeviceToHost, b->stream));
+    HGG_BCUDA(b, cudaStreamSynchronize(b->stream));
+    return 0;
+}
+
+void release_batch_graph(hgg_batch *b) {
+    if (b->graph) {
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+    }
+}
+
+// tables of every class, autotuning of untuned classes, capture of one step
+int prepare_batch(hgg_batch *b) {
+    if (!b->dirty && b->graph) return 0;
+    release_batch_graph(b);
+    // current counters (tuning below overwrites them for a moment)
+    int rc0 = read_counters(b);
+    if (rc0) return rc0;
+    for (auto &c : b->classes) {
+        if (c.slots.empty()) continue;
+        int rc = upload_class(b, c);
+        if (rc) return rc;
+        // tuning launches stage 1 of the members (every member must have steps left for it
+        // to run); a one-stage tableau's first stage is its final update, so it is not tuned
+        if (b->autotune && c.S > 1 && (!c.tuned || c.tuned_bucket != size_bucket(c.total_elements))) {
+            std::vector<int> ones(b->cap, 1);
+            HGG_BCUDA(b, cudaMemcpyAsync(b->d_remaining, ones.data(), sizeof(int) * b->cap, cudaMemcpyHostToDevice,
+                                         b->stream));
+            rc = tune_class(b, c);
+            if (rc) return rc;
+            HGG_BCUDA(b, cudaMemcpyAsync(b->d_remaining, b->remaining_host.data(), sizeof(int) * b->cap,
+                                         cudaMemcpyHostToDevice, b->stream));
+            HGG_BCUDA(b, cudaStreamSynchronize(b->stream));
+        }
+    }
+    cudaGraph_t g = nullptr;
+    HGG_BCUDA(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    const int64_t before = b->launches;
+    cudaEventRecord(b->fork, b->stream);
+    for (auto &c : b->classes) {
+        if (c.slots.empty()) continue;
+        cudaStreamWaitEvent(c.stream, b->fork, 0);
+        for (int st = 0; st < c.S; ++st) launch_class_stage(b, c, st, c.stream);
+        cudaEventRecord(c.done, c.stream);
+        cudaStreamWaitEvent(b->stream, c.done, 0);
+    }
+    batch_advance<<<(b->cap + 255) / 256, 256, 0, b->stream>>>(b->d_parity, b->d_remaining, b->cap);
+    cudaError_t ce = cudaStreamEndCapture(b->stream, &g);
+    b->launches = before;
+    if (ce != cudaSuccess) return bfail(b, HGG_ERR_CUDA, std::string("batch graph capture: ") + cudaGetErrorString(ce));
+    cudaError_t ie = cudaGraphInstantiate(&b->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (ie != cudaSuccess) return bfail(b, HGG_ERR_CUDA, std::string("batch graph instantiate: ") + cudaGetErrorString(ie));
+    b->dirty = false;
+    return 0;
+}
+
+int launches_per_step(const hgg_batch *b) {
+    int n = 1;
+    for (auto &c : b->classes)
+        if (!c.slots.empty()) n += c.S;
+    return n;
+}
+
+void destroy_batch(hgg_batch *b) {
+    if (!b) return;
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    release_batch_graph(b);
+    for (auto &c : b->classes) {
+        if (c.stream) cudaStreamSynchronize(c.stream);
+        for (void *p : c.d_items) cudaFree(p);
+        cudaFree(c.d_n);
+        cudaFree(c.d_total);
+        if (c.done) cudaEventDestroy(c.done);
+        if (c.stream) cudaStreamDestroy(c.stream);
+    }
+    cudaFree(b->d_parity);
+    cudaFree(b->d_remaining);
+    cudaFree(b->d_status);
+    if (b->fork) cudaEventDestroy(b->fork);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+}
+
+}  // namespace
+
+extern "C" {
+
+int hgg_batch_create(int32_t capacity, hgg_batch **out) {
+    if (!out || capacity < 1 || capacity > (1 << 20)) return bfail(nullptr, HGG_ERR_INVALID, "capacity must be 1..2^20");
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return bfail(nullptr, HGG_ERR_NOT_LOADED, "no CUDA device available");
+    auto *b = new hgg_batch();
+    b->cap = capacity;
+    b->handles.assign(capacity, nullptr);
+    b->dt.assign(capacity, 0.0);
+    b->base.assign(capacity, 0);
+    b->cls.assign(capacity, -1);
+    b->remaining_host.assign(capacity, 0);
+    b->parity_host.assign(capacity, 0);
+    auto fail_create = [&](cudaError_t e, const char *what) {
+        g_batch_create_error = std::string(what) + ": " + cudaGetErrorString(e);
+        destroy_batch(b);
+        return HGG_ERR_CUDA;
+    };
+    cudaError_t e;
+    if ((e = cudaGetDevice(&b->device)) != cudaSuccess) return fail_create(e, "cudaGetDevice");
+    if ((e = cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, b->device)) != cudaSuccess)
+        return fail_create(e, "cudaDeviceGetAttribute");
+    if ((e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking)) != cudaSuccess)
+        return fail_create(e, "cudaStreamCreateWithFlags");
+    if ((e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming)) != cudaSuccess)
+        return fail_create(e, "cudaEventCreate");
+    if ((e = cudaMalloc(&b->d_parity, sizeof(int) * capacity)) != cudaSuccess) return fail_create(e, "cudaMalloc");
+    if ((e = cudaMalloc(&b->d_remaining, sizeof(int) * capacity)) != cudaSuccess) return fail_create(e, "cudaMalloc");
+    if ((e = cudaMalloc(&b->d_status, sizeof(int))) != cudaSuccess) return fail_create(e, "cudaMalloc");
+    cudaMemsetAsync(b->d_parity, 0, sizeof(int) * capacity, b->stream);
+    cudaMemsetAsync(b->d_remaining, 0, sizeof(int) * capacity, b->stream);
+    cudaMemsetAsync(b->d_status, 0, sizeof(int), b->stream);
+    if ((e = cudaStreamSynchronize(b->stream)) != cudaSuccess) return fail_create(e, "cudaStreamSynchronize");
+    *out = b;
+    return 0;
+}
+
+int hgg_batch_destroy(hgg_batch *b) {
+    destroy_batch(b);
+    return 0;
+}
+
+const char *hgg_batch_last_error(const hgg_batch *b) { return b ? b->err.c_str() : g_batch_create_error.c_str(); }
+
+int hgg_batch_add(hgg_batch *b, hgg_handle *h, double dt, int32_t nsteps, int32_t *slot) {
+    if (!b || !h || !slot) return bfail(b, HGG_ERR_INVALID, "null argument");
+    if (nsteps < 0 || !(dt > 0.0)) return bfail(b, HGG_ERR_INVALID, "dt must be positive and nsteps >= 0");
+    if (h->device != b->device) return bfail(b, HGG_ERR_INVALID, "handle and batch are on different devices");
+    int free_slot = -1;
+    for (int i = 0; i < b->cap; ++i) {
+        if (b->handles[i] == h) return bfail(b, HGG_ERR_INVALID, "handle is already in the batch");
+        if (free_slot < 0 && !b->handles[i]) free_slot = i;
+    }
+    if (free_slot < 0) return bfail(b, HGG_ERR_INVALID, "batch is full");
+    if (!h->slice_ok && !h->op.tensor && dense_R(h) > 256)
+        return bfail(b, HGG_ERR_UNSUPPORTED, "dense kernel: more than 256 coefficients per element");
+    // the handle's own work must be finished before the batch uses its buffers
+    HGG_BCUDA(b, cudaStreamSynchronize(h->stream));
+    int ci = -1;
+    for (size_t i = 0; i < b->classes.size(); ++i)
+        if (same_class(b->classes[i], h)) ci = (int)i;
+    if (ci < 0) {
+        BatchClass c;
+        c.kind = batch_kind(h);
+        c.shape = h->op.shape;
+        c.order = h->op.order;
+        c.dim = h->op.dim;
+        c.physics = h->op.physics;
+        c.mixed = h->mixed;
+        c.S = h->S;
+        c.rk_a = h->rk_a;
+        c.rk_b = h->rk_b;
+        c.epb = c.kind == KIND_DENSE ? std::max(1, 256 / dense_R(h)) : 1;
+        c.item_bytes = class_item_bytes(c);
+        c.d_items.assign(c.S, nullptr);
+        for (int st = 0; st < c.S; ++st)
+            HGG_BCUDA(b, cudaMalloc(&c.d_items[st], c.item_bytes * (size_t)b->cap));
+        HGG_BCUDA(b, cudaMalloc(&c.d_n, sizeof(int)));
+        HGG_BCUDA(b, cudaMalloc(&c.d_total, sizeof(int64_t)));
+        HGG_BCUDA(b, cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
+        HGG_BCUDA(b, cudaEventCreateWithFlags(&c.done, cudaEventDisableTiming));
+        b->classes.push_back(std::move(c));
+        ci = (int)b->classes.size() - 1;
+    }
+    b->classes[ci].slots.push_back(free_slot);
+    b->handles[free_slot] = h;
+    b->dt[free_slot] = dt;
+    b->base[free_slot] = h->cur;
+    b->cls[free_slot] = ci;
+    b->remaining_host[free_slot] = nsteps;
+    b->parity_host[free_slot] = 0;
+    const int zero = 0;
+    HGG_BCUDA(b, cudaMemcpyAsync(b->d_parity + free_slot, &zero, sizeof(int), cudaMemcpyHostToDevice, b->stream));
+    HGG_BCUDA(b, cudaMemcpyAsync(b->d_remaining + free_slot, &b->remaining_host[free_slot], sizeof(int),
+                                 cudaMemcpyHostToDevice, b->stream));
+    HGG_BCUDA(b, cudaStreamSynchronize(b->stream));
+    b->dirty = true;
+    *slot = free_slot;
+    return 0;
+}
+
+int hgg_batch_remove(hgg_batch *b, int32_t slot) {
+    if (!b || slot < 0 || slot >= b->cap || !b->handles[slot]) return bfail(b, HGG_ERR_INVALID, "bad slot");
+    int rc = read_counters(b);
+    if (rc) return rc;
+    hgg_handle *h = b->handles[slot];
+    h->cur = b->parity_host[slot] ? 1 - b->base[slot] : b->base[slot];
+    BatchClass &c = b->classes[b->cls[slot]];
+    c.slots.erase(std::find(c.slots.begin(), c.slots.end(), slot));
+    b->handles[slot] = nullptr;
+    b->cls[slot] = -1;
+    b->remaining_host[slot] = 0;
+    const int zero = 0;
+    HGG_BCUDA(b, cudaMemcpyAsync(b->d_remaining + slot, &zero, sizeof(int), cudaMemcpyHostToDevice, b->stream));
+    HGG_BCUDA(b, cudaStreamSynchronize(b->stream));
+    b->dirty = true;
+    return 0;
+}
+
+int hgg_batch_step(hgg_batch *b, int32_t nsteps) {
+    if (!b || nsteps < 0) return bfail(b, HGG_ERR_INVALID, "bad argument");
+    if (nsteps == 0) return 0;
+    bool any = false;
+    for (auto &c : b->classes) any = any || !c.slots.empty();
+    if (!any) return 0;
+    int rc = prepare_batch(b);
+    if (rc) return rc;
+    for (int s = 0; s < nsteps; ++s) HGG_BCUDA(b, cudaGraphLaunch(b->graph, b->stream));
+    b->launches += (int64_t)nsteps * launches_per_step(b);
+    return 0;
+}
+
+int hgg_batch_synchronize(hgg_batch *b) {
+    if (!b) return bfail(b, HGG_ERR_INVALID, "null batch");
+    int rc = read_counters(b);
+    if (rc) return rc;
+    int st = 0;
+    HGG_BCUDA(b, cudaMemcpyAsync(&st, b->d_status, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+    HGG_BCUDA(b, cudaStreamSynchronize(b->stream));
+    if (st) return bfail(b, HGG_ERR_DEVICE, "kernel status word " + std::to_string(st) + " (bad neighbour index)");
+    // keep each member handle's notion of its current buffer up to date
+    for (int i = 0; i < b->cap; ++i)
+        if (b->handles[i]) b->handles[i]->cur = b->parity_host[i] ? 1 - b->base[i] : b->base[i];
+    return 0;
+}
+
+int32_t hgg_batch_remaining(const hgg_batch *b, int32_t slot) {
+    if (!b || slot < 0 || slot >= b->cap || !b->handles[slot]) return -1;
+    return b->remaining_host[slot];
+}
+
+int hgg_batch_set_autotune(hgg_batch *b, int32_t enable) {
+    if (!b) return bfail(b, HGG_ERR_INVALID, "null batch");
+    b->autotune = enable != 0;
+    return 0;
+}
+
+int64_t hgg_batch_launch_count(const hgg_batch *b) { return b ? b->launches : -1; }
+
+int32_t hgg_batch_num_classes(const hgg_batch *b) {
+    if (!b) return -1;
+    int n = 0;
+    for (auto &c : b->classes) n += !c.slots.empty();
+    return n;
+}
+
+}  // extern "C"

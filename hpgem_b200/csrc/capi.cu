@@ -337,41 +337,46 @@ void *vector_ptr(hgg_handle *h, int vec) {
 }
 bool vector_is_float(const hgg_handle *h, int vec) { return h->mixed && vec >= 1; }
 
-// One Runge-Kutta step from sol[from] into sol[1 - from] (stages as in
-// HpgemAPISimplified_Impl.h:788-820; zero tableau entries are skipped).
+// Inputs and outputs of stage i of one Runge-Kutta step from sol[from] into
+// sol[1 - from] (stages as in HpgemAPISimplified_Impl.h:788-820; zero tableau
+// entries are skipped).
+template <typename KT>
+StageIOT<KT> make_stage_io(const hgg_handle *h, int from, double dt, int i, int *status) {
+    const int S = h->S;
+    auto kv = [&](int j) { return static_cast<KT *>(h->k[j]); };
+    StageIOT<KT> io{};
+    io.u = h->sol[from];
+    io.n_elements = h->op.nE;
+    io.status = status;
+    for (int j = 0; j < i; ++j) {
+        double c = dt * h->rk_a[i * S + j];
+        if (c != 0.0) {
+            io.kin[io.nin] = kv(j);
+            io.cin[io.nin] = c;
+            io.nin++;
+        }
+    }
+    const bool last = i == S - 1;
+    io.kout = (!last || h->store_last) ? kv(i) : nullptr;
+    if (last) {
+        io.unew = h->sol[1 - from];
+        for (int j = 0; j < S - 1; ++j) {
+            double b = dt * h->rk_b[j];
+            if (b != 0.0) {
+                io.kfin[io.nfin] = kv(j);
+                io.bfin[io.nfin] = b;
+                io.nfin++;
+            }
+        }
+        io.blast = dt * h->rk_b[S - 1];
+    }
+    return io;
+}
+
 template <typename KT>
 int enqueue_step_t(hgg_handle *h, int from, double dt) {
-    const int S = h->S;
-    const double *u = h->sol[from];
-    auto kv = [&](int j) { return static_cast<KT *>(h->k[j]); };
-    for (int i = 0; i < S; ++i) {
-        StageIOT<KT> io{};
-        io.u = u;
-        io.n_elements = h->op.nE;
-        io.status = h->d_status;
-        for (int j = 0; j < i; ++j) {
-            double c = dt * h->rk_a[i * S + j];
-            if (c != 0.0) {
-                io.kin[io.nin] = kv(j);
-                io.cin[io.nin] = c;
-                io.nin++;
-            }
-        }
-        const bool last = i == S - 1;
-        io.kout = (!last || h->store_last) ? kv(i) : nullptr;
-        if (last) {
-            io.unew = h->sol[1 - from];
-            for (int j = 0; j < S - 1; ++j) {
-                double b = dt * h->rk_b[j];
-                if (b != 0.0) {
-                    io.kfin[io.nfin] = kv(j);
-                    io.bfin[io.nfin] = b;
-                    io.nfin++;
-                }
-            }
-            io.blast = dt * h->rk_b[S - 1];
-        }
-        int rc = launch_stage(h, io);
+    for (int i = 0; i < h->S; ++i) {
+        int rc = launch_stage(h, make_stage_io<KT>(h, from, dt, i, h->d_status));
         if (rc) return rc;
     }
     return 0;
@@ -900,3 +905,6 @@ int hgg_l2_error(hgg_handle *h, int32_t vec, const double *exact, double *error)
 }
 
 }  // extern "C"
+
+// grouped execution of many problems (hgg_batch_*)
+#include "batch_exec.cuh"

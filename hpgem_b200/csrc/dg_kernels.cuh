@@ -87,9 +87,12 @@ struct TensorGeom {
     const double *sigma;   // [E][2*DIM]
 };
 
+// One block's work: elements [block * EPB, block * EPB + EPB).  Called by the
+// one-shot launch (block = blockIdx.x) and by the grouped launch of many
+// problems (block = the block's index inside its problem).
 template <int P, int DIM, int EPB>
-__global__ void __launch_bounds__(EPB *TensorConsts<P, DIM>::NB)
-    tensor_stage(const StageIO io, const TensorGeom geo, const TensorConsts<P, DIM> tc) {
+__device__ __forceinline__ void tensor_stage_body(const StageIO &io, const TensorGeom &geo,
+                                                  const TensorConsts<P, DIM> &tc, int64_t block) {
     using TC = TensorConsts<P, DIM>;
     constexpr int NP = TC::NP, NB = TC::NB, NF = TC::NF, NS = TC::NS;
     __shared__ double W[EPB][NB];
@@ -111,7 +114,7 @@ __global__ void __launch_bounds__(EPB *TensorConsts<P, DIM>::NB)
 
     const int el = tid / NB;
     const int t = tid % NB;  // hpGEM basis index of this thread's DoF
-    const int64_t e0 = (int64_t)blockIdx.x * EPB;
+    const int64_t e0 = block * EPB;
     const int64_t e = e0 + el;
     const bool active = e < io.n_elements;
 
@@ -197,6 +200,12 @@ __global__ void __launch_bounds__(EPB *TensorConsts<P, DIM>::NB)
     stage_output(io, e * NB + t, u_own, ssign[t] * acc);
 }
 
+template <int P, int DIM, int EPB>
+__global__ void __launch_bounds__(EPB *TensorConsts<P, DIM>::NB)
+    tensor_stage(const StageIO io, const TensorGeom geo, const TensorConsts<P, DIM> tc) {
+    tensor_stage_body<P, DIM, EPB>(io, geo, tc, blockIdx.x);
+}
+
 // ---------------------------------------------------------------------------
 // dense reference operators, any shape and physics
 // ---------------------------------------------------------------------------
@@ -214,15 +223,16 @@ struct DenseGeom {
     int epb;                   // elements per block
 };
 
+// One block's work: elements [block * epb, block * epb + epb) (see tensor_stage_body).
 template <int DIM, int NFL, int WAVE>
-__global__ void __launch_bounds__(256) dense_stage(const StageIO io, const DenseGeom g) {
+__device__ __forceinline__ void dense_stage_body(const StageIO &io, const DenseGeom &g, int64_t block) {
     constexpr int V = WAVE ? DIM + 1 : 1;
     extern __shared__ double smem[];
     const int nB = g.nB, R = V * nB, epb = g.epb;
     double *W = smem;                        // [epb][R]
     double *WN = smem + (size_t)epb * R;     // [epb][NFL][R]
     const int tid = threadIdx.x;
-    const int64_t e0 = (int64_t)blockIdx.x * epb;
+    const int64_t e0 = block * epb;
 
     const int el = tid / R, r = tid % R;
     const int64_t e = e0 + el;
@@ -325,6 +335,11 @@ __global__ void __launch_bounds__(256) dense_stage(const StageIO io, const Dense
         }
     }
     stage_output(io, e * R + r, u_own, acc);
+}
+
+template <int DIM, int NFL, int WAVE>
+__global__ void __launch_bounds__(256) dense_stage(const StageIO io, const DenseGeom g) {
+    dense_stage_body<DIM, NFL, WAVE>(io, g, blockIdx.x);
 }
 
 }  // namespace hgg

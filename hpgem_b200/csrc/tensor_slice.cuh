@@ -84,8 +84,8 @@ __device__ __forceinline__ CT slice_flux(int md, CT sg, CT self, CT nbr) {
 // load loop unrolls and all loads of a phase are in flight together), or -1
 // for a count read from io.
 template <typename KT, int NIN, int NFIN>
-__global__ void __launch_bounds__(SliceShape::THREADS, sizeof(KT) == 4 ? 5 : 4)
-    tensor_slice(const StageIOT<KT> io, const double *__restrict__ geo, const SliceOps op) {
+__device__ __forceinline__ void tensor_slice_body(const StageIOT<KT> &io, const double *__restrict__ geo,
+                                                  const SliceOps &op, int64_t tile) {
     using CT = KT;  // contraction type
     constexpr int TE = SliceShape::TE, WS = SliceShape::WS, ZS = SliceShape::ZS, GR = SliceShape::GR;
     constexpr int TILE = SliceShape::TILE;
@@ -96,11 +96,11 @@ __global__ void __launch_bounds__(SliceShape::THREADS, sizeof(KT) == 4 ? 5 : 4)
 
     const int el = threadIdx.x & 31;
     const int c = threadIdx.x >> 5;  // z-slice, uniform in the warp
-    const int64_t t0 = (int64_t)blockIdx.x * TE;
+    const int64_t t0 = tile * TE;
     const int64_t e = t0 + el;
     const bool active = e < io.n_elements;
     // own coefficient j of this element: base + 32 j (padding lanes read their own zero slots)
-    const int64_t base = (int64_t)blockIdx.x * TILE + el;
+    const int64_t base = tile * TILE + el;
     const int nin = NIN >= 0 ? NIN : io.nin;
     const int nfin = NFIN >= 0 ? NFIN : io.nfin;
 
@@ -244,6 +244,13 @@ __global__ void __launch_bounds__(SliceShape::THREADS, sizeof(KT) == 4 ? 5 : 4)
             if (io.unew) io.unew[off] = fu[i] + io.blast * (double)r;
         }
     }
+}
+
+// One block per 32-element tile of one problem.
+template <typename KT, int NIN, int NFIN>
+__global__ void __launch_bounds__(SliceShape::THREADS, sizeof(KT) == 4 ? 5 : 4)
+    tensor_slice(const StageIOT<KT> io, const double *__restrict__ geo, const SliceOps op) {
+    tensor_slice_body<KT, NIN, NFIN>(io, geo, op, blockIdx.x);
 }
 
 }  // namespace hgg

@@ -235,6 +235,51 @@ int32_t hgg_num_error_points(const hgg_handle *h);
 int hgg_error_points(const hgg_handle *h, double *xyz);
 int hgg_l2_error(hgg_handle *h, int32_t vec, const double *exact, double *error);
 
+/* ---- many problems at once ------------------------------------------------
+ * No counterpart in the reference (hpGEM advances one mesh per process).  A
+ * batch advances many independent problems, each an existing handle with its
+ * own mesh, order, physics, dt and step count, together: every RK stage of all
+ * members of one kernel class (organisation, shape, order, physics,
+ * precision, tableau) is one persistent launch over all their element blocks,
+ * the classes of a step run as parallel branches of one CUDA graph, and each
+ * problem stops at exactly its own step count.  Launch shapes per class are
+ * picked by timing candidates on the members (autotuner, cached per class and
+ * size for the process).  A handle in a batch must not be stepped, read or
+ * destroyed through its own entry points until hgg_batch_synchronize (read)
+ * or hgg_batch_remove (anything) has returned. */
+typedef struct hgg_batch hgg_batch;
+
+/* A batch with room for `capacity` problems on the current device. */
+int hgg_batch_create(int32_t capacity, hgg_batch **out);
+int hgg_batch_destroy(hgg_batch *b);
+const char *hgg_batch_last_error(const hgg_batch *b);
+
+/* Adds handle h, to advance `nsteps` steps of `dt` from its current solution;
+ * *slot receives its slot number. */
+int hgg_batch_add(hgg_batch *b, hgg_handle *h, double dt, int32_t nsteps, int32_t *slot);
+
+/* Takes the problem out of the batch (waits for the batch's work); the handle's
+ * solution is then its state after the steps it took. */
+int hgg_batch_remove(hgg_batch *b, int32_t slot);
+
+/* Enqueues nsteps steps of every member that still has steps to take (asynchronous). */
+int hgg_batch_step(hgg_batch *b, int32_t nsteps);
+
+/* Waits for the batch, reads every member's remaining step count and the
+ * device status word (HGG_ERR_DEVICE on a bad neighbour index). */
+int hgg_batch_synchronize(hgg_batch *b);
+
+/* Steps the member in `slot` still has to take, as of the last synchronize;
+ * -1 for an empty slot. */
+int32_t hgg_batch_remaining(const hgg_batch *b, int32_t slot);
+
+/* 1 (default): time candidate launch shapes per kernel class; 0: fixed defaults. */
+int hgg_batch_set_autotune(hgg_batch *b, int32_t enable);
+
+/* Kernel launches the batch enqueued so far; kernel classes with members. */
+int64_t hgg_batch_launch_count(const hgg_batch *b);
+int32_t hgg_batch_num_classes(const hgg_batch *b);
+
 #ifdef __cplusplus
 }
 #endif
