@@ -7,8 +7,9 @@ Build it with ``python -m hpgem_b200.build``.
 """
 from ._native import NativeError, ProblemDesc, load  # noqa: F401
 from .batch import Batch  # noqa: F401
+from .server import Server  # noqa: F401
 from .solver import (AcousticWave, Advection, Handle, HpgemAPISimplified,  # noqa: F401
                      structured_description)
 
-__all__ = ["AcousticWave", "Advection", "Batch", "Handle", "HpgemAPISimplified", "NativeError",
+__all__ = ["AcousticWave", "Advection", "Batch", "Handle", "Server", "HpgemAPISimplified", "NativeError",
            "ProblemDesc", "load", "structured_description"]

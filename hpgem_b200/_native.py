@@ -27,7 +27,14 @@ EXPORTED = ["hgg_create", "hgg_destroy", "hgg_last_error", "hgg_set_state", "hgg
             "hgg_time_derivative_static",
             "hgg_batch_create", "hgg_batch_destroy", "hgg_batch_last_error", "hgg_batch_add",
             "hgg_batch_remove", "hgg_batch_step", "hgg_batch_synchronize", "hgg_batch_remaining",
-            "hgg_batch_set_autotune", "hgg_batch_launch_count", "hgg_batch_num_classes"]
+            "hgg_batch_set_autotune", "hgg_batch_launch_count", "hgg_batch_num_classes",
+            "hgg_server_start", "hgg_server_submit", "hgg_server_poll", "hgg_server_result_length",
+            "hgg_server_release", "hgg_server_times", "hgg_server_stats", "hgg_server_last_error",
+            "hgg_server_stop"]
+
+# void (*hgg_initial_fn)(const double *xyz, int64_t n_points, int32_t dim, double *values, void *user)
+INITIAL_FN = ctypes.CFUNCTYPE(None, ctypes.POINTER(ctypes.c_double), ctypes.c_int64, ctypes.c_int32,
+                              ctypes.POINTER(ctypes.c_double), ctypes.c_void_p)
 
 
 class ProblemDesc(ctypes.Structure):
@@ -91,6 +98,19 @@ def load():
         "hgg_batch_set_autotune": (ctypes.c_int, [B, ctypes.c_int32]),
         "hgg_batch_launch_count": (ctypes.c_int64, [B]),
         "hgg_batch_num_classes": (ctypes.c_int32, [B]),
+        "hgg_server_start": (ctypes.c_int, [ctypes.c_int64, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                            ctypes.POINTER(ctypes.c_void_p)]),
+        "hgg_server_submit": (ctypes.c_int, [B, ctypes.c_char_p, ctypes.c_int32, ctypes.c_int32, P, ctypes.c_int32,
+                                             ctypes.c_char_p, ctypes.c_int32, P, ctypes.c_int64, INITIAL_FN, P,
+                                             ctypes.c_double, ctypes.c_int32, ctypes.POINTER(ctypes.c_int64)]),
+        "hgg_server_poll": (ctypes.c_int, [B, ctypes.c_int64, ctypes.c_int32, P, ctypes.c_int64,
+                                           ctypes.POINTER(ctypes.c_double)]),
+        "hgg_server_result_length": (ctypes.c_int64, [B, ctypes.c_int64]),
+        "hgg_server_release": (ctypes.c_int, [B, ctypes.c_int64]),
+        "hgg_server_times": (ctypes.c_int, [B, ctypes.c_int64, P]),
+        "hgg_server_stats": (ctypes.c_int, [B, P]),
+        "hgg_server_last_error": (ctypes.c_char_p, [B]),
+        "hgg_server_stop": (ctypes.c_int, [B]),
         "hgg_synchronize": (ctypes.c_int, [H]),
         "hgg_vector_length": (ctypes.c_int64, [H]),
         "hgg_kernel_kind": (ctypes.c_int, [H]),
@@ -122,6 +142,13 @@ def load():
 def check(code, handle=None):
     if code != 0:
         msg = load().hgg_last_error(handle)
+        raise NativeError(code, msg.decode() if msg else "")
+    return code
+
+
+def check_server(code, server=None):
+    if code < 0:
+        msg = load().hgg_server_last_error(server)
         raise NativeError(code, msg.decode() if msg else "")
     return code
 

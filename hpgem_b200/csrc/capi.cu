@@ -908,3 +908,5 @@ int hgg_l2_error(hgg_handle *h, int32_t vec, const double *exact, double *error)
 
 // grouped execution of many problems (hgg_batch_*)
 #include "batch_exec.cuh"
+// serving loop over a batch (hgg_server_*)
+#include "server.cuh"

@@ -1,0 +1,456 @@
+// Serving loop (hgg_server_*): continuous batching of independent solves.
+//
+// Requests (a structured mesh description, order, physics, parameters,
+// tableau, precision, initial condition, dt, step count) are admitted in
+// arrival order by device-memory footprint: a set-up thread reserves the
+// request's footprint against the budget (waiting while it does not fit),
+// builds its handle and projects its initial condition.  The GPU thread owns
+// one hgg_batch: between chunks of steps it adds the requests that are ready
+// and takes out the ones that are done (their solution is copied to the host
+// and their device memory freed, which admits the next ones).  So requests that
+// arrive while others run join the running mix at the next chunk boundary, and
+// every RK stage of all running requests of a kernel class is one launch.  A
+// chunk is the smallest number of steps any running request still needs,
+// capped, so no request idles on the device after its last step.
+#pragma once
+
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <thread>
+#include <unordered_map>
+
+namespace {
+
+double now_s() {
+    using namespace std::chrono;
+    return duration<double>(steady_clock::now().time_since_epoch()).count();
+}
+
+struct ServerRequest {
+    int64_t id = 0;
+    std::string description, tableau;
+    int order = 1, physics = 0, precision = 0;
+    std::vector<double> params;
+    std::vector<double> u0;  // initial coefficients, or empty (then init_fn)
+    hgg_initial_fn init_fn = nullptr;
+    void *user = nullptr;
+    double dt = 0.0;
+    int nsteps = 0;
+    // life cycle
+    int state = 0;  // 0 queued, 1 set-up, 2 ready, 3 running, 4 done, 5 failed
+    int error = 0;
+    std::string message;
+    hgg_handle *h = nullptr;
+    int slot = -1;
+    int64_t footprint = 0;
+    int64_t dofs = 0;
+    std::vector<double> result;
+    double t_submit = 0, t_ready = 0, t_start = 0, t_done = 0;
+};
+
+}  // namespace
+
+struct hgg_server {
+    int device = 0;
+    int64_t budget = 0;
+    int max_chunk = 25;
+    std::mutex mu;
+    std::condition_variable cv_setup, cv_gpu, cv_done, cv_mem;
+    std::deque<ServerRequest *> queued, ready;
+    std::unordered_map<int64_t, std::unique_ptr<ServerRequest>> requests;
+    int64_t next_id = 1;
+    int64_t reserved = 0;
+    bool stopping = false;
+    std::vector<std::thread> setup_threads;
+    std::thread gpu_thread;
+    hgg_batch *batch = nullptr;
+    std::string err = "no error";
+    int gpu_error = 0;
+    // counters
+    int64_t completed = 0, dof_updates = 0, chunks = 0;
+};
+
+namespace {
+
+thread_local std::string g_server_create_error = "no error";
+
+// device bytes of a problem: both solution buffers, the stage vectors, the
+// conversion scratch and the per-element geometry and operator tables
+int64_t estimate_footprint(const hgg_problem_desc &d) {
+    const int64_t N = d.n_elements * (int64_t)d.n_vars * d.n_basis;
+    const int64_t kbytes = d.precision == HGG_PRECISION_FP32 ? 4 : 8;
+    return (3 * 8 + d.n_stages * kbytes) * (N + 64 * 64) + d.n_elements * 640 + (8 << 20);
+}
+
+void setup_loop(hgg_server *s) {
+    cudaSetDevice(s->device);
+    for (;;) {
+        ServerRequest *r = nullptr;
+        {
+            std::unique_lock<std::mutex> lk(s->mu);
+            s->cv_setup.wait(lk, [&] { return s->stopping || !s->queued.empty(); });
+            if (s->queued.empty()) return;  // stopping
+            r = s->queued.front();
+            s->queued.pop_front();
+            r->state = 1;
+        }
+        // footprint from the host descriptor
+        hgg_problem_desc d{};
+        void *owner = nullptr;
+        int rc = hgg_structured_descriptor(r->description.c_str(), r->order, r->physics, r->params.data(),
+                                           r->tableau.c_str(), r->precision, &d, &owner);
+        if (rc == 0) {
+            r->footprint = estimate_footprint(d);
+            r->dofs = d.n_elements * (int64_t)d.n_vars * d.n_basis;
+            hgg_free_descriptor(owner);
+        }
+        bool holds = false;  // this request's footprint is counted in s->reserved
+        if (rc == 0) {
+            std::unique_lock<std::mutex> lk(s->mu);
+            if (r->footprint > s->budget) {
+                rc = HGG_ERR_NOMEM;
+                r->message = "request needs more device memory than the server's budget";
+            } else {
+                // admission: wait until the footprint fits next to the requests already admitted
+                s->cv_mem.wait(lk, [&] { return s->stopping || s->reserved + r->footprint <= s->budget; });
+                if (s->stopping) {
+                    rc = HGG_ERR_INVALID;
+                    r->message = "server stopped";
+                } else {
+                    s->reserved += r->footprint;
+                    holds = true;
+                }
+            }
+        } else {
+            r->message = hgg_last_error(nullptr);
+        }
+        if (rc == 0) {
+            rc = hgg_create_structured(r->description.c_str(), r->order, r->physics, r->params.data(),
+                                       r->tableau.c_str(), r->precision, &r->h);
+            if (rc) r->message = hgg_last_error(nullptr);
+        }
+        if (rc == 0) {
+            if (!r->u0.empty()) {
+                if ((int64_t)r->u0.size() != hgg_vector_length(r->h)) {
+                    rc = HGG_ERR_INVALID;
+                    r->message = "initial coefficients have the wrong length";
+                } else {
+                    rc = hgg_set_state(r->h, 0, r->u0.data());
+                }
+            } else if (r->init_fn) {
+                const int32_t nq = hgg_num_quadrature_points(r->h);
+                const int64_t nE = hgg_vector_length(r->h) / ((int64_t)r->h->op.V * r->h->op.nB);
+                const int dim = r->h->op.dim;
+                std::vector<double> xyz((size_t)nE * nq * dim), vals((size_t)nE * nq * r->h->op.V);
+                rc = hgg_quadrature_points(r->h, xyz.data());
+                if (rc == 0) {
+                    r->init_fn(xyz.data(), nE * nq, dim, vals.data(), r->user);
+                    rc = hgg_project(r->h, vals.data(), 0);
+                }
+            }
+            if (rc) r->message = hgg_last_error(r->h);
+            else hgg_set_store_last_stage(r->h, 0);
+        }
+        std::vector<double>().swap(r->u0);
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (rc) {
+            if (r->h) {
+                hgg_destroy(r->h);
+                r->h = nullptr;
+            }
+            if (holds) s->reserved -= r->footprint;
+            r->error = rc;
+            r->state = 5;
+            r->t_done = now_s();
+            s->cv_done.notify_all();
+            s->cv_mem.notify_all();
+        } else {
+            r->state = 2;
+            r->t_ready = now_s();
+            s->ready.push_back(r);
+            s->cv_gpu.notify_all();
+        }
+    }
+}
+
+void gpu_loop(hgg_server *s) {
+    cudaSetDevice(s->device);
+    std::vector<ServerRequest *> running;
+    for (;;) {
+        std::vector<ServerRequest *> joining;
+        {
+            std::unique_lock<std::mutex> lk(s->mu);
+            if (running.empty())
+                s->cv_gpu.wait(lk, [&] {
+                    return !s->ready.empty() || (s->stopping && s->queued.empty() && s->ready.empty());
+                });
+            if (running.empty() && s->ready.empty() && s->stopping) return;
+            while (!s->ready.empty()) {
+                joining.push_back(s->ready.front());
+                s->ready.pop_front();
+            }
+        }
+        for (ServerRequest *r : joining) {
+            int32_t slot = -1;
+            int rc = hgg_batch_add(s->batch, r->h, r->dt, r->nsteps, &slot);
+            std::lock_guard<std::mutex> lk(s->mu);
+            if (rc) {
+                r->error = rc;
+                r->message = hgg_batch_last_error(s->batch);
+                r->state = 5;
+                r->t_done = now_s();
+                hgg_destroy(r->h);
+                r->h = nullptr;
+                s->reserved -= r->footprint;
+                s->cv_mem.notify_all();
+                s->cv_done.notify_all();
+                continue;
+            }
+            r->slot = slot;
+            r->state = 3;
+            r->t_start = now_s();
+            running.push_back(r);
+        }
+        if (running.empty()) continue;
+        int chunk = s->max_chunk;
+        for (ServerRequest *r : running) {
+            const int left = hgg_batch_remaining(s->batch, r->slot);
+            if (left > 0) chunk = std::min(chunk, left);
+        }
+        chunk = std::max(chunk, 1);
+        int rc = hgg_batch_step(s->batch, chunk);
+        if (rc == 0) rc = hgg_batch_synchronize(s->batch);
+        if (rc) {
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->gpu_error = rc;
+            s->err = hgg_batch_last_error(s->batch);
+            // every request not finished fails with the device error
+            for (auto &kv : s->requests) {
+                ServerRequest *r = kv.second.get();
+                if (r->state >= 4) continue;
+                r->error = rc;
+                r->message = s->err;
+                r->state = 5;
+                r->t_done = now_s();
+            }
+            s->queued.clear();
+            s->ready.clear();
+            s->stopping = true;
+            s->cv_done.notify_all();
+            s->cv_setup.notify_all();
+            s->cv_mem.notify_all();
+            return;
+        }
+        s->chunks++;
+        std::vector<ServerRequest *> still;
+        for (ServerRequest *r : running) {
+            if (hgg_batch_remaining(s->batch, r->slot) > 0) {
+                still.push_back(r);
+                continue;
+            }
+            int rr = hgg_batch_remove(s->batch, r->slot);
+            if (rr == 0) {
+                r->result.resize((size_t)hgg_vector_length(r->h));
+                rr = hgg_get_state(r->h, 0, r->result.data());
+            }
+            hgg_destroy(r->h);
+            r->h = nullptr;
+            std::lock_guard<std::mutex> lk(s->mu);
+            r->error = rr;
+            if (rr) r->message = hgg_batch_last_error(s->batch);
+            r->state = rr ? 5 : 4;
+            r->t_done = now_s();
+            s->reserved -= r->footprint;
+            s->completed++;
+            s->dof_updates += r->dofs * (int64_t)r->nsteps;
+            s->cv_mem.notify_all();
+            s->cv_done.notify_all();
+        }
+        running.swap(still);
+    }
+}
+
+int sfail(hgg_server *s, int code, const std::string &msg) {
+    if (s) {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->err = msg;
+    } else {
+        g_server_create_error = msg;
+    }
+    return code;
+}
+
+}  // namespace
+
+extern "C" {
+
+int hgg_server_start(int64_t budget_bytes, int32_t max_chunk, int32_t setup_threads, int32_t capacity,
+                     hgg_server **out) {
+    if (!out || budget_bytes <= 0 || max_chunk < 1 || setup_threads < 1 || capacity < 1)
+        return sfail(nullptr, HGG_ERR_INVALID, "budget, chunk, set-up threads and capacity must be positive");
+    *out = nullptr;
+    auto *s = new hgg_server();
+    if (cudaGetDevice(&s->device) != cudaSuccess) {
+        delete s;
+        return sfail(nullptr, HGG_ERR_NOT_LOADED, "no CUDA device available");
+    }
+    s->budget = budget_bytes;
+    s->max_chunk = max_chunk;
+    int rc = hgg_batch_create(capacity, &s->batch);
+    if (rc) {
+        g_server_create_error = hgg_batch_last_error(nullptr);
+        delete s;
+        return rc;
+    }
+    for (int i = 0; i < setup_threads; ++i) s->setup_threads.emplace_back(setup_loop, s);
+    s->gpu_thread = std::thread(gpu_loop, s);
+    *out = s;
+    return 0;
+}
+
+int hgg_server_submit(hgg_server *s, const char *description, int32_t order, int32_t physics, const double *params,
+                      int32_t n_params, const char *tableau, int32_t precision, const double *u0, int64_t n_u0,
+                      hgg_initial_fn init_fn, void *user, double dt, int32_t nsteps, int64_t *id) {
+    if (!s || !description || !params || n_params < 1 || !tableau || !id || !(dt > 0.0) || nsteps < 1)
+        return sfail(s, HGG_ERR_INVALID, "bad request");
+    if (!u0 && !init_fn) return sfail(s, HGG_ERR_INVALID, "an initial condition is required");
+    auto r = std::make_unique<ServerRequest>();
+    r->description = description;
+    r->tableau = tableau;
+    r->order = order;
+    r->physics = physics;
+    r->precision = precision;
+    r->params.assign(params, params + n_params);
+    if (u0) r->u0.assign(u0, u0 + n_u0);
+    r->init_fn = init_fn;
+    r->user = user;
+    r->dt = dt;
+    r->nsteps = nsteps;
+    r->t_submit = now_s();
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->stopping) {
+        s->err = "server is stopping";
+        return HGG_ERR_INVALID;
+    }
+    r->id = s->next_id++;
+    *id = r->id;
+    s->queued.push_back(r.get());
+    s->requests.emplace(r->id, std::move(r));
+    s->cv_setup.notify_one();
+    return 0;
+}
+
+// 1: done (solution copied to `out` if not null, latency in seconds), 0: not yet,
+// < 0: the request failed (message via hgg_server_last_error) or the id is unknown.
+// With wait != 0 it blocks until the request is finished.
+int hgg_server_poll(hgg_server *s, int64_t id, int32_t wait, double *out, int64_t n_out, double *latency_s) {
+    if (!s) return sfail(s, HGG_ERR_INVALID, "null server");
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto it = s->requests.find(id);
+    if (it == s->requests.end()) {
+        s->err = "unknown request id";
+        return HGG_ERR_INVALID;
+    }
+    ServerRequest *r = it->second.get();
+    if (wait) s->cv_done.wait(lk, [&] { return r->state >= 4; });
+    if (r->state < 4) return 0;
+    if (latency_s) *latency_s = r->t_done - r->t_submit;
+    if (r->state == 5) {
+        s->err = r->message;
+        return r->error ? r->error : HGG_ERR_INVALID;
+    }
+    if (out) {
+        if (n_out != (int64_t)r->result.size()) {
+            s->err = "output length " + std::to_string(n_out) + " != " + std::to_string(r->result.size());
+            return HGG_ERR_INVALID;
+        }
+        std::copy(r->result.begin(), r->result.end(), out);
+    }
+    return 1;
+}
+
+// number of coefficients of a finished request's solution (0 while running)
+int64_t hgg_server_result_length(hgg_server *s, int64_t id) {
+    if (!s) return -1;
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->requests.find(id);
+    if (it == s->requests.end()) return -1;
+    return it->second->state == 4 ? (int64_t)it->second->result.size() : 0;
+}
+
+// drops a finished request's record and result
+int hgg_server_release(hgg_server *s, int64_t id) {
+    if (!s) return sfail(s, HGG_ERR_INVALID, "null server");
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->requests.find(id);
+    if (it == s->requests.end() || it->second->state < 4) {
+        s->err = "unknown or unfinished request";
+        return HGG_ERR_INVALID;
+    }
+    s->requests.erase(it);
+    return 0;
+}
+
+// timestamps (seconds, steady clock) of a request: submit, ready (set up), start (first step), done
+int hgg_server_times(hgg_server *s, int64_t id, double *t4) {
+    if (!s || !t4) return sfail(s, HGG_ERR_INVALID, "null argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->requests.find(id);
+    if (it == s->requests.end()) {
+        s->err = "unknown request id";
+        return HGG_ERR_INVALID;
+    }
+    const ServerRequest *r = it->second.get();
+    t4[0] = r->t_submit;
+    t4[1] = r->t_ready;
+    t4[2] = r->t_start;
+    t4[3] = r->t_done;
+    return 0;
+}
+
+// completed requests, their DoF-updates, chunks stepped, bytes reserved now
+int hgg_server_stats(hgg_server *s, int64_t *stats4) {
+    if (!s || !stats4) return sfail(s, HGG_ERR_INVALID, "null argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    stats4[0] = s->completed;
+    stats4[1] = s->dof_updates;
+    stats4[2] = s->chunks;
+    stats4[3] = s->reserved;
+    return 0;
+}
+
+const char *hgg_server_last_error(hgg_server *s) {
+    if (!s) return g_server_create_error.c_str();
+    std::lock_guard<std::mutex> lk(s->mu);
+    thread_local std::string copy;
+    copy = s->err;
+    return copy.c_str();
+}
+
+// Finishes every submitted request, then stops the threads and frees the server.
+int hgg_server_stop(hgg_server *s) {
+    if (!s) return sfail(s, HGG_ERR_INVALID, "null server");
+    {
+        std::unique_lock<std::mutex> lk(s->mu);
+        s->cv_done.wait(lk, [&] {
+            for (auto &kv : s->requests)
+                if (kv.second->state < 4) return s->gpu_error != 0;
+            return true;
+        });
+        s->stopping = true;
+    }
+    s->cv_setup.notify_all();
+    s->cv_gpu.notify_all();
+    s->cv_mem.notify_all();
+    for (auto &t : s->setup_threads) t.join();
+    s->gpu_thread.join();
+    const int rc = s->gpu_error;
+    hgg_batch_destroy(s->batch);
+    for (auto &kv : s->requests)
+        if (kv.second->h) hgg_destroy(kv.second->h);
+    delete s;
+    return rc;
+}
+
+}  // extern "C"

@@ -280,6 +280,57 @@ int hgg_batch_set_autotune(hgg_batch *b, int32_t enable);
 int64_t hgg_batch_launch_count(const hgg_batch *b);
 int32_t hgg_batch_num_classes(const hgg_batch *b);
 
+/* ---- serving loop ------------------------------------------------------------
+ * No counterpart in the reference.  A server admits solves (a Preprocessor
+ * structured description, order, physics, parameters, tableau, precision,
+ * initial condition, dt, step count) in arrival order while their device
+ * footprint fits a byte budget, keeps their state on the device, and advances
+ * all running solves together through one batch of the kind above (every RK stage of all
+ * running solves of a kernel class is one launch); solves that arrive while
+ * others run join at the next chunk boundary, and a finished solve's memory
+ * admits the next.  Set-up (host descriptor, handle, projection) runs on
+ * `setup_threads` threads beside the GPU thread.  submit/poll/release/times/
+ * stats are thread-safe. */
+typedef struct hgg_server hgg_server;
+
+/* Initial condition callback: values[n_points][n_vars] at points xyz[n_points][dim]
+ * (the element quadrature points; the server projects the values). */
+typedef void (*hgg_initial_fn)(const double *xyz, int64_t n_points, int32_t dim, double *values, void *user);
+
+/* Starts a server on the current device: budget_bytes of device memory for the
+ * solves' state, at most max_chunk steps between admissions, `capacity`
+ * solves running at once. */
+int hgg_server_start(int64_t budget_bytes, int32_t max_chunk, int32_t setup_threads, int32_t capacity,
+                     hgg_server **out);
+
+/* Queues one solve; the initial condition is either n_u0 coefficients in hpGEM
+ * order (u0) or a callback (init_fn, user; called on a set-up thread). */
+int hgg_server_submit(hgg_server *s, const char *description, int32_t order, int32_t physics, const double *params,
+                      int32_t n_params, const char *tableau, int32_t precision, const double *u0, int64_t n_u0,
+                      hgg_initial_fn init_fn, void *user, double dt, int32_t nsteps, int64_t *id);
+
+/* 1 when the solve is done (its solution copied into out[n_out] unless out is
+ * null; *latency_s = done - submit), 0 while it is queued or running, < 0 if it
+ * failed (message via hgg_server_last_error).  wait != 0 blocks until done. */
+int hgg_server_poll(hgg_server *s, int64_t id, int32_t wait, double *out, int64_t n_out, double *latency_s);
+
+/* Coefficients in a finished solve's solution (0 while not finished). */
+int64_t hgg_server_result_length(hgg_server *s, int64_t id);
+
+/* Forgets a finished solve. */
+int hgg_server_release(hgg_server *s, int64_t id);
+
+/* Steady-clock times in seconds of submit, set-up done, first step, done. */
+int hgg_server_times(hgg_server *s, int64_t id, double *t4);
+
+/* Completed solves, their DoF-updates, chunks stepped, device bytes reserved now. */
+int hgg_server_stats(hgg_server *s, int64_t *stats4);
+
+const char *hgg_server_last_error(hgg_server *s);
+
+/* Waits for every submitted solve, stops the threads, frees the server. */
+int hgg_server_stop(hgg_server *s);
+
 #ifdef __cplusplus
 }
 #endif
