@@ -351,6 +351,10 @@ def run_ours(args):
                          "traffic": (tr * ndof if tr else None),
                          "traffic_unit": "bytes per RK4 step (4 launches)"},
             "forms": forms}
+    if rank == 0 and world == 1 and not args.no_batched:
+        line["batched"] = run_batched(args, stream)
+    if rank == 0 and world == 1 and not args.no_served:
+        line["served"] = run_served(args)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, sample = cpu_sample_rate()
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
@@ -362,6 +366,113 @@ def run_ours(args):
         print(json.dumps(line), flush=True)
 
 
+def run_batched(args, stream):
+    """512 independent 2D advection problems (quads/triangles, p 1..5, 8^2..128^2, per-problem
+    velocity and CFL dt), RK4, 100 steps each, advanced together by one batch."""
+    import torch
+
+    import hpgem_b200
+    from hpgem_b200 import workloads
+
+    specs = workloads.batched_problems()
+    t0 = time.perf_counter()
+    solvers = [workloads.make_solver(sp) for sp in specs]
+    setup_s = time.perf_counter() - t0
+    total_dof = sum(workloads.dof(sp) for sp in specs)
+    warm = 3
+    steps = specs[0]["steps"]
+    batch = hpgem_b200.Batch(len(specs))
+    u0 = [s.getTimeIntegrationVector(0).reshape(-1).copy() for s in solvers]
+    for s, sp in zip(solvers, specs):
+        batch.add(s, sp["dt"], steps + warm)
+    batch.step(warm)  # first step: tables, autotuning, graph capture
+    batch.synchronize()
+    launches0 = batch.launch_count
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    batch.step(steps)
+    batch.synchronize()
+    wall = time.perf_counter() - t0
+    launches = batch.launch_count - launches0
+    # end to end through the public API: initial coefficients from the host into every
+    # problem, the 100 steps, every solution back to the host
+    for i, s in enumerate(solvers):
+        batch.remove(i)
+    t0 = time.perf_counter()
+    for i, (s, sp) in enumerate(zip(solvers, specs)):
+        s.setTimeIntegrationVector(0, u0[i])
+        batch.add(s, sp["dt"], steps)
+    batch.step(steps)
+    batch.synchronize()
+    outs = [s.getTimeIntegrationVector(0) for s in solvers]
+    e2e = time.perf_counter() - t0
+    finite = all(np.isfinite(o).all() for o in outs)
+    classes = batch.num_classes
+    batch.close()
+    return {"workload": "512 2D advection problems, quads/triangles, p 1..5, 8^2..128^2 cells, "
+                        "RK4, 100 steps each, seed 4",
+            "value": total_dof * steps / wall, "unit": UNIT, "dtype": "f64", "problems": len(specs),
+            "dof": total_dof, "steps": steps, "wall_s": wall, "kernel_classes": classes,
+            "gpu_launches": int(launches), "host_setup_s": setup_s,
+            "timing": "host wall clock around batch step + synchronize (device idle before)",
+            "e2e": {"value": total_dof * steps / e2e, "unit": UNIT, "wall_s": e2e,
+                    "h2d_bytes": 8 * total_dof, "d2h_bytes": 8 * total_dof, "finite": bool(finite)},
+            "form_note": "FP64: the FP32-mixed form has kernels for hexahedra of order 3 only"}
+
+
+def run_served(args):
+    """Poisson stream (200 requests/s, seed 5) of 2D/3D advection and acoustic-wave solves,
+    1e3..2e6 DoF, p 1..4, 50..2000 steps, replayed in real time into the server."""
+    import hpgem_b200
+    from hpgem_b200 import workloads
+
+    specs = workloads.served_requests(n=args.served_requests)
+    setup_threads = max(2, min(16, (os.cpu_count() or 4) // 2))
+    server = hpgem_b200.Server(budget_bytes=48 << 30, max_chunk=25, setup_threads=setup_threads)
+
+    def desc(sp):
+        d = len(sp["cells"])
+        return hpgem_b200.structured_description(sp["cells"], [0.0] * d, [1.0] * d, sp["triangular"], True)
+
+    ids = []
+    t_start = time.perf_counter()
+    for sp in specs:
+        delay = sp["arrival"] - (time.perf_counter() - t_start)
+        if delay > 0:
+            time.sleep(delay)
+        d = len(sp["cells"])
+        u0 = sp["u0"]
+        if sp["physics"] == "advection":
+            fn, nv = u0, 1
+        else:
+            fn, nv = (lambda x, u0=u0, d=d: np.concatenate([u0(x)[:, None], np.zeros((len(x), d))], axis=1)), d + 1
+        ids.append(server.submit(desc(sp), sp["order"], sp["physics"], sp["params"], sp["dt"], sp["steps"],
+                                 initial=fn, n_vars=nv))
+    lat, done_t, sub_t = [], [], []
+    for rid in ids:
+        ok, _, l = server.poll(rid, wait=True, result=False)
+        t = server.times(rid)
+        lat.append(l)
+        sub_t.append(t[0])
+        done_t.append(t[3])
+        server.release(rid)
+    stats = server.stats()
+    server.stop()
+    span = max(done_t) - min(sub_t)
+    lat = np.array(lat)
+    return {"workload": "Poisson stream, 200 requests/s, %d requests, seed 5: 2D/3D advection and "
+                        "acoustic wave, 1e3..2e6 DoF, p 1..4, 50..2000 steps" % len(specs),
+            "value": stats["dof_updates"] / span, "unit": UNIT, "dtype": "f64",
+            "requests": len(specs), "p50_latency_s": float(np.percentile(lat, 50)),
+            "p99_latency_s": float(np.percentile(lat, 99)), "mean_latency_s": float(lat.mean()),
+            "span_s": span, "dof_updates": stats["dof_updates"], "chunks": stats["chunks"],
+            "setup_threads": setup_threads, "budget_bytes": 48 << 30,
+            "offered_dof_updates_per_s": sum(workloads.dof(sp) * sp["steps"] for sp in specs)
+            / max(specs[-1]["arrival"], 1e-9),
+            "timing": "host steady clock, latency = done - submit (set-up, queueing, steps, copy back)",
+            "form_note": "FP64: the FP32-mixed form has kernels for hexahedra of order 3 only"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -369,6 +480,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true", help="skip the 512-problem batched leg")
+    ap.add_argument("--no-served", action="store_true", help="skip the served request-stream leg")
+    ap.add_argument("--served-requests", type=int, default=2000)
     args = ap.parse_args()
     if args.impl == "reference":
         if int(os.environ.get("RANK", "0")) != 0:

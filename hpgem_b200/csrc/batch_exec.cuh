@@ -59,7 +59,7 @@ __device__ __forceinline__ int find_item(const Item *items, int n, int64_t vb) {
     return lo;
 }
 
-template <int DIM, int NFL, int WAVE>
+template <int DIM, int NFL, int WAVE, int NB>
 __global__ void __launch_bounds__(256)
     grouped_dense(const DenseItem *items, const int *n_items, const int64_t *total, const int *parity,
                   const int *remaining) {
@@ -70,7 +70,7 @@ __global__ void __launch_bounds__(256)
         const int slot = items[i].slot;
         __syncthreads();  // shared memory of the previous virtual block is free
         if (remaining[slot] <= 0) continue;
-        dense_stage_body<DIM, NFL, WAVE>(items[i].io[parity[slot]], items[i].g, vb - items[i].block0);
+        dense_stage_body<DIM, NFL, WAVE, NB>(items[i].io[parity[slot]], items[i].g, vb - items[i].block0);
     }
 }
 
@@ -299,13 +299,18 @@ int upload_class(hgg_batch *b, BatchClass &c) {
 
 template <int DIM, int NFL, int WAVE>
 void launch_grouped_dense(const hgg_batch *b, const BatchClass &c, int st, unsigned grid, cudaStream_t s) {
-    const int R = (WAVE ? DIM + 1 : 1) * b->handles[c.slots[0]]->op.nB;
+    const int nB = b->handles[c.slots[0]]->op.nB;
+    const int R = (WAVE ? DIM + 1 : 1) * nB;
     const int threads = ((c.epb * R + 31) / 32) * 32;
     const size_t smem = sizeof(double) * (size_t)c.epb * R * (1 + NFL);
-    if (smem > 48 * 1024)
-        cudaFuncSetAttribute(grouped_dense<DIM, NFL, WAVE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    grouped_dense<DIM, NFL, WAVE><<<grid, threads, smem, s>>>(static_cast<const DenseItem *>(c.d_items[st]), c.d_n,
-                                                             c.d_total, b->d_parity, b->d_remaining);
+    dense_dispatch<DIM, NFL, WAVE>(nB, [&](auto nbc) {
+        constexpr int NB = decltype(nbc)::value;
+        if (smem > 48 * 1024)
+            cudaFuncSetAttribute(grouped_dense<DIM, NFL, WAVE, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem);
+        grouped_dense<DIM, NFL, WAVE, NB><<<grid, threads, smem, s>>>(
+            static_cast<const DenseItem *>(c.d_items[st]), c.d_n, c.d_total, b->d_parity, b->d_remaining);
+    });
 }
 
 template <int P, int DIM>

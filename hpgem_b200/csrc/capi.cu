@@ -278,13 +278,16 @@ int launch_dense(hgg_handle *h, const StageIO &io) {
     DenseGeom g{h->d_vol, h->d_pairs, h->d_nbr, h->d_self, h->d_nbrp, h->d_mode,
                 h->d_elem_geo, h->d_face_geo, 1.0 / op.c_inv, op.nB, epb};
     size_t smem = sizeof(double) * (size_t)epb * R * (1 + NFL);
-    if (smem > 48 * 1024) {
-        cudaFuncSetAttribute(dense_stage<DIM, NFL, WAVE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem);
-    }
     int64_t blocks = (op.nE + epb - 1) / epb;
     int threads = ((epb * R + 31) / 32) * 32;
-    dense_stage<DIM, NFL, WAVE><<<(unsigned)blocks, threads, smem, h->stream>>>(io, g);
+    const bool ok = dense_dispatch<DIM, NFL, WAVE>(op.nB, [&](auto nbc) {
+        constexpr int NB = decltype(nbc)::value;
+        if (smem > 48 * 1024)
+            cudaFuncSetAttribute(dense_stage<DIM, NFL, WAVE, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem);
+        dense_stage<DIM, NFL, WAVE, NB><<<(unsigned)blocks, threads, smem, h->stream>>>(io, g);
+    });
+    if (!ok) return fail(h, HGG_ERR_UNSUPPORTED, "dense kernel: no kernel for this basis size");
     return 0;
 }
 
@@ -482,7 +485,16 @@ int create_from_desc(const hgg_problem_desc *desc, hgg_handle *h) {
         if ((rc = alloc(h, sizeof(double) * h->N_alloc, (void **)&h->d_scratch))) return rc;
     } else {
         if (h->mixed && (rc = alloc(h, sizeof(double) * h->N_alloc, (void **)&h->d_scratch))) return rc;
-        if ((rc = upload(h, op.vol, &h->d_vol)) || (rc = upload(h, op.pairs, &h->d_pairs)) ||
+        // the dense kernel reads its operators transposed ([..][j][i]): coalesced across rows i
+        auto transposed = [&](const std::vector<double> &m) {
+            std::vector<double> t(m.size());
+            const size_t nb = (size_t)op.nB, blocks = nb ? m.size() / (nb * nb) : 0;
+            for (size_t q = 0; q < blocks; ++q)
+                for (size_t i = 0; i < nb; ++i)
+                    for (size_t j = 0; j < nb; ++j) t[(q * nb + j) * nb + i] = m[(q * nb + i) * nb + j];
+            return t;
+        };
+        if ((rc = upload(h, transposed(op.vol), &h->d_vol)) || (rc = upload(h, transposed(op.pairs), &h->d_pairs)) ||
             (rc = upload(h, op.nbr, &h->d_nbr)) || (rc = upload(h, op.self_pair, &h->d_self)) ||
             (rc = upload(h, op.nbr_pair, &h->d_nbrp)) || (rc = upload(h, op.mode, &h->d_mode)) ||
             (rc = upload(h, op.elem_geo, &h->d_elem_geo)) || (rc = upload(h, op.face_geo, &h->d_face_geo)))

@@ -19,6 +19,7 @@
 #pragma once
 
 #include <cstdint>
+#include <type_traits>
 
 namespace hgg {
 
@@ -210,8 +211,8 @@ __global__ void __launch_bounds__(EPB *TensorConsts<P, DIM>::NB)
 // dense reference operators, any shape and physics
 // ---------------------------------------------------------------------------
 struct DenseGeom {
-    const double *vol;         // [DIM][NB][NB]
-    const double *pairs;       // [n_pairs][NB][NB]
+    const double *vol;         // [DIM][NB][NB], transposed: vol[c][j][i] = (Mhat^{-1} K_c)_{ij}
+    const double *pairs;       // [n_pairs][NB][NB], transposed the same way
     const int32_t *nbr;        // [E][NFL]
     const int32_t *self_pair;  // [E][NFL]
     const int32_t *nbr_pair;   // [E][NFL]
@@ -224,11 +225,18 @@ struct DenseGeom {
 };
 
 // One block's work: elements [block * epb, block * epb + epb) (see tensor_stage_body).
-template <int DIM, int NFL, int WAVE>
+// Thread (el, r) produces output row r of element el.  The operators are stored
+// transposed, so at every column j the threads of a warp read consecutive rows'
+// entries: one or two sectors per warp instead of one per thread.
+//
+// NB (basis functions) is a compile-time constant, so the row loops unroll and
+// the index arithmetic needs no runtime division.
+template <int DIM, int NFL, int WAVE, int NB>
 __device__ __forceinline__ void dense_stage_body(const StageIO &io, const DenseGeom &g, int64_t block) {
     constexpr int V = WAVE ? DIM + 1 : 1;
+    constexpr int nB = NB, R = V * NB;
     extern __shared__ double smem[];
-    const int nB = g.nB, R = V * nB, epb = g.epb;
+    const int epb = g.epb;
     double *W = smem;                        // [epb][R]
     double *WN = smem + (size_t)epb * R;     // [epb][NFL][R]
     const int tid = threadIdx.x;
@@ -257,6 +265,51 @@ __device__ __forceinline__ void dense_stage_body(const StageIO &io, const DenseG
         WN[(size_t)(l * NFL + f) * R + rr] = v;
     }
     __syncthreads();
+    if (WAVE && DIM >= 2) {
+        // per element and axis c: t_c = sum_d G[d][c] s_d (the velocity combination the
+        // divergence row needs), and per face: the normal jumps n . s of both sides,
+        // formed once per element instead of once per output row; they replace the
+        // velocity blocks of W and WN (the velocity rows read only the pressure block)
+        double tmp[DIM];
+        const int64_t ee = e;
+        if (active && r < nB) {
+            const double *G = g.elem_geo + ee * DIM * DIM;
+            double *w = W + el * R;
+#pragma unroll
+            for (int c = 0; c < DIM; ++c) {
+                double t = 0.0;
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) t += G[d * DIM + c] * w[(d + 1) * nB + r];
+                tmp[c] = t;
+            }
+        }
+        double jl[NFL], jn[NFL];
+        if (active && r < nB) {
+            const double *w = W + el * R;
+            const double *wn = WN + (size_t)el * NFL * R;
+            for (int f = 0; f < NFL; ++f) {
+                const double *nu = g.face_geo + ((size_t)ee * NFL + f) * DIM;
+                double a = 0.0, b = 0.0;
+                for (int d = 0; d < DIM; ++d) {
+                    a += nu[d] * w[(d + 1) * nB + r];
+                    b += nu[d] * wn[f * R + (d + 1) * nB + r];
+                }
+                jl[f] = a;
+                jn[f] = b;
+            }
+        }
+        __syncthreads();
+        if (active && r < nB) {
+            double *w = W + el * R;
+            double *wn = WN + (size_t)el * NFL * R;
+            for (int c = 0; c < DIM; ++c) w[(c + 1) * nB + r] = tmp[c];
+            for (int f = 0; f < NFL; ++f) {  // velocity blocks 1 and 2 of the face slot
+                wn[f * R + nB + r] = jl[f];
+                wn[f * R + 2 * nB + r] = jn[f];
+            }
+        }
+        __syncthreads();
+    }
     if (!active) return;
 
     const double *w = W + el * R;
@@ -265,9 +318,10 @@ __device__ __forceinline__ void dense_stage_body(const StageIO &io, const DenseG
     if (!WAVE) {
         const int i = r;
         for (int c = 0; c < DIM; ++c) {
-            const double *op = g.vol + ((size_t)c * nB + i) * nB;
+            const double *op = g.vol + (size_t)c * nB * nB + i;
             double s = 0.0;
-            for (int j = 0; j < nB; ++j) s += op[j] * w[j];
+            #pragma unroll
+            for (int j = 0; j < nB; ++j) s += op[(size_t)j * nB] * w[j];
             acc += g.elem_geo[e * DIM + c] * s;
         }
         for (int f = 0; f < NFL; ++f) {
@@ -275,60 +329,72 @@ __device__ __forceinline__ void dense_stage_body(const StageIO &io, const DenseG
             const double sg = g.face_geo[e * NFL + f];
             double ts = 0.0, tn = 0.0;
             if (mode == 1 || mode == 3) {
-                const double *op = g.pairs + ((size_t)g.self_pair[e * NFL + f] * nB + i) * nB;
-                for (int j = 0; j < nB; ++j) ts += op[j] * w[j];
+                const double *op = g.pairs + (size_t)g.self_pair[e * NFL + f] * nB * nB + i;
+                #pragma unroll
+                for (int j = 0; j < nB; ++j) ts += op[(size_t)j * nB] * w[j];
             }
             if (mode == 2 || mode == 3) {
-                const double *op = g.pairs + ((size_t)g.nbr_pair[e * NFL + f] * nB + i) * nB;
-                for (int j = 0; j < nB; ++j) tn += op[j] * wn[f * R + j];
+                const double *op = g.pairs + (size_t)g.nbr_pair[e * NFL + f] * nB * nB + i;
+                #pragma unroll
+                for (int j = 0; j < nB; ++j) tn += op[(size_t)j * nB] * wn[f * R + j];
             }
             acc -= mode == 1 ? sg * ts : (mode == 2 ? sg * tn : (mode == 3 ? 0.5 * sg * (ts + tn) : 0.0));
         }
     } else {
         const int v = r / nB, i = r % nB;
         const double *G = g.elem_geo + e * DIM * DIM;  // G[d][c] = (J^{-T})_{dc}
-        if (v == 0) {
-            // k_q = sum_c vol[c] (sum_d G[d][c] s_d)   (strong-form divergence)
+        if (v == 0 && DIM >= 2) {
+            // k_q = sum_c vol[c] t_c  (strong-form divergence), minus the face jumps of n . s
             for (int c = 0; c < DIM; ++c) {
-                const double *op = g.vol + ((size_t)c * nB + i) * nB;
+                const double *op = g.vol + (size_t)c * nB * nB + i;
+                const double *t = w + (c + 1) * nB;
                 double s = 0.0;
-                for (int j = 0; j < nB; ++j) {
-                    double t = 0.0;
-                    for (int d = 0; d < DIM; ++d) t += G[d * DIM + c] * w[(d + 1) * nB + j];
-                    s += op[j] * t;
-                }
+                #pragma unroll
+                for (int j = 0; j < nB; ++j) s += op[(size_t)j * nB] * t[j];
                 acc += s;
             }
             for (int f = 0; f < NFL; ++f) {
-                const double *nu = g.face_geo + ((size_t)e * NFL + f) * DIM;
-                const double *ops = g.pairs + ((size_t)g.self_pair[e * NFL + f] * nB + i) * nB;
-                const double *opn = g.pairs + ((size_t)g.nbr_pair[e * NFL + f] * nB + i) * nB;
+                const double *ops = g.pairs + (size_t)g.self_pair[e * NFL + f] * nB * nB + i;
+                const double *opn = g.pairs + (size_t)g.nbr_pair[e * NFL + f] * nB * nB + i;
+                const double *js = wn + f * R + nB, *jn = wn + f * R + 2 * nB;
                 double s = 0.0;
-                for (int j = 0; j < nB; ++j) {
-                    double js = 0.0, jn = 0.0;
-                    for (int d = 0; d < DIM; ++d) {
-                        js += nu[d] * w[(d + 1) * nB + j];
-                        jn += nu[d] * wn[f * R + (d + 1) * nB + j];
-                    }
-                    s += ops[j] * js - opn[j] * jn;
-                }
+                #pragma unroll
+                for (int j = 0; j < nB; ++j) s += ops[(size_t)j * nB] * js[j] - opn[(size_t)j * nB] * jn[j];
                 acc -= s;
+            }
+        } else if (v == 0) {
+            // one dimension: G and the normal are scalars
+            const double *op = g.vol + i;
+            double s = 0.0;
+            #pragma unroll
+            for (int j = 0; j < nB; ++j) s += op[(size_t)j * nB] * w[nB + j];
+            acc += G[0] * s;
+            for (int f = 0; f < NFL; ++f) {
+                const double nu = g.face_geo[(size_t)e * NFL + f];
+                const double *ops = g.pairs + (size_t)g.self_pair[e * NFL + f] * nB * nB + i;
+                const double *opn = g.pairs + (size_t)g.nbr_pair[e * NFL + f] * nB * nB + i;
+                double t = 0.0;
+                #pragma unroll
+                for (int j = 0; j < nB; ++j) t += ops[(size_t)j * nB] * w[nB + j] - opn[(size_t)j * nB] * wn[f * R + nB + j];
+                acc -= nu * t;
             }
         } else {
             // k_{s_d} = (1/cInv) [ sum_c G[d][c] vol[c] q  - face jumps of q ]
             const int d = v - 1;
             for (int c = 0; c < DIM; ++c) {
-                const double *op = g.vol + ((size_t)c * nB + i) * nB;
+                const double *op = g.vol + (size_t)c * nB * nB + i;
                 double s = 0.0;
-                for (int j = 0; j < nB; ++j) s += op[j] * w[j];
+                #pragma unroll
+                for (int j = 0; j < nB; ++j) s += op[(size_t)j * nB] * w[j];
                 acc += G[d * DIM + c] * s;
             }
             for (int f = 0; f < NFL; ++f) {
                 const double nud = g.face_geo[((size_t)e * NFL + f) * DIM + d];
-                const double *ops = g.pairs + ((size_t)g.self_pair[e * NFL + f] * nB + i) * nB;
-                const double *opn = g.pairs + ((size_t)g.nbr_pair[e * NFL + f] * nB + i) * nB;
+                const double *ops = g.pairs + (size_t)g.self_pair[e * NFL + f] * nB * nB + i;
+                const double *opn = g.pairs + (size_t)g.nbr_pair[e * NFL + f] * nB * nB + i;
                 double s = 0.0;
-                for (int j = 0; j < nB; ++j) s += ops[j] * w[j] - opn[j] * wn[f * R + j];
+                #pragma unroll
+                for (int j = 0; j < nB; ++j) s += ops[(size_t)j * nB] * w[j] - opn[(size_t)j * nB] * wn[f * R + j];
                 acc -= nud * s;
             }
             acc *= g.inv_cinv;
@@ -337,9 +403,42 @@ __device__ __forceinline__ void dense_stage_body(const StageIO &io, const DenseG
     stage_output(io, e * R + r, u_own, acc);
 }
 
-template <int DIM, int NFL, int WAVE>
+template <int DIM, int NFL, int WAVE, int NB>
 __global__ void __launch_bounds__(256) dense_stage(const StageIO io, const DenseGeom g) {
-    dense_stage_body<DIM, NFL, WAVE>(io, g, blockIdx.x);
+    dense_stage_body<DIM, NFL, WAVE, NB>(io, g, blockIdx.x);
+}
+
+// basis sizes of the shapes the dense kernel serves, orders 1..5
+template <int DIM, int NFL> struct DenseSizes;
+template <> struct DenseSizes<1, 2> { static constexpr int nb[5] = {2, 3, 4, 5, 6}; };
+template <> struct DenseSizes<2, 3> { static constexpr int nb[5] = {3, 6, 10, 15, 21}; };
+template <> struct DenseSizes<2, 4> { static constexpr int nb[5] = {4, 9, 16, 25, 36}; };
+template <> struct DenseSizes<3, 4> { static constexpr int nb[5] = {4, 10, 20, 35, 56}; };
+template <> struct DenseSizes<3, 6> { static constexpr int nb[5] = {8, 27, 64, 125, 216}; };
+
+// calls f(std::integral_constant<int, NB>) for the runtime nB, if it is one of
+// the shape's sizes and fits the kernel (at most 256 coefficients per element);
+// returns false otherwise
+template <int DIM, int NFL, int WAVE, typename F>
+bool dense_dispatch(int nB, F &&f) {
+    using S = DenseSizes<DIM, NFL>;
+    constexpr int V = WAVE ? DIM + 1 : 1;
+    bool done = false;
+    auto one = [&](auto k) {
+        constexpr int NB = S::nb[decltype(k)::value];
+        if constexpr (V * NB <= 256) {
+            if (!done && nB == NB) {
+                f(std::integral_constant<int, NB>{});
+                done = true;
+            }
+        }
+    };
+    one(std::integral_constant<int, 0>{});
+    one(std::integral_constant<int, 1>{});
+    one(std::integral_constant<int, 2>{});
+    one(std::integral_constant<int, 3>{});
+    one(std::integral_constant<int, 4>{});
+    return done;
 }
 
 }  // namespace hgg
