@@ -70,7 +70,7 @@ __global__ void __launch_bounds__(256)
         const int slot = items[i].slot;
         __syncthreads();  // shared memory of the previous virtual block is free
         if (remaining[slot] <= 0) continue;
-        dense_stage_body<DIM, NFL, WAVE, NB>(items[i].io[parity[slot]], items[i].g, vb - items[i].block0);
+        dense_any_body<DIM, NFL, WAVE, NB>(items[i].io[parity[slot]], items[i].g, vb - items[i].block0);
     }
 }
 
@@ -300,9 +300,8 @@ int upload_class(hgg_batch *b, BatchClass &c) {
 template <int DIM, int NFL, int WAVE>
 void launch_grouped_dense(const hgg_batch *b, const BatchClass &c, int st, unsigned grid, cudaStream_t s) {
     const int nB = b->handles[c.slots[0]]->op.nB;
-    const int R = (WAVE ? DIM + 1 : 1) * nB;
-    const int threads = ((c.epb * R + 31) / 32) * 32;
-    const size_t smem = sizeof(double) * (size_t)c.epb * R * (1 + NFL);
+    const int threads = dense_threads(DIM, WAVE, nB, c.epb);
+    const size_t smem = dense_smem(DIM, NFL, WAVE, nB, c.epb);
     dense_dispatch<DIM, NFL, WAVE>(nB, [&](auto nbc) {
         constexpr int NB = decltype(nbc)::value;
         if (smem > 48 * 1024)
@@ -401,11 +400,13 @@ int tune_class(hgg_batch *b, BatchClass &c) {
     std::vector<std::pair<int, int>> cands;  // (epb, ctas_per_sm)
     const int ctas[] = {1, 2, 4, 8};
     if (c.kind == KIND_DENSE) {
-        const int R = dense_R(b->handles[c.slots[0]]);
+        const hgg_handle *h0 = b->handles[c.slots[0]];
+        const int wave = c.physics == HGG_PHYSICS_WAVE;
+        const int rows = dense_rows(c.dim, wave, h0->op.nB);
         const int nfl = c.shape == HGG_SHAPE_LINE ? 2 : (c.shape == HGG_SHAPE_TRIANGLE ? 3
                         : (c.shape == HGG_SHAPE_SQUARE || c.shape == HGG_SHAPE_TETRAHEDRON ? 4 : 6));
-        for (int epb : {1, 2, 4, 8, 16, 32}) {
-            if (epb * R > 256 || sizeof(double) * (size_t)epb * R * (1 + nfl) > 200 * 1024) continue;
+        for (int epb : {1, 2, 4, 8, 16, 32, 64}) {
+            if (epb * rows > 256 || dense_smem(c.dim, nfl, wave, h0->op.nB, epb) > 200 * 1024) continue;
             for (int cs : ctas) cands.push_back({epb, cs});
         }
     } else {
@@ -619,7 +620,7 @@ int hgg_batch_add(hgg_batch *b, hgg_handle *h, double dt, int32_t nsteps, int32_
         c.S = h->S;
         c.rk_a = h->rk_a;
         c.rk_b = h->rk_b;
-        c.epb = c.kind == KIND_DENSE ? std::max(1, 256 / dense_R(h)) : 1;
+        c.epb = c.kind == KIND_DENSE ? std::max(1, 256 / dense_rows(h->op.dim, h->op.physics == HGG_PHYSICS_WAVE, h->op.nB)) : 1;
         c.item_bytes = class_item_bytes(c);
         c.d_items.assign(c.S, nullptr);
         for (int st = 0; st < c.S; ++st)

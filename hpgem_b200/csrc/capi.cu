@@ -274,12 +274,12 @@ int launch_dense(hgg_handle *h, const StageIO &io) {
     const int V = WAVE ? DIM + 1 : 1;
     const int R = V * op.nB;
     if (R > 256) return fail(h, HGG_ERR_UNSUPPORTED, "dense kernel: more than 256 coefficients per element");
-    int epb = std::max(1, 256 / R);
+    int epb = std::max(1, 256 / dense_rows(DIM, WAVE, op.nB));
     DenseGeom g{h->d_vol, h->d_pairs, h->d_nbr, h->d_self, h->d_nbrp, h->d_mode,
                 h->d_elem_geo, h->d_face_geo, 1.0 / op.c_inv, op.nB, epb};
-    size_t smem = sizeof(double) * (size_t)epb * R * (1 + NFL);
+    const size_t smem = dense_smem(DIM, NFL, WAVE, op.nB, epb);
     int64_t blocks = (op.nE + epb - 1) / epb;
-    int threads = ((epb * R + 31) / 32) * 32;
+    const int threads = dense_threads(DIM, WAVE, op.nB, epb);
     const bool ok = dense_dispatch<DIM, NFL, WAVE>(op.nB, [&](auto nbc) {
         constexpr int NB = decltype(nbc)::value;
         if (smem > 48 * 1024)

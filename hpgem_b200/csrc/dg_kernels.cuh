@@ -403,9 +403,140 @@ __device__ __forceinline__ void dense_stage_body(const StageIO &io, const DenseG
     stage_output(io, e * R + r, u_own, acc);
 }
 
+// Acoustic wave in 2D and 3D: thread (el, i) produces row i of all DIM + 1
+// fields of element el.  The velocity rows of one basis row share the
+// pressure contractions (vol_c q and the face brackets S_f q - N_f q_n), so
+// they are formed once per row instead of once per velocity component; the
+// pressure row uses t_c = sum_d G[d][c] s_d and the normal jumps n . s of both
+// sides, formed once per element and column.
+template <int DIM, int NFL, int NB>
+__device__ __forceinline__ void wave_stage_body(const StageIO &io, const DenseGeom &g, int64_t block) {
+    constexpr int V = DIM + 1, R = V * NB, NX = DIM + 2 * NFL;
+    extern __shared__ double smem[];
+    const int epb = g.epb;
+    double *W = smem;                              // [epb][R]
+    double *WN = W + (size_t)epb * R;              // [epb][NFL][R]
+    double *X = WN + (size_t)epb * NFL * R;        // [epb][NX][NB]: t_c, then n . s self, then n . s neighbour
+    const int tid = threadIdx.x;
+    const int64_t e0 = block * epb;
+    const int el = tid / NB, i = tid % NB;
+    const int64_t e = e0 + el;
+    const bool active = el < epb && e < io.n_elements;
+
+    double u_own[V];
+    if (active) {
+#pragma unroll
+        for (int v = 0; v < V; ++v) {
+            const int64_t idx = e * R + v * NB + i;
+            u_own[v] = io.u[idx];
+            double w = u_own[v];
+            for (int j = 0; j < io.nin; ++j) w += io.cin[j] * io.kin[j][idx];
+            W[el * R + v * NB + i] = w;
+        }
+    }
+    for (int k = tid; k < epb * NFL * R; k += blockDim.x) {
+        const int l = k / (NFL * R), f = (k / R) % NFL, rr = k % R;
+        const int64_t ee = e0 + l;
+        double v = 0.0;
+        if (ee < io.n_elements) {
+            const int32_t n = g.nbr[ee * NFL + f];
+            if (n >= 0 && n < io.n_elements) v = stage_input(io, (int64_t)n * R + rr);
+            else atomicOr(io.status, 1);
+        }
+        WN[(size_t)(l * NFL + f) * R + rr] = v;
+    }
+    __syncthreads();
+    const double *w = W + el * R;
+    const double *wn = WN + (size_t)el * NFL * R;
+    double *x = X + (size_t)el * NX * NB;
+    if (active) {
+        const double *G = g.elem_geo + e * DIM * DIM;  // G[d][c] = (J^{-T})_{dc}
+#pragma unroll
+        for (int c = 0; c < DIM; ++c) {
+            double t = 0.0;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) t += G[d * DIM + c] * w[(d + 1) * NB + i];
+            x[c * NB + i] = t;
+        }
+#pragma unroll
+        for (int f = 0; f < NFL; ++f) {
+            const double *nu = g.face_geo + ((size_t)e * NFL + f) * DIM;
+            double a = 0.0, b = 0.0;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) {
+                a += nu[d] * w[(d + 1) * NB + i];
+                b += nu[d] * wn[f * R + (d + 1) * NB + i];
+            }
+            x[(DIM + f) * NB + i] = a;
+            x[(DIM + NFL + f) * NB + i] = b;
+        }
+    }
+    __syncthreads();
+    if (!active) return;
+
+    double P = 0.0, A[DIM], B[NFL];
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) {
+        const double *op = g.vol + (size_t)c * NB * NB + i;
+        double sp = 0.0, sa = 0.0;
+#pragma unroll
+        for (int j = 0; j < NB; ++j) {
+            const double o = op[(size_t)j * NB];
+            sp += o * x[c * NB + j];
+            sa += o * w[j];
+        }
+        P += sp;
+        A[c] = sa;
+    }
+#pragma unroll
+    for (int f = 0; f < NFL; ++f) {
+        const double *ops = g.pairs + (size_t)g.self_pair[e * NFL + f] * NB * NB + i;
+        const double *opn = g.pairs + (size_t)g.nbr_pair[e * NFL + f] * NB * NB + i;
+        const double *js = x + (DIM + f) * NB, *jn = x + (DIM + NFL + f) * NB;
+        double sp = 0.0, sb = 0.0;
+#pragma unroll
+        for (int j = 0; j < NB; ++j) {
+            const double os = ops[(size_t)j * NB], on = opn[(size_t)j * NB];
+            sp += os * js[j] - on * jn[j];
+            sb += os * w[j] - on * wn[f * R + j];
+        }
+        P -= sp;
+        B[f] = sb;
+    }
+    stage_output(io, e * R + i, u_own[0], P);
+    const double *G = g.elem_geo + e * DIM * DIM;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+        double acc = 0.0;
+#pragma unroll
+        for (int c = 0; c < DIM; ++c) acc += G[d * DIM + c] * A[c];
+#pragma unroll
+        for (int f = 0; f < NFL; ++f) acc -= g.face_geo[((size_t)e * NFL + f) * DIM + d] * B[f];
+        stage_output(io, e * R + (d + 1) * NB + i, u_own[d + 1], acc * g.inv_cinv);
+    }
+}
+
+// threads and dynamic shared memory of one dense-kernel block of `epb` elements
+__host__ __device__ inline int dense_rows(int dim, int wave, int nb) { return wave && dim >= 2 ? nb : (wave ? dim + 1 : 1) * nb; }
+__host__ __device__ inline int dense_threads(int dim, int wave, int nb, int epb) {
+    return ((epb * dense_rows(dim, wave, nb) + 31) / 32) * 32;
+}
+__host__ __device__ inline size_t dense_smem(int dim, int nfl, int wave, int nb, int epb) {
+    const int R = (wave ? dim + 1 : 1) * nb;
+    size_t d = (size_t)epb * R * (1 + nfl);
+    if (wave && dim >= 2) d += (size_t)epb * (dim + 2 * nfl) * nb;
+    return sizeof(double) * d;
+}
+
+template <int DIM, int NFL, int WAVE, int NB>
+__device__ __forceinline__ void dense_any_body(const StageIO &io, const DenseGeom &g, int64_t block) {
+    if constexpr (WAVE && DIM >= 2) wave_stage_body<DIM, NFL, NB>(io, g, block);
+    else dense_stage_body<DIM, NFL, WAVE, NB>(io, g, block);
+}
+
 template <int DIM, int NFL, int WAVE, int NB>
 __global__ void __launch_bounds__(256) dense_stage(const StageIO io, const DenseGeom g) {
-    dense_stage_body<DIM, NFL, WAVE, NB>(io, g, blockIdx.x);
+    dense_any_body<DIM, NFL, WAVE, NB>(io, g, blockIdx.x);
 }
 
 // basis sizes of the shapes the dense kernel serves, orders 1..5
