@@ -29,7 +29,8 @@ EXPORTED = ["hgg_create", "hgg_destroy", "hgg_last_error", "hgg_set_state", "hgg
             "hgg_batch_remove", "hgg_batch_step", "hgg_batch_synchronize", "hgg_batch_remaining",
             "hgg_batch_set_autotune", "hgg_batch_launch_count", "hgg_batch_num_classes",
             "hgg_server_start", "hgg_server_submit", "hgg_server_poll", "hgg_server_result_length",
-            "hgg_server_release", "hgg_server_times", "hgg_server_stats", "hgg_server_last_error",
+            "hgg_server_release", "hgg_server_times", "hgg_server_stats", "hgg_server_timing",
+            "hgg_server_last_error",
             "hgg_server_stop"]
 
 # void (*hgg_initial_fn)(const double *xyz, int64_t n_points, int32_t dim, double *values, void *user)
@@ -109,6 +110,7 @@ def load():
         "hgg_server_release": (ctypes.c_int, [B, ctypes.c_int64]),
         "hgg_server_times": (ctypes.c_int, [B, ctypes.c_int64, P]),
         "hgg_server_stats": (ctypes.c_int, [B, P]),
+        "hgg_server_timing": (ctypes.c_int, [B, P]),
         "hgg_server_last_error": (ctypes.c_char_p, [B]),
         "hgg_server_stop": (ctypes.c_int, [B]),
         "hgg_synchronize": (ctypes.c_int, [H]),

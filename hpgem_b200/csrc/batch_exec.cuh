@@ -130,6 +130,7 @@ struct BatchClass {
     int ctas_per_sm = 2;  // persistent CTAs per SM
     bool tuned = false;
     int tuned_bucket = -1;
+    bool table_dirty = true;  // members changed since the tables were uploaded
     // device tables: items [S][cap] (one array per stage), count and block total
     std::vector<void *> d_items;
     size_t item_bytes = 0;
@@ -174,6 +175,7 @@ struct hgg_batch {
     int *d_parity = nullptr, *d_remaining = nullptr, *d_status = nullptr;
     std::vector<BatchClass> classes;
     cudaGraphExec_t graph = nullptr;
+    std::vector<int> graph_sig;  // (class, epb, ctas per SM) of the captured step
     bool dirty = true;
     bool autotune = true;
     int64_t launches = 0;
@@ -345,8 +347,8 @@ void launch_grouped_slice(const hgg_batch *b, const BatchClass &c, int st, unsig
 
 // one stage of one class
 void launch_class_stage(hgg_batch *b, const BatchClass &c, int st, cudaStream_t s) {
-    const unsigned grid = (unsigned)std::max<int64_t>(
-        1, std::min<int64_t>(c.total_blocks, (int64_t)c.ctas_per_sm * b->num_sms));
+    // a fixed persistent grid: membership changes leave the launch (and the graph) as it is
+    const unsigned grid = (unsigned)(c.ctas_per_sm * b->num_sms);
     if (c.kind == KIND_SLICE) {
         if (c.mixed) launch_grouped_slice<float>(b, c, st, grid, s);
         else launch_grouped_slice<double>(b, c, st, grid, s);
@@ -398,16 +400,19 @@ int tune_class(hgg_batch *b, BatchClass &c) {
         }
     }
     std::vector<std::pair<int, int>> cands;  // (epb, ctas_per_sm)
-    const int ctas[] = {1, 2, 4, 8};
+    const int ctas[] = {2, 4, 8};
     if (c.kind == KIND_DENSE) {
+        // elements per block: the largest that fills 256 threads, and half of it
         const hgg_handle *h0 = b->handles[c.slots[0]];
         const int wave = c.physics == HGG_PHYSICS_WAVE;
         const int rows = dense_rows(c.dim, wave, h0->op.nB);
         const int nfl = c.shape == HGG_SHAPE_LINE ? 2 : (c.shape == HGG_SHAPE_TRIANGLE ? 3
                         : (c.shape == HGG_SHAPE_SQUARE || c.shape == HGG_SHAPE_TETRAHEDRON ? 4 : 6));
-        for (int epb : {1, 2, 4, 8, 16, 32, 64}) {
-            if (epb * rows > 256 || dense_smem(c.dim, nfl, wave, h0->op.nB, epb) > 200 * 1024) continue;
+        const int full = std::max(1, 256 / rows);
+        for (int epb : {full, std::max(1, full / 2)}) {
+            if (dense_smem(c.dim, nfl, wave, h0->op.nB, epb) > 200 * 1024) continue;
             for (int cs : ctas) cands.push_back({epb, cs});
+            if (full == 1) break;
         }
     } else {
         for (int cs : ctas) cands.push_back({c.epb, cs});
@@ -426,7 +431,7 @@ int tune_class(hgg_batch *b, BatchClass &c) {
         }
         c.ctas_per_sm = cs;
         float tmin = 1e30f;
-        for (int rep = 0; rep < 3; ++rep) {
+        for (int rep = 0; rep < 2; ++rep) {
             cudaEventRecord(e0, b->stream);
             launch_class_stage(b, c, 0, b->stream);
             cudaEventRecord(e1, b->stream);
@@ -470,30 +475,52 @@ void release_batch_graph(hgg_batch *b) {
     }
 }
 
-// tables of every class, autotuning of untuned classes, capture of one step
+// tables of the classes whose members changed, autotuning of classes with
+// enough work and no tuned shape for their size, and a new capture of one step
+// only when the launch shapes changed
 int prepare_batch(hgg_batch *b) {
     if (!b->dirty && b->graph) return 0;
-    release_batch_graph(b);
-    // current counters (tuning below overwrites them for a moment)
-    int rc0 = read_counters(b);
-    if (rc0) return rc0;
+    bool counters_read = false;
     for (auto &c : b->classes) {
         if (c.slots.empty()) continue;
-        int rc = upload_class(b, c);
-        if (rc) return rc;
+        if (c.table_dirty) {
+            int rc = upload_class(b, c);
+            if (rc) return rc;
+            c.table_dirty = false;
+        }
         // tuning launches stage 1 of the members (every member must have steps left for it
-        // to run); a one-stage tableau's first stage is its final update, so it is not tuned
-        if (b->autotune && c.S > 1 && (!c.tuned || c.tuned_bucket != size_bucket(c.total_elements))) {
+        // to run); a one-stage tableau's first stage is its final update, so it is not tuned;
+        // classes with less than two blocks per SM keep the default shape
+        const int bucket = size_bucket(c.total_elements);
+        if (b->autotune && c.S > 1 && c.total_blocks >= 2 * b->num_sms && (!c.tuned || c.tuned_bucket != bucket)) {
+            if (!counters_read) {
+                int rc = read_counters(b);  // the values the tuning below overwrites for a moment
+                if (rc) return rc;
+                counters_read = true;
+            }
             std::vector<int> ones(b->cap, 1);
             HGG_BCUDA(b, cudaMemcpyAsync(b->d_remaining, ones.data(), sizeof(int) * b->cap, cudaMemcpyHostToDevice,
                                          b->stream));
-            rc = tune_class(b, c);
+            int rc = tune_class(b, c);
             if (rc) return rc;
             HGG_BCUDA(b, cudaMemcpyAsync(b->d_remaining, b->remaining_host.data(), sizeof(int) * b->cap,
                                          cudaMemcpyHostToDevice, b->stream));
             HGG_BCUDA(b, cudaStreamSynchronize(b->stream));
         }
     }
+    std::vector<int> sig;
+    for (size_t i = 0; i < b->classes.size(); ++i) {
+        const auto &c = b->classes[i];
+        if (c.slots.empty()) continue;
+        sig.push_back((int)i);
+        sig.push_back(c.epb);
+        sig.push_back(c.ctas_per_sm);
+    }
+    if (b->graph && sig == b->graph_sig) {
+        b->dirty = false;
+        return 0;
+    }
+    release_batch_graph(b);
     cudaGraph_t g = nullptr;
     HGG_BCUDA(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
     const int64_t before = b->launches;
@@ -512,6 +539,7 @@ int prepare_batch(hgg_batch *b) {
     cudaError_t ie = cudaGraphInstantiate(&b->graph, g, 0);
     cudaGraphDestroy(g);
     if (ie != cudaSuccess) return bfail(b, HGG_ERR_CUDA, std::string("batch graph instantiate: ") + cudaGetErrorString(ie));
+    b->graph_sig = sig;
     b->dirty = false;
     return 0;
 }
@@ -633,6 +661,7 @@ int hgg_batch_add(hgg_batch *b, hgg_handle *h, double dt, int32_t nsteps, int32_
         ci = (int)b->classes.size() - 1;
     }
     b->classes[ci].slots.push_back(free_slot);
+    b->classes[ci].table_dirty = true;
     b->handles[free_slot] = h;
     b->dt[free_slot] = dt;
     b->base[free_slot] = h->cur;
@@ -657,6 +686,7 @@ int hgg_batch_remove(hgg_batch *b, int32_t slot) {
     h->cur = b->parity_host[slot] ? 1 - b->base[slot] : b->base[slot];
     BatchClass &c = b->classes[b->cls[slot]];
     c.slots.erase(std::find(c.slots.begin(), c.slots.end(), slot));
+    c.table_dirty = true;
     b->handles[slot] = nullptr;
     b->cls[slot] = -1;
     b->remaining_host[slot] = 0;

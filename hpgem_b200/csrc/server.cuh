@@ -69,6 +69,7 @@ struct hgg_server {
     int gpu_error = 0;
     // counters
     int64_t completed = 0, dof_updates = 0, chunks = 0;
+    double t_step = 0, t_members = 0, t_idle = 0;  // GPU thread: stepping, joining/retiring, waiting
 };
 
 namespace {
@@ -179,6 +180,7 @@ void gpu_loop(hgg_server *s) {
     std::vector<ServerRequest *> running;
     for (;;) {
         std::vector<ServerRequest *> joining;
+        const double t_wait0 = now_s();
         {
             std::unique_lock<std::mutex> lk(s->mu);
             if (running.empty())
@@ -190,6 +192,11 @@ void gpu_loop(hgg_server *s) {
                 joining.push_back(s->ready.front());
                 s->ready.pop_front();
             }
+        }
+        const double t_join0 = now_s();
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->t_idle += t_join0 - t_wait0;
         }
         for (ServerRequest *r : joining) {
             int32_t slot = -1;
@@ -219,8 +226,15 @@ void gpu_loop(hgg_server *s) {
             if (left > 0) chunk = std::min(chunk, left);
         }
         chunk = std::max(chunk, 1);
+        const double t_step0 = now_s();
         int rc = hgg_batch_step(s->batch, chunk);
         if (rc == 0) rc = hgg_batch_synchronize(s->batch);
+        const double t_step1 = now_s();
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->t_members += t_step0 - t_join0;
+            s->t_step += t_step1 - t_step0;
+        }
         if (rc) {
             std::lock_guard<std::mutex> lk(s->mu);
             s->gpu_error = rc;
@@ -268,6 +282,8 @@ void gpu_loop(hgg_server *s) {
             s->cv_done.notify_all();
         }
         running.swap(still);
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->t_members += now_s() - t_step1;
     }
 }
 
@@ -417,6 +433,17 @@ int hgg_server_stats(hgg_server *s, int64_t *stats4) {
     stats4[1] = s->dof_updates;
     stats4[2] = s->chunks;
     stats4[3] = s->reserved;
+    return 0;
+}
+
+// GPU-thread seconds: stepping (launches and the wait for them), joining and
+// retiring solves (tables, graph, copies back, frees), waiting for work
+int hgg_server_timing(hgg_server *s, double *t3) {
+    if (!s || !t3) return sfail(s, HGG_ERR_INVALID, "null argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    t3[0] = s->t_step;
+    t3[1] = s->t_members;
+    t3[2] = s->t_idle;
     return 0;
 }
 

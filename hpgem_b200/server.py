@@ -85,7 +85,11 @@ class Server:
     def stats(self):
         st = np.zeros(4, dtype=np.int64)
         self._check(self._lib.hgg_server_stats(self._raw, ctypes.c_void_p(st.ctypes.data)))
-        return dict(completed=int(st[0]), dof_updates=int(st[1]), chunks=int(st[2]), reserved_bytes=int(st[3]))
+        t = np.zeros(3)
+        self._check(self._lib.hgg_server_timing(self._raw, ctypes.c_void_p(t.ctypes.data)))
+        return dict(completed=int(st[0]), dof_updates=int(st[1]), chunks=int(st[2]), reserved_bytes=int(st[3]),
+                    gpu_thread_step_s=float(t[0]), gpu_thread_members_s=float(t[1]),
+                    gpu_thread_idle_s=float(t[2]))
 
     def stop(self):
         if self._raw:

@@ -326,6 +326,10 @@ int hgg_server_times(hgg_server *s, int64_t id, double *t4);
 /* Completed solves, their DoF-updates, chunks stepped, device bytes reserved now. */
 int hgg_server_stats(hgg_server *s, int64_t *stats4);
 
+/* GPU-thread seconds so far: stepping (launches and the wait for them),
+ * joining and retiring solves (tables, graph, copies back, frees), idle. */
+int hgg_server_timing(hgg_server *s, double *t3);
+
 const char *hgg_server_last_error(hgg_server *s);
 
 /* Waits for every submitted solve, stops the threads, frees the server. */
