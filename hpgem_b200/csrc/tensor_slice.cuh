@@ -83,9 +83,30 @@ __device__ __forceinline__ CT slice_flux(int md, CT sg, CT self, CT nbr) {
 // update, fixed at compile time for the common Runge-Kutta stages (so every
 // load loop unrolls and all loads of a phase are in flight together), or -1
 // for a count read from io.
+// L2 prefetch of `bytes` (a multiple of 16) from a 16-byte aligned global address
+__device__ __forceinline__ void prefetch_l2(const void *p, uint32_t bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
+// Tiles of one vector are contiguous runs (TILE coefficients), so the inputs a
+// later block will read are a handful of bulk prefetches.
+template <typename KT>
+__device__ __forceinline__ void prefetch_tile(const StageIOT<KT> &io, const double *geo, int64_t tile, int nin,
+                                              int nfin) {
+    constexpr int TILE = SliceShape::TILE;
+    prefetch_l2(io.u + tile * TILE, TILE * sizeof(double));
+    for (int j = 0; j < nin; ++j) prefetch_l2(io.kin[j] + tile * TILE, TILE * sizeof(KT));
+    if (io.unew)
+        for (int j = 0; j < nfin; ++j) prefetch_l2(io.kfin[j] + tile * TILE, TILE * sizeof(KT));
+    prefetch_l2(geo + tile * SliceShape::TE * SliceShape::GR, SliceShape::TE * SliceShape::GR * sizeof(double));
+}
+
+// prefetch_ahead: this block asks L2 for the inputs of tile + prefetch_ahead (the
+// tile a block of the next resident wave runs), 0 for none; n_tiles bounds it.
 template <typename KT, int NIN, int NFIN>
 __device__ __forceinline__ void tensor_slice_body(const StageIOT<KT> &io, const double *__restrict__ geo,
-                                                  const SliceOps &op, int64_t tile) {
+                                                  const SliceOps &op, int64_t tile, int64_t prefetch_ahead = 0,
+                                                  int64_t n_tiles = 0) {
     using CT = KT;  // contraction type
     constexpr int TE = SliceShape::TE, WS = SliceShape::WS, ZS = SliceShape::ZS, GR = SliceShape::GR;
     constexpr int TILE = SliceShape::TILE;
@@ -105,6 +126,8 @@ __device__ __forceinline__ void tensor_slice_body(const StageIOT<KT> &io, const 
     const int nfin = NFIN >= 0 ? NFIN : io.nfin;
 
     // ---- phase 1: geometry records, own slice, stage input -------------------------
+    if (prefetch_ahead > 0 && threadIdx.x == 0 && tile + prefetch_ahead < n_tiles)
+        prefetch_tile(io, geo, tile + prefetch_ahead, nin, nfin);
     for (int i = threadIdx.x; i < TE * GR; i += SliceShape::THREADS) G[i] = ldg_f64(geo + t0 * GR + i);
     CT w[16];
     {
@@ -249,8 +272,8 @@ __device__ __forceinline__ void tensor_slice_body(const StageIOT<KT> &io, const 
 // One block per 32-element tile of one problem.
 template <typename KT, int NIN, int NFIN>
 __global__ void __launch_bounds__(SliceShape::THREADS, sizeof(KT) == 4 ? 5 : 4)
-    tensor_slice(const StageIOT<KT> io, const double *__restrict__ geo, const SliceOps op) {
-    tensor_slice_body<KT, NIN, NFIN>(io, geo, op, blockIdx.x);
+    tensor_slice(const StageIOT<KT> io, const double *__restrict__ geo, const SliceOps op, int64_t prefetch_ahead) {
+    tensor_slice_body<KT, NIN, NFIN>(io, geo, op, blockIdx.x, prefetch_ahead, gridDim.x);
 }
 
 }  // namespace hgg
