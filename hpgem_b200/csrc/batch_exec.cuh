@@ -90,7 +90,7 @@ __global__ void __launch_bounds__(EPB *TensorConsts<P, DIM>::NB)
 }
 
 template <typename KT, int NIN, int NFIN>
-__global__ void __launch_bounds__(SliceShape::THREADS, sizeof(KT) == 4 ? 5 : 4)
+__global__ void __launch_bounds__(SliceShape::THREADS, sizeof(KT) == 4 ? 5 : (NFIN == 0 ? 5 : 4))
     grouped_slice(const SliceItem<KT> *items, const int *n_items, const int64_t *total, const int *parity,
                   const int *remaining, const SliceOps op) {
     const int n = *n_items;
