@@ -185,10 +185,11 @@ int launch_slice(hgg_handle *h, const StageIOT<KT> &io) {
     const int64_t blocks = (op.nE + SliceShape::TE - 1) / SliceShape::TE;
     const dim3 grid((unsigned)blocks), block(SliceShape::THREADS);
     const bool fin = io.unew != nullptr;
-    // FP32 form: each block asks L2 for the tile a block of the next resident wave runs
-    // (5 blocks per SM resident); measured 4 % faster for it, 1 % slower for the FP64 form,
-    // whose 4 resident blocks per SM already keep enough loads in flight
-    const int64_t ahead = sizeof(KT) == 4 ? (int64_t)h->num_sms * 5 : 0;
+    // each block asks L2 for the inputs of the tile a block of the next resident wave runs
+    // (5 blocks per SM resident): measured 4 % faster per RK4 step for the FP32 form and
+    // 2-3 % for the FP64 form's first three stages; the FP64 final stage (4 resident
+    // blocks, three more input vectors) measured slower with it and goes without
+    const int64_t ahead = (sizeof(KT) == 4 || !io.unew) ? (int64_t)h->num_sms * 5 : 0;
     if (io.nin == 0 && (!fin || io.nfin == 0))
         tensor_slice<KT, 0, 0><<<grid, block, 0, h->stream>>>(io, h->d_slice_geo, sops, ahead);
     else if (io.nin == 1 && (!fin || io.nfin == 0))
