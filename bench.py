@@ -353,9 +353,10 @@ def run_ours(args):
             "forms": forms}
     if rank == 0 and world == 1 and not args.no_batched:
         line["tet_wave"] = run_tet_wave(args, stream)
-        line["batched"] = run_batched(args, stream)
+        line["batched"] = run_batched_forms(args, stream)
     if rank == 0 and world == 1 and not args.no_served:
-        line["served"] = run_served(args)
+        line["served"] = run_served(args, 0)
+        line["served"]["forms"] = {"fp32_mixed": run_served(args, 1)}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, sample = cpu_sample_rate()
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
@@ -367,7 +368,7 @@ def run_ours(args):
         print(json.dumps(line), flush=True)
 
 
-def run_batched(args, stream):
+def run_batched(args, stream, precision=0):
     """512 independent 2D advection problems (quads/triangles, p 1..5, 8^2..128^2, per-problem
     velocity and CFL dt), RK4, 100 steps each, advanced together by one batch."""
     import torch
@@ -377,7 +378,7 @@ def run_batched(args, stream):
 
     specs = workloads.batched_problems()
     t0 = time.perf_counter()
-    solvers = [workloads.make_solver(sp) for sp in specs]
+    solvers = [workloads.make_solver(sp, precision=precision) for sp in specs]
     setup_s = time.perf_counter() - t0
     total_dof = sum(workloads.dof(sp) for sp in specs)
     warm = 3
@@ -410,15 +411,24 @@ def run_batched(args, stream):
     finite = all(np.isfinite(o).all() for o in outs)
     classes = batch.num_classes
     batch.close()
-    return {"workload": "512 2D advection problems, quads/triangles, p 1..5, 8^2..128^2 cells, "
-                        "RK4, 100 steps each, seed 4",
-            "value": total_dof * steps / wall, "unit": UNIT, "dtype": "f64", "problems": len(specs),
-            "dof": total_dof, "steps": steps, "wall_s": wall, "kernel_classes": classes,
-            "gpu_launches": int(launches), "host_setup_s": setup_s,
-            "timing": "host wall clock around batch step + synchronize (device idle before)",
-            "e2e": {"value": total_dof * steps / e2e, "unit": UNIT, "wall_s": e2e,
-                    "h2d_bytes": 8 * total_dof, "d2h_bytes": 8 * total_dof, "finite": bool(finite)},
-            "form_note": "FP64: the FP32-mixed form has kernels for hexahedra of order 3 only"}
+    res = {"workload": "512 2D advection problems, quads/triangles, p 1..5, 8^2..128^2 cells, "
+                       "RK4, 100 steps each, seed 4",
+           "value": total_dof * steps / wall, "unit": UNIT, "dtype": "f32-mixed" if precision else "f64",
+           "problems": len(specs), "dof": total_dof, "steps": steps, "wall_s": wall, "kernel_classes": classes,
+           "gpu_launches": int(launches), "host_setup_s": setup_s,
+           "timing": "host wall clock around batch step + synchronize (device idle before)",
+           "e2e": {"value": total_dof * steps / e2e, "unit": UNIT, "wall_s": e2e,
+                   "h2d_bytes": 8 * total_dof, "d2h_bytes": 8 * total_dof, "finite": bool(finite)}}
+    return res, outs, solvers
+
+
+def run_batched_forms(args, stream):
+    """The batched set in both forms; the mixed form's error against the FP64 result."""
+    r64, o64, s64 = run_batched(args, stream, 0)
+    r32, o32, _ = run_batched(args, stream, 1)
+    r32["max_rel_coef_diff_vs_fp64"] = max(float(np.abs(a - b).max() / np.abs(b).max()) for a, b in zip(o32, o64))
+    r32["max_l2_distance_to_fp64"] = max(s.l2Distance(a, b) for s, a, b in zip(s64, o32, o64))
+    return dict(r64, forms={"fp32_mixed": r32})
 
 
 def run_tet_wave(args, stream):
@@ -443,31 +453,42 @@ def run_tet_wave(args, stream):
         return np.concatenate([q[:, None], np.zeros((len(x), 3))], axis=1)
 
     d = hpgem_b200.structured_description([32, 32, 32], [0, 0, 0], [1, 1, 1], True, True)
-    s = hpgem_b200.AcousticWave(3, 2, c_inv=1.0, tableau="RK4_4").readMesh(d)
-    h = s.handle
-    h.set_stream(stream.cuda_stream)
-    h.set_store_last_stage(False)
-    s.setInitialSolution(p0)
-    t = h.step(0.0, 5e-4, 3)
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    steps = 20
-    launches0 = h.launch_count
-    e0.record(stream)
-    h.step(t, 5e-4, steps)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / steps
-    n = h.vector_length
-    fin = bool(np.isfinite(h.get_state(0)).all())
-    return {"workload": "3D acoustic wave, 32^3 x 5 periodic tetrahedra, p = 2, central flux, RK4, "
-                        "dt = 5e-4, seeded 3-mode pressure", "value": n / (ms / 1e3), "unit": UNIT,
-            "dtype": "f64", "dof": n, "ms_per_step": ms, "steps": steps,
-            "gpu_launches": int(h.launch_count - launches0), "finite": fin,
-            "kernel": "dense_stage<3,4,1,10> (wave rows)"}
+    out = {}
+    sols = {}
+    for name, prec in (("fp64", 0), ("fp32_mixed", 1)):
+        s = hpgem_b200.AcousticWave(3, 2, c_inv=1.0, tableau="RK4_4", precision=prec).readMesh(d)
+        h = s.handle
+        h.set_stream(stream.cuda_stream)
+        h.set_store_last_stage(False)
+        s.setInitialSolution(p0)
+        t = h.step(0.0, 5e-4, 3)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        steps = 20
+        launches0 = h.launch_count
+        e0.record(stream)
+        h.step(t, 5e-4, steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        n = h.vector_length
+        sols[name] = (s, s.getTimeIntegrationVector(0))
+        out[name] = {"value": n / (ms / 1e3), "unit": UNIT, "dof": n, "ms_per_step": ms, "steps": steps,
+                     "gpu_launches": int(h.launch_count - launches0),
+                     "finite": bool(np.isfinite(sols[name][1]).all())}
+    s64, u64 = sols["fp64"]
+    u32 = sols["fp32_mixed"][1]
+    out["fp32_mixed"]["l2_distance_to_fp64"] = s64.l2Distance(u32, u64)
+    out["fp32_mixed"]["max_rel_coef_diff_vs_fp64"] = float(np.abs(u32 - u64).max() / np.abs(u64).max())
+    res = {"workload": "3D acoustic wave, 32^3 x 5 periodic tetrahedra, p = 2, central flux, RK4, "
+                       "dt = 5e-4, seeded 3-mode pressure, 23 steps", "dtype": "f64",
+           "kernel": "dense_stage<KT,3,4,1,10> (wave rows)"}
+    res.update(out["fp64"])
+    res["forms"] = {"fp32_mixed": out["fp32_mixed"]}
+    return res
 
 
-def run_served(args):
+def run_served(args, precision=0):
     """Poisson stream (200 requests/s, seed 5) of 2D/3D advection and acoustic-wave solves,
     1e3..2e6 DoF, p 1..4, 50..2000 steps, replayed in real time into the server."""
     import hpgem_b200
@@ -494,7 +515,7 @@ def run_served(args):
         else:
             fn, nv = (lambda x, u0=u0, d=d: np.concatenate([u0(x)[:, None], np.zeros((len(x), d))], axis=1)), d + 1
         ids.append(server.submit(desc(sp), sp["order"], sp["physics"], sp["params"], sp["dt"], sp["steps"],
-                                 initial=fn, n_vars=nv))
+                                 initial=fn, n_vars=nv, precision=precision))
     lat, done_t, sub_t = [], [], []
     for rid in ids:
         ok, _, l = server.poll(rid, wait=True, result=False)
@@ -509,7 +530,7 @@ def run_served(args):
     lat = np.array(lat)
     return {"workload": "Poisson stream, 200 requests/s, %d requests, seed 5: 2D/3D advection and "
                         "acoustic wave, 1e3..2e6 DoF, p 1..4, 50..2000 steps" % len(specs),
-            "value": stats["dof_updates"] / span, "unit": UNIT, "dtype": "f64",
+            "value": stats["dof_updates"] / span, "unit": UNIT, "dtype": "f32-mixed" if precision else "f64",
             "requests": len(specs), "p50_latency_s": float(np.percentile(lat, 50)),
             "p99_latency_s": float(np.percentile(lat, 99)), "mean_latency_s": float(lat.mean()),
             "span_s": span, "dof_updates": stats["dof_updates"], "chunks": stats["chunks"],
@@ -518,8 +539,7 @@ def run_served(args):
             "setup_threads": setup_threads, "budget_bytes": 48 << 30,
             "offered_dof_updates_per_s": sum(workloads.dof(sp) * sp["steps"] for sp in specs)
             / max(specs[-1]["arrival"], 1e-9),
-            "timing": "host steady clock, latency = done - submit (set-up, queueing, steps, copy back)",
-            "form_note": "FP64: the FP32-mixed form has kernels for hexahedra of order 3 only"}
+            "timing": "host steady clock, latency = done - submit (set-up, queueing, steps, copy back)"}
 
 
 def main():

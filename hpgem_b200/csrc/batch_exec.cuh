@@ -27,14 +27,16 @@
 
 namespace hgg {
 
+template <typename KT>
 struct DenseItem {
-    StageIO io[2];  // [parity]: from sol[base] / from sol[1 - base]
+    StageIOT<KT> io[2];  // [parity]: from sol[base] / from sol[1 - base]
     DenseGeom g;
     int64_t block0;  // first virtual block
     int slot;
 };
+template <typename KT>
 struct TensorItem {
-    StageIO io[2];
+    StageIOT<KT> io[2];
     TensorGeom geo;
     int64_t block0;
     int slot;
@@ -59,9 +61,9 @@ __device__ __forceinline__ int find_item(const Item *items, int n, int64_t vb) {
     return lo;
 }
 
-template <int DIM, int NFL, int WAVE, int NB>
+template <typename KT, int DIM, int NFL, int WAVE, int NB>
 __global__ void __launch_bounds__(256)
-    grouped_dense(const DenseItem *items, const int *n_items, const int64_t *total, const int *parity,
+    grouped_dense(const DenseItem<KT> *items, const int *n_items, const int64_t *total, const int *parity,
                   const int *remaining) {
     const int n = *n_items;
     const int64_t nb = *total;
@@ -70,13 +72,13 @@ __global__ void __launch_bounds__(256)
         const int slot = items[i].slot;
         __syncthreads();  // shared memory of the previous virtual block is free
         if (remaining[slot] <= 0) continue;
-        dense_any_body<DIM, NFL, WAVE, NB>(items[i].io[parity[slot]], items[i].g, vb - items[i].block0);
+        dense_any_body<KT, DIM, NFL, WAVE, NB>(items[i].io[parity[slot]], items[i].g, vb - items[i].block0);
     }
 }
 
-template <int P, int DIM, int EPB>
+template <typename KT, int P, int DIM, int EPB>
 __global__ void __launch_bounds__(EPB *TensorConsts<P, DIM>::NB)
-    grouped_tensor(const TensorItem *items, const int *n_items, const int64_t *total, const int *parity,
+    grouped_tensor(const TensorItem<KT> *items, const int *n_items, const int64_t *total, const int *parity,
                    const int *remaining, const TensorConsts<P, DIM> tc) {
     const int n = *n_items;
     const int64_t nb = *total;
@@ -85,7 +87,7 @@ __global__ void __launch_bounds__(EPB *TensorConsts<P, DIM>::NB)
         const int slot = items[i].slot;
         __syncthreads();
         if (remaining[slot] <= 0) continue;
-        tensor_stage_body<P, DIM, EPB>(items[i].io[parity[slot]], items[i].geo, tc, vb - items[i].block0);
+        tensor_stage_body<KT, P, DIM, EPB>(items[i].io[parity[slot]], items[i].geo, tc, vb - items[i].block0);
     }
 }
 
@@ -227,14 +229,14 @@ int64_t item_blocks(const BatchClass &c, const hgg_handle *h) {
 }
 
 size_t class_item_bytes(const BatchClass &c) {
-    if (c.kind == KIND_DENSE) return sizeof(DenseItem);
-    if (c.kind == KIND_TENSOR) return sizeof(TensorItem);
+    if (c.kind == KIND_DENSE) return c.mixed ? sizeof(DenseItem<float>) : sizeof(DenseItem<double>);
+    if (c.kind == KIND_TENSOR) return c.mixed ? sizeof(TensorItem<float>) : sizeof(TensorItem<double>);
     return c.mixed ? sizeof(SliceItem<float>) : sizeof(SliceItem<double>);
 }
 
 DenseGeom dense_geom(const hgg_handle *h, int epb) {
     const HostOperators &op = h->op;
-    return DenseGeom{h->d_vol, h->d_pairs, h->d_nbr, h->d_self, h->d_nbrp, h->d_mode,
+    return DenseGeom{h->d_vol, h->d_pairs, h->d_vol_f, h->d_pairs_f, h->d_nbr, h->d_self, h->d_nbrp, h->d_mode,
                      h->d_elem_geo, h->d_face_geo, 1.0 / op.c_inv, op.nB, epb};
 }
 
@@ -249,17 +251,17 @@ void fill_items(const hgg_batch *b, const BatchClass &c, int stage, std::vector<
         const int base = b->base[slot];
         unsigned char *dst = buf.data() + m * c.item_bytes;
         if (c.kind == KIND_DENSE) {
-            DenseItem it{};
+            DenseItem<KT> it{};
             for (int par = 0; par < 2; ++par)
-                it.io[par] = make_stage_io<double>(h, par ? 1 - base : base, b->dt[slot], stage, b->d_status);
+                it.io[par] = make_stage_io<KT>(h, par ? 1 - base : base, b->dt[slot], stage, b->d_status);
             it.g = dense_geom(h, c.epb);
             it.block0 = block0;
             it.slot = slot;
             std::memcpy(dst, &it, sizeof(it));
         } else if (c.kind == KIND_TENSOR) {
-            TensorItem it{};
+            TensorItem<KT> it{};
             for (int par = 0; par < 2; ++par)
-                it.io[par] = make_stage_io<double>(h, par ? 1 - base : base, b->dt[slot], stage, b->d_status);
+                it.io[par] = make_stage_io<KT>(h, par ? 1 - base : base, b->dt[slot], stage, b->d_status);
             it.geo = TensorGeom{h->d_ahat, h->d_tnbr, h->d_tmode, h->d_tsigma};
             it.block0 = block0;
             it.slot = slot;
@@ -299,19 +301,25 @@ int upload_class(hgg_batch *b, BatchClass &c) {
     return 0;
 }
 
-template <int DIM, int NFL, int WAVE>
+template <typename KT, int DIM, int NFL, int WAVE>
 void launch_grouped_dense(const hgg_batch *b, const BatchClass &c, int st, unsigned grid, cudaStream_t s) {
     const int nB = b->handles[c.slots[0]]->op.nB;
     const int threads = dense_threads(DIM, WAVE, nB, c.epb);
-    const size_t smem = dense_smem(DIM, NFL, WAVE, nB, c.epb);
     dense_dispatch<DIM, NFL, WAVE>(nB, [&](auto nbc) {
         constexpr int NB = decltype(nbc)::value;
+        const size_t smem = dense_smem(DIM, NFL, WAVE, NB, c.epb, sizeof(DenseCT<KT, NB>));
         if (smem > 48 * 1024)
-            cudaFuncSetAttribute(grouped_dense<DIM, NFL, WAVE, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            cudaFuncSetAttribute(grouped_dense<KT, DIM, NFL, WAVE, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem);
-        grouped_dense<DIM, NFL, WAVE, NB><<<grid, threads, smem, s>>>(
-            static_cast<const DenseItem *>(c.d_items[st]), c.d_n, c.d_total, b->d_parity, b->d_remaining);
+        grouped_dense<KT, DIM, NFL, WAVE, NB><<<grid, threads, smem, s>>>(
+            static_cast<const DenseItem<KT> *>(c.d_items[st]), c.d_n, c.d_total, b->d_parity, b->d_remaining);
     });
+}
+
+template <int DIM, int NFL, int WAVE>
+void launch_grouped_dense_any(const hgg_batch *b, const BatchClass &c, int st, unsigned grid, cudaStream_t s) {
+    if (c.mixed) launch_grouped_dense<float, DIM, NFL, WAVE>(b, c, st, grid, s);
+    else launch_grouped_dense<double, DIM, NFL, WAVE>(b, c, st, grid, s);
 }
 
 template <int P, int DIM>
@@ -319,8 +327,12 @@ void launch_grouped_tensor(const hgg_batch *b, const BatchClass &c, int st, unsi
     constexpr int NB = TensorConsts<P, DIM>::NB;
     constexpr int EPB = (256 / NB) > 0 ? (256 / NB) : 1;
     const TensorConsts<P, DIM> tc = tensor_consts<P, DIM>(b->handles[c.slots[0]]->op);
-    grouped_tensor<P, DIM, EPB><<<grid, EPB * NB, 0, s>>>(static_cast<const TensorItem *>(c.d_items[st]), c.d_n,
-                                                         c.d_total, b->d_parity, b->d_remaining, tc);
+    if (c.mixed)
+        grouped_tensor<float, P, DIM, EPB><<<grid, EPB * NB, 0, s>>>(
+            static_cast<const TensorItem<float> *>(c.d_items[st]), c.d_n, c.d_total, b->d_parity, b->d_remaining, tc);
+    else
+        grouped_tensor<double, P, DIM, EPB><<<grid, EPB * NB, 0, s>>>(
+            static_cast<const TensorItem<double> *>(c.d_items[st]), c.d_n, c.d_total, b->d_parity, b->d_remaining, tc);
 }
 
 template <typename KT>
@@ -363,11 +375,11 @@ void launch_class_stage(hgg_batch *b, const BatchClass &c, int st, cudaStream_t 
     } else {
         const bool wave = c.physics == HGG_PHYSICS_WAVE;
         switch (c.shape) {
-            case HGG_SHAPE_LINE: wave ? launch_grouped_dense<1, 2, 1>(b, c, st, grid, s) : launch_grouped_dense<1, 2, 0>(b, c, st, grid, s); break;
-            case HGG_SHAPE_TRIANGLE: wave ? launch_grouped_dense<2, 3, 1>(b, c, st, grid, s) : launch_grouped_dense<2, 3, 0>(b, c, st, grid, s); break;
-            case HGG_SHAPE_SQUARE: wave ? launch_grouped_dense<2, 4, 1>(b, c, st, grid, s) : launch_grouped_dense<2, 4, 0>(b, c, st, grid, s); break;
-            case HGG_SHAPE_TETRAHEDRON: wave ? launch_grouped_dense<3, 4, 1>(b, c, st, grid, s) : launch_grouped_dense<3, 4, 0>(b, c, st, grid, s); break;
-            case HGG_SHAPE_CUBE: wave ? launch_grouped_dense<3, 6, 1>(b, c, st, grid, s) : launch_grouped_dense<3, 6, 0>(b, c, st, grid, s); break;
+            case HGG_SHAPE_LINE: wave ? launch_grouped_dense_any<1, 2, 1>(b, c, st, grid, s) : launch_grouped_dense_any<1, 2, 0>(b, c, st, grid, s); break;
+            case HGG_SHAPE_TRIANGLE: wave ? launch_grouped_dense_any<2, 3, 1>(b, c, st, grid, s) : launch_grouped_dense_any<2, 3, 0>(b, c, st, grid, s); break;
+            case HGG_SHAPE_SQUARE: wave ? launch_grouped_dense_any<2, 4, 1>(b, c, st, grid, s) : launch_grouped_dense_any<2, 4, 0>(b, c, st, grid, s); break;
+            case HGG_SHAPE_TETRAHEDRON: wave ? launch_grouped_dense_any<3, 4, 1>(b, c, st, grid, s) : launch_grouped_dense_any<3, 4, 0>(b, c, st, grid, s); break;
+            case HGG_SHAPE_CUBE: wave ? launch_grouped_dense_any<3, 6, 1>(b, c, st, grid, s) : launch_grouped_dense_any<3, 6, 0>(b, c, st, grid, s); break;
         }
     }
     b->launches++;
@@ -410,7 +422,7 @@ int tune_class(hgg_batch *b, BatchClass &c) {
                         : (c.shape == HGG_SHAPE_SQUARE || c.shape == HGG_SHAPE_TETRAHEDRON ? 4 : 6));
         const int full = std::max(1, 256 / rows);
         for (int epb : {full, std::max(1, full / 2)}) {
-            if (dense_smem(c.dim, nfl, wave, h0->op.nB, epb) > 200 * 1024) continue;
+            if (dense_smem(c.dim, nfl, wave, h0->op.nB, epb, 8) > 200 * 1024) continue;
             for (int cs : ctas) cands.push_back({epb, cs});
             if (full == 1) break;
         }

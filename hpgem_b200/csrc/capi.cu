@@ -49,6 +49,7 @@ struct hgg_handle {
     std::vector<DevBuf> bufs;      // every device allocation
     // device operator / geometry arrays
     double *d_vol = nullptr, *d_pairs = nullptr, *d_elem_geo = nullptr, *d_face_geo = nullptr;
+    float *d_vol_f = nullptr, *d_pairs_f = nullptr;  // FP32-mixed form: the dense operators in FP32
     int32_t *d_nbr = nullptr, *d_self = nullptr, *d_nbrp = nullptr;
     int8_t *d_mode = nullptr;
     double *d_ahat = nullptr, *d_tsigma = nullptr;
@@ -237,7 +238,7 @@ int launch_tensor(hgg_handle *h, const StageIO &io) {
         constexpr int EPB = (256 / TC::NB) > 0 ? (256 / TC::NB) : 1;
         TensorGeom geo{h->d_ahat, h->d_tnbr, h->d_tmode, h->d_tsigma};
         int64_t blocks = (op.nE + EPB - 1) / EPB;
-        tensor_stage<P, DIM, EPB><<<(unsigned)blocks, EPB * TC::NB, 0, h->stream>>>(io, geo, tc);
+        tensor_stage<double, P, DIM, EPB><<<(unsigned)blocks, EPB * TC::NB, 0, h->stream>>>(io, geo, tc);
         return 0;
     }
     pa.geo = h->d_pgeo;
@@ -273,27 +274,67 @@ int launch_tensor_dim(hgg_handle *h, const StageIO &io) {
     return fail(h, HGG_ERR_UNSUPPORTED, "tensor kernel: order out of range");
 }
 
-template <int DIM, int NFL, int WAVE>
-int launch_dense(hgg_handle *h, const StageIO &io) {
+// dense kernel launch for the handle's shape and physics
+template <typename KT>
+int launch_dense_any(hgg_handle *h, const StageIOT<KT> &io);
+
+// FP32-mixed form on squares and cubes other than the slice kernel's: the one-shot kernel
+template <int DIM>
+int launch_tensor_oneshot_f(hgg_handle *h, const StageIOT<float> &io) {
+    auto go = [&](auto pc) {
+        constexpr int P = decltype(pc)::value;
+        using TC = TensorConsts<P, DIM>;
+        constexpr int EPB = (256 / TC::NB) > 0 ? (256 / TC::NB) : 1;
+        const TC tc = tensor_consts<P, DIM>(h->op);
+        TensorGeom geo{h->d_ahat, h->d_tnbr, h->d_tmode, h->d_tsigma};
+        const int64_t blocks = (h->op.nE + EPB - 1) / EPB;
+        tensor_stage<float, P, DIM, EPB><<<(unsigned)blocks, EPB * TC::NB, 0, h->stream>>>(io, geo, tc);
+        return 0;
+    };
+    switch (h->op.order) {
+        case 1: return go(std::integral_constant<int, 1>{});
+        case 2: return go(std::integral_constant<int, 2>{});
+        case 3: return go(std::integral_constant<int, 3>{});
+        case 4: return go(std::integral_constant<int, 4>{});
+        case 5: return go(std::integral_constant<int, 5>{});
+    }
+    return fail(h, HGG_ERR_UNSUPPORTED, "tensor kernel: order out of range");
+}
+
+template <typename KT, int DIM, int NFL, int WAVE>
+int launch_dense(hgg_handle *h, const StageIOT<KT> &io) {
     const HostOperators &op = h->op;
     const int V = WAVE ? DIM + 1 : 1;
     const int R = V * op.nB;
     if (R > 256) return fail(h, HGG_ERR_UNSUPPORTED, "dense kernel: more than 256 coefficients per element");
     int epb = std::max(1, 256 / dense_rows(DIM, WAVE, op.nB));
-    DenseGeom g{h->d_vol, h->d_pairs, h->d_nbr, h->d_self, h->d_nbrp, h->d_mode,
+    DenseGeom g{h->d_vol, h->d_pairs, h->d_vol_f, h->d_pairs_f, h->d_nbr, h->d_self, h->d_nbrp, h->d_mode,
                 h->d_elem_geo, h->d_face_geo, 1.0 / op.c_inv, op.nB, epb};
-    const size_t smem = dense_smem(DIM, NFL, WAVE, op.nB, epb);
     int64_t blocks = (op.nE + epb - 1) / epb;
     const int threads = dense_threads(DIM, WAVE, op.nB, epb);
     const bool ok = dense_dispatch<DIM, NFL, WAVE>(op.nB, [&](auto nbc) {
         constexpr int NB = decltype(nbc)::value;
+        const size_t smem = dense_smem(DIM, NFL, WAVE, NB, epb, sizeof(DenseCT<KT, NB>));
         if (smem > 48 * 1024)
-            cudaFuncSetAttribute(dense_stage<DIM, NFL, WAVE, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            cudaFuncSetAttribute(dense_stage<KT, DIM, NFL, WAVE, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem);
-        dense_stage<DIM, NFL, WAVE, NB><<<(unsigned)blocks, threads, smem, h->stream>>>(io, g);
+        dense_stage<KT, DIM, NFL, WAVE, NB><<<(unsigned)blocks, threads, smem, h->stream>>>(io, g);
     });
     if (!ok) return fail(h, HGG_ERR_UNSUPPORTED, "dense kernel: no kernel for this basis size");
     return 0;
+}
+
+template <typename KT>
+int launch_dense_any(hgg_handle *h, const StageIOT<KT> &io) {
+    const bool wave = h->op.physics == HGG_PHYSICS_WAVE;
+    switch (h->op.shape) {
+        case HGG_SHAPE_LINE: return wave ? launch_dense<KT, 1, 2, 1>(h, io) : launch_dense<KT, 1, 2, 0>(h, io);
+        case HGG_SHAPE_TRIANGLE: return wave ? launch_dense<KT, 2, 3, 1>(h, io) : launch_dense<KT, 2, 3, 0>(h, io);
+        case HGG_SHAPE_SQUARE: return wave ? launch_dense<KT, 2, 4, 1>(h, io) : launch_dense<KT, 2, 4, 0>(h, io);
+        case HGG_SHAPE_TETRAHEDRON: return wave ? launch_dense<KT, 3, 4, 1>(h, io) : launch_dense<KT, 3, 4, 0>(h, io);
+        case HGG_SHAPE_CUBE: return wave ? launch_dense<KT, 3, 6, 1>(h, io) : launch_dense<KT, 3, 6, 0>(h, io);
+    }
+    return fail(h, HGG_ERR_UNSUPPORTED, "shape");
 }
 
 int launch_stage(hgg_handle *h, const StageIO &io) {
@@ -306,15 +347,7 @@ int launch_stage(hgg_handle *h, const StageIO &io) {
                          : (op.dim == 3 ? launch_tensor_dim<3>(h, io)
                                         : fail(h, HGG_ERR_UNSUPPORTED, "tensor kernel needs dim 2 or 3"));
     } else {
-        const bool wave = op.physics == HGG_PHYSICS_WAVE;
-        switch (op.shape) {
-            case HGG_SHAPE_LINE: rc = wave ? launch_dense<1, 2, 1>(h, io) : launch_dense<1, 2, 0>(h, io); break;
-            case HGG_SHAPE_TRIANGLE: rc = wave ? launch_dense<2, 3, 1>(h, io) : launch_dense<2, 3, 0>(h, io); break;
-            case HGG_SHAPE_SQUARE: rc = wave ? launch_dense<2, 4, 1>(h, io) : launch_dense<2, 4, 0>(h, io); break;
-            case HGG_SHAPE_TETRAHEDRON: rc = wave ? launch_dense<3, 4, 1>(h, io) : launch_dense<3, 4, 0>(h, io); break;
-            case HGG_SHAPE_CUBE: rc = wave ? launch_dense<3, 6, 1>(h, io) : launch_dense<3, 6, 0>(h, io); break;
-            default: rc = fail(h, HGG_ERR_UNSUPPORTED, "shape");
-        }
+        rc = launch_dense_any<double>(h, io);
     }
     if (rc) return rc;
     h->launches++;
@@ -327,7 +360,11 @@ int launch_stage(hgg_handle *h, const StageIO &io) {
 int launch_stage(hgg_handle *h, const StageIOT<float> &io) {
     int rc;
     if (h->slice_ok) rc = launch_slice(h, io);
-    else return fail(h, HGG_ERR_UNSUPPORTED, "the FP32-mixed form has no kernel for this shape and order");
+    else if (h->op.tensor)
+        rc = h->op.dim == 2 ? launch_tensor_oneshot_f<2>(h, io)
+                            : (h->op.dim == 3 ? launch_tensor_oneshot_f<3>(h, io)
+                                              : fail(h, HGG_ERR_UNSUPPORTED, "tensor kernel needs dim 2 or 3"));
+    else rc = launch_dense_any<float>(h, io);
     if (rc) return rc;
     h->launches++;
     cudaError_t e = cudaGetLastError();
@@ -335,8 +372,8 @@ int launch_stage(hgg_handle *h, const StageIOT<float> &io) {
     return 0;
 }
 
-// whether the mixed form has a kernel for this handle's shape and order
-bool mixed_supported(const hgg_handle *h) { return h->slice_ok; }
+// whether the mixed form has a kernel for this handle's shape and order (all have)
+bool mixed_supported(const hgg_handle *h) { return h != nullptr; }
 
 void *vector_ptr(hgg_handle *h, int vec) {
     if (vec == 0) return h->sol[h->cur];
@@ -499,6 +536,12 @@ int create_from_desc(const hgg_problem_desc *desc, hgg_handle *h) {
                     for (size_t j = 0; j < nb; ++j) t[(q * nb + j) * nb + i] = m[(q * nb + i) * nb + j];
             return t;
         };
+        if (h->mixed) {
+            auto to_float = [](const std::vector<double> &m) { return std::vector<float>(m.begin(), m.end()); };
+            if ((rc = upload(h, to_float(transposed(op.vol)), &h->d_vol_f)) ||
+                (rc = upload(h, to_float(transposed(op.pairs)), &h->d_pairs_f)))
+                return rc;
+        }
         if ((rc = upload(h, transposed(op.vol), &h->d_vol)) || (rc = upload(h, transposed(op.pairs), &h->d_pairs)) ||
             (rc = upload(h, op.nbr, &h->d_nbr)) || (rc = upload(h, op.self_pair, &h->d_self)) ||
             (rc = upload(h, op.nbr_pair, &h->d_nbrp)) || (rc = upload(h, op.mode, &h->d_mode)) ||

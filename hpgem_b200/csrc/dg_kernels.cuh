@@ -46,19 +46,24 @@ struct StageIOT {
 };
 using StageIO = StageIOT<double>;
 
-__device__ __forceinline__ double stage_input(const StageIO &io, int64_t idx) {
+// stage input u + sum_j cin_j k_j of entry idx, formed in FP64
+template <typename KT>
+__device__ __forceinline__ double stage_input(const StageIOT<KT> &io, int64_t idx) {
     double w = io.u[idx];
 #pragma unroll 1
-    for (int j = 0; j < io.nin; ++j) w += io.cin[j] * io.kin[j][idx];
+    for (int j = 0; j < io.nin; ++j) w += io.cin[j] * (double)io.kin[j][idx];
     return w;
 }
 
-__device__ __forceinline__ void stage_output(const StageIO &io, int64_t idx, double u, double k) {
-    if (io.kout) io.kout[idx] = k;
+// this stage's derivative k of entry idx (stored as KT) and, in the final stage,
+// the new solution u + sum_j bfin_j k_j + blast k accumulated in FP64
+template <typename KT>
+__device__ __forceinline__ void stage_output(const StageIOT<KT> &io, int64_t idx, double u, double k) {
+    if (io.kout) io.kout[idx] = (KT)k;
     if (io.unew) {
         double r = u;
 #pragma unroll 1
-        for (int j = 0; j < io.nfin; ++j) r += io.bfin[j] * io.kfin[j][idx];
+        for (int j = 0; j < io.nfin; ++j) r += io.bfin[j] * (double)io.kfin[j][idx];
         r += io.blast * k;
         io.unew[idx] = r;
     }
@@ -91,26 +96,27 @@ struct TensorGeom {
 // One block's work: elements [block * EPB, block * EPB + EPB).  Called by the
 // one-shot launch (block = blockIdx.x) and by the grouped launch of many
 // problems (block = the block's index inside its problem).
-template <int P, int DIM, int EPB>
-__device__ __forceinline__ void tensor_stage_body(const StageIO &io, const TensorGeom &geo,
+template <typename KT, int P, int DIM, int EPB>
+__device__ __forceinline__ void tensor_stage_body(const StageIOT<KT> &io, const TensorGeom &geo,
                                                   const TensorConsts<P, DIM> &tc, int64_t block) {
     using TC = TensorConsts<P, DIM>;
+    using CT = KT;  // contraction type
     constexpr int NP = TC::NP, NB = TC::NB, NF = TC::NF, NS = TC::NS;
-    __shared__ double W[EPB][NB];
-    __shared__ double TR[EPB][NS][NF];
+    __shared__ CT W[EPB][NB];
+    __shared__ CT TR[EPB][NS][NF];
     // the small tables live in shared memory: indexing kernel parameters with a
     // thread-dependent index would serialise the warp on the constant cache
-    __shared__ double sD1[NP * NP], slift[2 * NP], ssign[NB];
+    __shared__ CT sD1[NP * NP], slift[2 * NP], ssign[NB];
     __shared__ short spos[NB], sinv[NB];
 
     const int tid = threadIdx.x;
     for (int i = tid; i < NB; i += EPB * NB) {
         spos[i] = tc.tpos[i];
         sinv[i] = tc.tinv[i];
-        ssign[i] = tc.tsign[i];
+        ssign[i] = (CT)tc.tsign[i];
     }
-    if (tid < NP * NP) sD1[tid] = tc.D1[tid];
-    if (tid < 2 * NP) slift[tid] = tc.lift[tid];
+    if (tid < NP * NP) sD1[tid] = (CT)tc.D1[tid];
+    if (tid < 2 * NP) slift[tid] = (CT)tc.lift[tid];
     __syncthreads();
 
     const int el = tid / NB;
@@ -124,8 +130,8 @@ __device__ __forceinline__ void tensor_stage_body(const StageIO &io, const Tenso
         const int64_t idx = e * NB + t;
         u_own = io.u[idx];
         double w = u_own;
-        for (int j = 0; j < io.nin; ++j) w += io.cin[j] * io.kin[j][idx];
-        W[el][spos[t]] = ssign[t] * w;
+        for (int j = 0; j < io.nin; ++j) w += io.cin[j] * (double)io.kin[j][idx];
+        W[el][spos[t]] = ssign[t] * (CT)w;
     }
     __syncthreads();
 
@@ -135,7 +141,7 @@ __device__ __forceinline__ void tensor_stage_body(const StageIO &io, const Tenso
         const int s = (i / NF) % NS;
         const int m = i % NF;
         const int64_t ee = e0 + l;
-        double val = 0.0;
+        CT val = CT(0);
         if (ee < io.n_elements) {
             const int axis = s >> 1, side = s & 1;
             const int8_t mode = geo.mode[ee * NS + s];
@@ -149,7 +155,7 @@ __device__ __forceinline__ void tensor_stage_body(const StageIO &io, const Tenso
                 else if (axis == 1) { c[0] = a0; c[2] = a1; }
                 else { c[0] = a0; c[1] = a1; }
             }
-            double tself = 0.0, tnbr = 0.0;
+            CT tself = CT(0), tnbr = CT(0);
             if (mode == 1 || mode == 3) {
                 c[axis] = tc.trace_pos[side];
                 int pos = c[0] + NP * c[1] + (DIM == 3 ? NP * NP * c[2] : 0);
@@ -161,13 +167,13 @@ __device__ __forceinline__ void tensor_stage_body(const StageIO &io, const Tenso
                     c[axis] = tc.trace_pos[1 - side];
                     int pos = c[0] + NP * c[1] + (DIM == 3 ? NP * NP * c[2] : 0);
                     const int hi = sinv[pos];
-                    tnbr = ssign[hi] * stage_input(io, (int64_t)n * NB + hi);
+                    tnbr = ssign[hi] * (CT)stage_input(io, (int64_t)n * NB + hi);
                 } else {
                     atomicOr(io.status, 1);
                 }
             }
-            const double sg = geo.sigma[ee * NS + s];
-            val = mode == 1 ? sg * tself : (mode == 2 ? sg * tnbr : (mode == 3 ? 0.5 * sg * (tself + tnbr) : 0.0));
+            const CT sg = (CT)geo.sigma[ee * NS + s];
+            val = mode == 1 ? sg * tself : (mode == 2 ? sg * tnbr : (mode == 3 ? CT(0.5) * sg * (tself + tnbr) : CT(0)));
         }
         TR[l][s][m] = val;
     }
@@ -179,13 +185,13 @@ __device__ __forceinline__ void tensor_stage_body(const StageIO &io, const Tenso
     a[0] = pos % NP;
     a[1] = (pos / NP) % NP;
     a[2] = DIM == 3 ? pos / (NP * NP) : 0;
-    double acc = 0.0;
+    CT acc = CT(0);
 #pragma unroll
     for (int c = 0; c < DIM; ++c) {
-        const double ah = geo.ahat[e * DIM + c];
+        const CT ah = (CT)geo.ahat[e * DIM + c];
         const int stride = c == 0 ? 1 : (c == 1 ? NP : NP * NP);
         const int base = pos - a[c] * stride;
-        double s = 0.0;
+        CT s = CT(0);
 #pragma unroll
         for (int b = 0; b < NP; ++b) s += sD1[a[c] * NP + b] * W[el][base + b * stride];
         acc += ah * s;
@@ -198,21 +204,25 @@ __device__ __forceinline__ void tensor_stage_body(const StageIO &io, const Tenso
         else m = axis == 0 ? a[1] + NP * a[2] : (axis == 1 ? a[0] + NP * a[2] : a[0] + NP * a[1]);
         acc -= slift[side * NP + a[axis]] * TR[el][s][m];
     }
-    stage_output(io, e * NB + t, u_own, ssign[t] * acc);
+    stage_output(io, e * NB + t, u_own, (double)(ssign[t] * acc));
 }
 
-template <int P, int DIM, int EPB>
+template <typename KT, int P, int DIM, int EPB>
 __global__ void __launch_bounds__(EPB *TensorConsts<P, DIM>::NB)
-    tensor_stage(const StageIO io, const TensorGeom geo, const TensorConsts<P, DIM> tc) {
-    tensor_stage_body<P, DIM, EPB>(io, geo, tc, blockIdx.x);
+    tensor_stage(const StageIOT<KT> io, const TensorGeom geo, const TensorConsts<P, DIM> tc) {
+    tensor_stage_body<KT, P, DIM, EPB>(io, geo, tc, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------
 // dense reference operators, any shape and physics
 // ---------------------------------------------------------------------------
+// Dense reference operators of one problem, in FP64 and (FP32-mixed form) FP32;
+// the geometry is FP64 in both forms.
 struct DenseGeom {
     const double *vol;         // [DIM][NB][NB], transposed: vol[c][j][i] = (Mhat^{-1} K_c)_{ij}
     const double *pairs;       // [n_pairs][NB][NB], transposed the same way
+    const float *vol_f;        // the same in FP32 (FP32-mixed form only, else null)
+    const float *pairs_f;
     const int32_t *nbr;        // [E][NFL]
     const int32_t *self_pair;  // [E][NFL]
     const int32_t *nbr_pair;   // [E][NFL]
@@ -224,21 +234,47 @@ struct DenseGeom {
     int epb;                   // elements per block
 };
 
+// Contraction type of the dense kernel: FP64 in the FP64 form; in the FP32-mixed
+// form FP32 up to kMixedFp32MaxBasis basis functions and FP64 above, where the
+// operators Mhat^{-1} K (the mass inverse folded in) grow large with cancelling
+// entries and FP32 contractions would cost the mixed form its accuracy target
+// (observed: triangles at p = 5, 21 functions, 1.0e-6 L2 distance to FP64 after
+// 100 steps in FP32 contractions).  The stage vectors stay FP32 either way.
+constexpr int kMixedFp32MaxBasis = 20;
+template <typename KT, int NB>
+using DenseCT = std::conditional_t<std::is_same_v<KT, float> && NB <= kMixedFp32MaxBasis, float, double>;
+
+template <typename CT>
+__device__ __forceinline__ const CT *dense_vol(const DenseGeom &g);
+template <>
+__device__ __forceinline__ const double *dense_vol<double>(const DenseGeom &g) { return g.vol; }
+template <>
+__device__ __forceinline__ const float *dense_vol<float>(const DenseGeom &g) { return g.vol_f; }
+template <typename CT>
+__device__ __forceinline__ const CT *dense_pairs(const DenseGeom &g);
+template <>
+__device__ __forceinline__ const double *dense_pairs<double>(const DenseGeom &g) { return g.pairs; }
+template <>
+__device__ __forceinline__ const float *dense_pairs<float>(const DenseGeom &g) { return g.pairs_f; }
+
 // One block's work: elements [block * epb, block * epb + epb) (see tensor_stage_body).
-// Thread (el, r) produces output row r of element el.  The operators are stored
-// transposed, so at every column j the threads of a warp read consecutive rows'
-// entries: one or two sectors per warp instead of one per thread.
-//
-// NB (basis functions) is a compile-time constant, so the row loops unroll and
-// the index arithmetic needs no runtime division.
-template <int DIM, int NFL, int WAVE, int NB>
-__device__ __forceinline__ void dense_stage_body(const StageIO &io, const DenseGeom &g, int64_t block) {
+// Thread (el, r) produces output row r of element el (advection, and the wave in
+// one dimension).  The operators are stored transposed, so at every column j the
+// threads of a warp read consecutive rows' entries: one or two sectors per warp
+// instead of one per thread.  NB (basis functions) is a compile-time constant, so
+// the row loops unroll and the index arithmetic needs no runtime division.  KT is
+// the stage vectors' type and the contraction type (see StageIOT).
+template <typename KT, int DIM, int NFL, int WAVE, int NB>
+__device__ __forceinline__ void dense_stage_body(const StageIOT<KT> &io, const DenseGeom &g, int64_t block) {
+    static_assert(!(WAVE && DIM >= 2), "the wave in 2D and 3D runs wave_stage_body");
+    using CT = DenseCT<KT, NB>;
+    const CT *gvol = dense_vol<CT>(g), *gpairs = dense_pairs<CT>(g);
     constexpr int V = WAVE ? DIM + 1 : 1;
     constexpr int nB = NB, R = V * NB;
-    extern __shared__ double smem[];
+    extern __shared__ __align__(16) unsigned char dense_shared[];
     const int epb = g.epb;
-    double *W = smem;                        // [epb][R]
-    double *WN = smem + (size_t)epb * R;     // [epb][NFL][R]
+    CT *W = reinterpret_cast<CT *>(dense_shared);  // [epb][R]
+    CT *WN = W + (size_t)epb * R;                 // [epb][NFL][R]
     const int tid = threadIdx.x;
     const int64_t e0 = block * epb;
 
@@ -250,8 +286,8 @@ __device__ __forceinline__ void dense_stage_body(const StageIO &io, const DenseG
         const int64_t idx = e * R + r;
         u_own = io.u[idx];
         double w = u_own;
-        for (int j = 0; j < io.nin; ++j) w += io.cin[j] * io.kin[j][idx];
-        W[el * R + r] = w;
+        for (int j = 0; j < io.nin; ++j) w += io.cin[j] * (double)io.kin[j][idx];
+        W[el * R + r] = (CT)w;
     }
     for (int i = tid; i < epb * NFL * R; i += blockDim.x) {
         const int l = i / (NFL * R), f = (i / R) % NFL, rr = i % R;
@@ -262,145 +298,78 @@ __device__ __forceinline__ void dense_stage_body(const StageIO &io, const DenseG
             if (n >= 0 && n < io.n_elements) v = stage_input(io, (int64_t)n * R + rr);
             else atomicOr(io.status, 1);
         }
-        WN[(size_t)(l * NFL + f) * R + rr] = v;
+        WN[(size_t)(l * NFL + f) * R + rr] = (CT)v;
     }
     __syncthreads();
-    if (WAVE && DIM >= 2) {
-        // per element and axis c: t_c = sum_d G[d][c] s_d (the velocity combination the
-        // divergence row needs), and per face: the normal jumps n . s of both sides,
-        // formed once per element instead of once per output row; they replace the
-        // velocity blocks of W and WN (the velocity rows read only the pressure block)
-        double tmp[DIM];
-        const int64_t ee = e;
-        if (active && r < nB) {
-            const double *G = g.elem_geo + ee * DIM * DIM;
-            double *w = W + el * R;
-#pragma unroll
-            for (int c = 0; c < DIM; ++c) {
-                double t = 0.0;
-#pragma unroll
-                for (int d = 0; d < DIM; ++d) t += G[d * DIM + c] * w[(d + 1) * nB + r];
-                tmp[c] = t;
-            }
-        }
-        double jl[NFL], jn[NFL];
-        if (active && r < nB) {
-            const double *w = W + el * R;
-            const double *wn = WN + (size_t)el * NFL * R;
-            for (int f = 0; f < NFL; ++f) {
-                const double *nu = g.face_geo + ((size_t)ee * NFL + f) * DIM;
-                double a = 0.0, b = 0.0;
-                for (int d = 0; d < DIM; ++d) {
-                    a += nu[d] * w[(d + 1) * nB + r];
-                    b += nu[d] * wn[f * R + (d + 1) * nB + r];
-                }
-                jl[f] = a;
-                jn[f] = b;
-            }
-        }
-        __syncthreads();
-        if (active && r < nB) {
-            double *w = W + el * R;
-            double *wn = WN + (size_t)el * NFL * R;
-            for (int c = 0; c < DIM; ++c) w[(c + 1) * nB + r] = tmp[c];
-            for (int f = 0; f < NFL; ++f) {  // velocity blocks 1 and 2 of the face slot
-                wn[f * R + nB + r] = jl[f];
-                wn[f * R + 2 * nB + r] = jn[f];
-            }
-        }
-        __syncthreads();
-    }
     if (!active) return;
 
-    const double *w = W + el * R;
-    const double *wn = WN + (size_t)el * NFL * R;
-    double acc = 0.0;
+    const CT *w = W + el * R;
+    const CT *wn = WN + (size_t)el * NFL * R;
+    CT acc = CT(0);
     if (!WAVE) {
         const int i = r;
         for (int c = 0; c < DIM; ++c) {
-            const double *op = g.vol + (size_t)c * nB * nB + i;
-            double s = 0.0;
-            #pragma unroll
+            const CT *op = gvol + (size_t)c * nB * nB + i;
+            CT s = CT(0);
+#pragma unroll
             for (int j = 0; j < nB; ++j) s += op[(size_t)j * nB] * w[j];
-            acc += g.elem_geo[e * DIM + c] * s;
+            acc += (CT)g.elem_geo[e * DIM + c] * s;
         }
         for (int f = 0; f < NFL; ++f) {
             const int8_t mode = g.mode[e * NFL + f];
-            const double sg = g.face_geo[e * NFL + f];
-            double ts = 0.0, tn = 0.0;
+            const CT sg = (CT)g.face_geo[e * NFL + f];
+            CT ts = CT(0), tn = CT(0);
             if (mode == 1 || mode == 3) {
-                const double *op = g.pairs + (size_t)g.self_pair[e * NFL + f] * nB * nB + i;
-                #pragma unroll
+                const CT *op = gpairs + (size_t)g.self_pair[e * NFL + f] * nB * nB + i;
+#pragma unroll
                 for (int j = 0; j < nB; ++j) ts += op[(size_t)j * nB] * w[j];
             }
             if (mode == 2 || mode == 3) {
-                const double *op = g.pairs + (size_t)g.nbr_pair[e * NFL + f] * nB * nB + i;
-                #pragma unroll
+                const CT *op = gpairs + (size_t)g.nbr_pair[e * NFL + f] * nB * nB + i;
+#pragma unroll
                 for (int j = 0; j < nB; ++j) tn += op[(size_t)j * nB] * wn[f * R + j];
             }
-            acc -= mode == 1 ? sg * ts : (mode == 2 ? sg * tn : (mode == 3 ? 0.5 * sg * (ts + tn) : 0.0));
+            acc -= mode == 1 ? sg * ts : (mode == 2 ? sg * tn : (mode == 3 ? CT(0.5) * sg * (ts + tn) : CT(0)));
         }
     } else {
+        // the wave in one dimension: G and the normal are scalars
         const int v = r / nB, i = r % nB;
-        const double *G = g.elem_geo + e * DIM * DIM;  // G[d][c] = (J^{-T})_{dc}
-        if (v == 0 && DIM >= 2) {
-            // k_q = sum_c vol[c] t_c  (strong-form divergence), minus the face jumps of n . s
-            for (int c = 0; c < DIM; ++c) {
-                const double *op = g.vol + (size_t)c * nB * nB + i;
-                const double *t = w + (c + 1) * nB;
-                double s = 0.0;
-                #pragma unroll
-                for (int j = 0; j < nB; ++j) s += op[(size_t)j * nB] * t[j];
-                acc += s;
-            }
-            for (int f = 0; f < NFL; ++f) {
-                const double *ops = g.pairs + (size_t)g.self_pair[e * NFL + f] * nB * nB + i;
-                const double *opn = g.pairs + (size_t)g.nbr_pair[e * NFL + f] * nB * nB + i;
-                const double *js = wn + f * R + nB, *jn = wn + f * R + 2 * nB;
-                double s = 0.0;
-                #pragma unroll
-                for (int j = 0; j < nB; ++j) s += ops[(size_t)j * nB] * js[j] - opn[(size_t)j * nB] * jn[j];
-                acc -= s;
-            }
-        } else if (v == 0) {
-            // one dimension: G and the normal are scalars
-            const double *op = g.vol + i;
-            double s = 0.0;
-            #pragma unroll
+        const CT G = (CT)g.elem_geo[e];
+        if (v == 0) {
+            const CT *op = gvol + i;
+            CT s = CT(0);
+#pragma unroll
             for (int j = 0; j < nB; ++j) s += op[(size_t)j * nB] * w[nB + j];
-            acc += G[0] * s;
+            acc += G * s;
             for (int f = 0; f < NFL; ++f) {
-                const double nu = g.face_geo[(size_t)e * NFL + f];
-                const double *ops = g.pairs + (size_t)g.self_pair[e * NFL + f] * nB * nB + i;
-                const double *opn = g.pairs + (size_t)g.nbr_pair[e * NFL + f] * nB * nB + i;
-                double t = 0.0;
-                #pragma unroll
+                const CT nu = (CT)g.face_geo[(size_t)e * NFL + f];
+                const CT *ops = gpairs + (size_t)g.self_pair[e * NFL + f] * nB * nB + i;
+                const CT *opn = gpairs + (size_t)g.nbr_pair[e * NFL + f] * nB * nB + i;
+                CT t = CT(0);
+#pragma unroll
                 for (int j = 0; j < nB; ++j) t += ops[(size_t)j * nB] * w[nB + j] - opn[(size_t)j * nB] * wn[f * R + nB + j];
                 acc -= nu * t;
             }
         } else {
-            // k_{s_d} = (1/cInv) [ sum_c G[d][c] vol[c] q  - face jumps of q ]
-            const int d = v - 1;
-            for (int c = 0; c < DIM; ++c) {
-                const double *op = g.vol + (size_t)c * nB * nB + i;
-                double s = 0.0;
-                #pragma unroll
-                for (int j = 0; j < nB; ++j) s += op[(size_t)j * nB] * w[j];
-                acc += G[d * DIM + c] * s;
-            }
+            // k_s = (1/cInv) [ G vol q - face jumps of q ]
+            const CT *op = gvol + i;
+            CT s = CT(0);
+#pragma unroll
+            for (int j = 0; j < nB; ++j) s += op[(size_t)j * nB] * w[j];
+            acc += G * s;
             for (int f = 0; f < NFL; ++f) {
-                const double nud = g.face_geo[((size_t)e * NFL + f) * DIM + d];
-                const double *ops = g.pairs + (size_t)g.self_pair[e * NFL + f] * nB * nB + i;
-                const double *opn = g.pairs + (size_t)g.nbr_pair[e * NFL + f] * nB * nB + i;
-                double s = 0.0;
-                #pragma unroll
-                for (int j = 0; j < nB; ++j) s += ops[(size_t)j * nB] * w[j] - opn[(size_t)j * nB] * wn[f * R + j];
-                acc -= nud * s;
+                const CT nud = (CT)g.face_geo[(size_t)e * NFL + f];
+                const CT *ops = gpairs + (size_t)g.self_pair[e * NFL + f] * nB * nB + i;
+                const CT *opn = gpairs + (size_t)g.nbr_pair[e * NFL + f] * nB * nB + i;
+                CT t = CT(0);
+#pragma unroll
+                for (int j = 0; j < nB; ++j) t += ops[(size_t)j * nB] * w[j] - opn[(size_t)j * nB] * wn[f * R + j];
+                acc -= nud * t;
             }
-            acc *= g.inv_cinv;
+            acc *= (CT)g.inv_cinv;
         }
     }
-    stage_output(io, e * R + r, u_own, acc);
+    stage_output(io, e * R + r, u_own, (double)acc);
 }
 
 // Acoustic wave in 2D and 3D: thread (el, i) produces row i of all DIM + 1
@@ -409,14 +378,16 @@ __device__ __forceinline__ void dense_stage_body(const StageIO &io, const DenseG
 // they are formed once per row instead of once per velocity component; the
 // pressure row uses t_c = sum_d G[d][c] s_d and the normal jumps n . s of both
 // sides, formed once per element and column.
-template <int DIM, int NFL, int NB>
-__device__ __forceinline__ void wave_stage_body(const StageIO &io, const DenseGeom &g, int64_t block) {
+template <typename KT, int DIM, int NFL, int NB>
+__device__ __forceinline__ void wave_stage_body(const StageIOT<KT> &io, const DenseGeom &g, int64_t block) {
+    using CT = DenseCT<KT, NB>;
+    const CT *gvol = dense_vol<CT>(g), *gpairs = dense_pairs<CT>(g);
     constexpr int V = DIM + 1, R = V * NB, NX = DIM + 2 * NFL;
-    extern __shared__ double smem[];
+    extern __shared__ __align__(16) unsigned char dense_shared[];
     const int epb = g.epb;
-    double *W = smem;                              // [epb][R]
-    double *WN = W + (size_t)epb * R;              // [epb][NFL][R]
-    double *X = WN + (size_t)epb * NFL * R;        // [epb][NX][NB]: t_c, then n . s self, then n . s neighbour
+    CT *W = reinterpret_cast<CT *>(dense_shared);  // [epb][R]
+    CT *WN = W + (size_t)epb * R;                 // [epb][NFL][R]
+    CT *X = WN + (size_t)epb * NFL * R;           // [epb][NX][NB]: t_c, then n . s self, then n . s neighbour
     const int tid = threadIdx.x;
     const int64_t e0 = block * epb;
     const int el = tid / NB, i = tid % NB;
@@ -430,8 +401,8 @@ __device__ __forceinline__ void wave_stage_body(const StageIO &io, const DenseGe
             const int64_t idx = e * R + v * NB + i;
             u_own[v] = io.u[idx];
             double w = u_own[v];
-            for (int j = 0; j < io.nin; ++j) w += io.cin[j] * io.kin[j][idx];
-            W[el * R + v * NB + i] = w;
+            for (int j = 0; j < io.nin; ++j) w += io.cin[j] * (double)io.kin[j][idx];
+            W[el * R + v * NB + i] = (CT)w;
         }
     }
     for (int k = tid; k < epb * NFL * R; k += blockDim.x) {
@@ -443,29 +414,29 @@ __device__ __forceinline__ void wave_stage_body(const StageIO &io, const DenseGe
             if (n >= 0 && n < io.n_elements) v = stage_input(io, (int64_t)n * R + rr);
             else atomicOr(io.status, 1);
         }
-        WN[(size_t)(l * NFL + f) * R + rr] = v;
+        WN[(size_t)(l * NFL + f) * R + rr] = (CT)v;
     }
     __syncthreads();
-    const double *w = W + el * R;
-    const double *wn = WN + (size_t)el * NFL * R;
-    double *x = X + (size_t)el * NX * NB;
+    const CT *w = W + el * R;
+    const CT *wn = WN + (size_t)el * NFL * R;
+    CT *x = X + (size_t)el * NX * NB;
     if (active) {
         const double *G = g.elem_geo + e * DIM * DIM;  // G[d][c] = (J^{-T})_{dc}
 #pragma unroll
         for (int c = 0; c < DIM; ++c) {
-            double t = 0.0;
+            CT t = CT(0);
 #pragma unroll
-            for (int d = 0; d < DIM; ++d) t += G[d * DIM + c] * w[(d + 1) * NB + i];
+            for (int d = 0; d < DIM; ++d) t += (CT)G[d * DIM + c] * w[(d + 1) * NB + i];
             x[c * NB + i] = t;
         }
 #pragma unroll
         for (int f = 0; f < NFL; ++f) {
             const double *nu = g.face_geo + ((size_t)e * NFL + f) * DIM;
-            double a = 0.0, b = 0.0;
+            CT a = CT(0), b = CT(0);
 #pragma unroll
             for (int d = 0; d < DIM; ++d) {
-                a += nu[d] * w[(d + 1) * NB + i];
-                b += nu[d] * wn[f * R + (d + 1) * NB + i];
+                a += (CT)nu[d] * w[(d + 1) * NB + i];
+                b += (CT)nu[d] * wn[f * R + (d + 1) * NB + i];
             }
             x[(DIM + f) * NB + i] = a;
             x[(DIM + NFL + f) * NB + i] = b;
@@ -474,14 +445,14 @@ __device__ __forceinline__ void wave_stage_body(const StageIO &io, const DenseGe
     __syncthreads();
     if (!active) return;
 
-    double P = 0.0, A[DIM], B[NFL];
+    CT P = CT(0), A[DIM], B[NFL];
 #pragma unroll
     for (int c = 0; c < DIM; ++c) {
-        const double *op = g.vol + (size_t)c * NB * NB + i;
-        double sp = 0.0, sa = 0.0;
+        const CT *op = gvol + (size_t)c * NB * NB + i;
+        CT sp = CT(0), sa = CT(0);
 #pragma unroll
         for (int j = 0; j < NB; ++j) {
-            const double o = op[(size_t)j * NB];
+            const CT o = op[(size_t)j * NB];
             sp += o * x[c * NB + j];
             sa += o * w[j];
         }
@@ -490,53 +461,54 @@ __device__ __forceinline__ void wave_stage_body(const StageIO &io, const DenseGe
     }
 #pragma unroll
     for (int f = 0; f < NFL; ++f) {
-        const double *ops = g.pairs + (size_t)g.self_pair[e * NFL + f] * NB * NB + i;
-        const double *opn = g.pairs + (size_t)g.nbr_pair[e * NFL + f] * NB * NB + i;
-        const double *js = x + (DIM + f) * NB, *jn = x + (DIM + NFL + f) * NB;
-        double sp = 0.0, sb = 0.0;
+        const CT *ops = gpairs + (size_t)g.self_pair[e * NFL + f] * NB * NB + i;
+        const CT *opn = gpairs + (size_t)g.nbr_pair[e * NFL + f] * NB * NB + i;
+        const CT *js = x + (DIM + f) * NB, *jn = x + (DIM + NFL + f) * NB;
+        CT sp = CT(0), sb = CT(0);
 #pragma unroll
         for (int j = 0; j < NB; ++j) {
-            const double os = ops[(size_t)j * NB], on = opn[(size_t)j * NB];
+            const CT os = ops[(size_t)j * NB], on = opn[(size_t)j * NB];
             sp += os * js[j] - on * jn[j];
             sb += os * w[j] - on * wn[f * R + j];
         }
         P -= sp;
         B[f] = sb;
     }
-    stage_output(io, e * R + i, u_own[0], P);
+    stage_output(io, e * R + i, u_own[0], (double)P);
     const double *G = g.elem_geo + e * DIM * DIM;
 #pragma unroll
     for (int d = 0; d < DIM; ++d) {
-        double acc = 0.0;
+        CT acc = CT(0);
 #pragma unroll
-        for (int c = 0; c < DIM; ++c) acc += G[d * DIM + c] * A[c];
+        for (int c = 0; c < DIM; ++c) acc += (CT)G[d * DIM + c] * A[c];
 #pragma unroll
-        for (int f = 0; f < NFL; ++f) acc -= g.face_geo[((size_t)e * NFL + f) * DIM + d] * B[f];
-        stage_output(io, e * R + (d + 1) * NB + i, u_own[d + 1], acc * g.inv_cinv);
+        for (int f = 0; f < NFL; ++f) acc -= (CT)g.face_geo[((size_t)e * NFL + f) * DIM + d] * B[f];
+        stage_output(io, e * R + (d + 1) * NB + i, u_own[d + 1], (double)(acc * (CT)g.inv_cinv));
     }
 }
 
 // threads and dynamic shared memory of one dense-kernel block of `epb` elements
+// (elem: bytes of the contraction type)
 __host__ __device__ inline int dense_rows(int dim, int wave, int nb) { return wave && dim >= 2 ? nb : (wave ? dim + 1 : 1) * nb; }
 __host__ __device__ inline int dense_threads(int dim, int wave, int nb, int epb) {
     return ((epb * dense_rows(dim, wave, nb) + 31) / 32) * 32;
 }
-__host__ __device__ inline size_t dense_smem(int dim, int nfl, int wave, int nb, int epb) {
+__host__ __device__ inline size_t dense_smem(int dim, int nfl, int wave, int nb, int epb, size_t elem = 8) {
     const int R = (wave ? dim + 1 : 1) * nb;
     size_t d = (size_t)epb * R * (1 + nfl);
     if (wave && dim >= 2) d += (size_t)epb * (dim + 2 * nfl) * nb;
-    return sizeof(double) * d;
+    return elem * d;
 }
 
-template <int DIM, int NFL, int WAVE, int NB>
-__device__ __forceinline__ void dense_any_body(const StageIO &io, const DenseGeom &g, int64_t block) {
-    if constexpr (WAVE && DIM >= 2) wave_stage_body<DIM, NFL, NB>(io, g, block);
-    else dense_stage_body<DIM, NFL, WAVE, NB>(io, g, block);
+template <typename KT, int DIM, int NFL, int WAVE, int NB>
+__device__ __forceinline__ void dense_any_body(const StageIOT<KT> &io, const DenseGeom &g, int64_t block) {
+    if constexpr (WAVE && DIM >= 2) wave_stage_body<KT, DIM, NFL, NB>(io, g, block);
+    else dense_stage_body<KT, DIM, NFL, WAVE, NB>(io, g, block);
 }
 
-template <int DIM, int NFL, int WAVE, int NB>
-__global__ void __launch_bounds__(256) dense_stage(const StageIO io, const DenseGeom g) {
-    dense_any_body<DIM, NFL, WAVE, NB>(io, g, blockIdx.x);
+template <typename KT, int DIM, int NFL, int WAVE, int NB>
+__global__ void __launch_bounds__(256) dense_stage(const StageIOT<KT> io, const DenseGeom g) {
+    dense_any_body<KT, DIM, NFL, WAVE, NB>(io, g, blockIdx.x);
 }
 
 // basis sizes of the shapes the dense kernel serves, orders 1..5

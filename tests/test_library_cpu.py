@@ -101,22 +101,21 @@ def test_create_reports_a_missing_device_or_succeeds():
 
 
 def test_precision_forms_are_checked_before_the_device():
-    """An unknown precision is invalid; the FP32-mixed form exists only where a kernel
-    has it (hexahedra of order 3), which create decides before looking for a device."""
+    """An unknown precision is invalid (decided before looking for a device); both
+    forms exist for every shape, so they get as far as the device check."""
     lib = _native.load()
     h = ctypes.c_void_p()
-    a = (ctypes.c_double * 2)(1.0, 0.5)
+    a = (ctypes.c_double * 3)(1.0, 0.5, 0.3)
     quads = b"structured 1 2\n4 4\n0 0\n1 1\nrectangular\ntrue true\n"
     assert lib.hgg_create_structured(quads, 2, 0, a, b"RK4_4", 7, ctypes.byref(h)) == -1
-    assert lib.hgg_create_structured(quads, 2, 0, a, b"RK4_4", _native.PRECISION_FP32, ctypes.byref(h)) == -2
-    assert b"FP32-mixed" in lib.hgg_last_error(None)
-    a3 = (ctypes.c_double * 3)(1.0, 0.7, 0.3)
-    cubes = b"structured 1 3\n4 4 4\n0 0 0\n1 1 1\nrectangular\ntrue true true\n"
-    rc = lib.hgg_create_structured(cubes, 3, 0, a3, b"RK4_4", _native.PRECISION_FP32, ctypes.byref(h))
-    if rc == 0:
-        lib.hgg_destroy(h)
-    else:
-        assert rc == -6
+    for text in (quads, b"structured 1 2\n4 4\n0 0\n1 1\ntriangular\ntrue true\n",
+                 b"structured 1 3\n4 4 4\n0 0 0\n1 1 1\nrectangular\ntrue true true\n"):
+        for prec in (_native.PRECISION_FP64, _native.PRECISION_FP32):
+            rc = lib.hgg_create_structured(text, 3, 0, a, b"RK4_4", prec, ctypes.byref(h))
+            if rc == 0:
+                lib.hgg_destroy(h)
+            else:
+                assert rc == -6, (text, prec, rc)
 
 
 def test_solve_step_count_rule():
