@@ -24,7 +24,7 @@ EXPORTED = ["hgg_create", "hgg_destroy", "hgg_last_error", "hgg_set_state", "hgg
             "hgg_create_structured", "hgg_structured_descriptor", "hgg_free_descriptor",
             "hgg_quadrature_points", "hgg_num_quadrature_points",
             "hgg_project", "hgg_num_error_points", "hgg_error_points", "hgg_l2_error",
-            "hgg_time_derivative_static",
+            "hgg_time_derivative_static", "hgg_step_adaptive", "hgg_set_error_estimate",
             "hgg_batch_create", "hgg_batch_destroy", "hgg_batch_last_error", "hgg_batch_add",
             "hgg_batch_remove", "hgg_batch_step", "hgg_batch_synchronize", "hgg_batch_remaining",
             "hgg_batch_set_autotune", "hgg_batch_launch_count", "hgg_batch_num_classes",
@@ -88,6 +88,10 @@ def load():
         "hgg_step": (ctypes.c_int, [H, ctypes.POINTER(ctypes.c_double), ctypes.c_double, ctypes.c_int32]),
         "hgg_time_derivative": (ctypes.c_int, [H, ctypes.c_int32, ctypes.c_int32]),
         "hgg_time_derivative_static": (ctypes.c_int, [H, ctypes.c_void_p, ctypes.c_void_p]),
+        "hgg_step_adaptive": (ctypes.c_int, [H, ctypes.POINTER(ctypes.c_double), ctypes.c_double, ctypes.c_double,
+                                             ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
+                                             ctypes.POINTER(ctypes.c_int32)]),
+        "hgg_set_error_estimate": (ctypes.c_int, [H, P, ctypes.c_int32]),
         "hgg_batch_create": (ctypes.c_int, [ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p)]),
         "hgg_batch_destroy": (ctypes.c_int, [B]),
         "hgg_batch_last_error": (ctypes.c_char_p, [B]),

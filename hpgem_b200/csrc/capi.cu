@@ -6,6 +6,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <limits>
 #include <memory>
 #include <mutex>
 #include <stdexcept>
@@ -40,6 +41,8 @@ struct hgg_handle {
     std::unique_ptr<StructuredProblem> sp;  // set when built from a structured description
     int S = 0;
     std::vector<double> rk_a, rk_b, rk_c;
+    std::vector<double> rk_err;   // error coefficients of an embedded tableau (empty: none)
+    int rk_order = 0;
     int64_t N = 0;                 // doubles per vector
     int64_t N_alloc = 0;           // doubles allocated per vector (whole tiles)
     double *sol[2] = {nullptr, nullptr};
@@ -61,6 +64,7 @@ struct hgg_handle {
     bool tensor_layout = false;       // device vectors in tensor order (signs folded)
     bool tiled = false;               // ... and in tiles of 32 elements, coefficient-major (slice kernel)
     double *d_scratch = nullptr;      // one vector, for layout conversion of set/get_state
+    double *d_reduce = nullptr;       // adaptive steps: per-element error and norm, partial sums
     int32_t *d_tpos = nullptr;        // hpGEM index -> tensor position
     double *d_tsign = nullptr;
     // slice kernel (hexahedra, p = 3): per-element records of SliceShape::GR doubles
@@ -148,6 +152,15 @@ TensorConsts<P, DIM> tensor_consts(const HostOperators &op) {
 __device__ __forceinline__ int64_t device_index(int64_t e, int pos, int nb, bool tiled) {
     return tiled ? (e >> 5) * ((int64_t)nb << 5) + (int64_t)pos * 32 + (e & 31) : e * nb + pos;
 }
+// stage vectors and per-stage coefficients of the error estimate and the rewind
+template <typename KT>
+struct ErrStages {
+    const KT *k[kMaxStages];
+    double err[kMaxStages];
+    double dt;
+    int n;
+};
+
 template <typename TD>
 __global__ void to_tensor_order(const double *src, TD *dst, const int32_t *tpos, const double *tsign,
                                 int nb, int64_t n, bool tiled) {
@@ -809,6 +822,173 @@ int hgg_time_derivative_static(hgg_handle *h, const double *u, double *k) {
     return check_status(h);
 }
 
+}  // extern "C"
+
+// ---- adaptive time step -------------------------------------------------------
+// computeErrorAndNormOfUpdate (HpgemAPISimplified_Impl.h:719-749) per element:
+// the deviation sum_i (k_i dt) err_i of the element's coefficients, its squared
+// Euclidean norm, and the Euclidean norm of the element's (updated) solution.
+// The layout is the device's (tensor order, tiled or not): a permutation with
+// sign flips inside each element, which leaves both norms unchanged.
+template <typename KT>
+__global__ void element_error_norm(const double *u, ErrStages<KT> ks, int nb, int64_t n_elements, bool tiled,
+                                   double *err2, double *norm) {
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= n_elements) return;
+    double s2 = 0.0, n2 = 0.0;
+    for (int pos = 0; pos < nb; ++pos) {
+        const int64_t idx = device_index(e, pos, nb, tiled);
+        double dev = 0.0;
+        for (int i = 0; i < ks.n; ++i) dev += ((double)ks.k[i][idx] * ks.dt) * ks.err[i];
+        s2 += dev * dev;
+        n2 += u[idx] * u[idx];
+    }
+    err2[e] = s2;
+    norm[e] = sqrt(n2);
+}
+
+// deterministic sums of two arrays: block partials in a fixed order, then the partials
+constexpr int kSumThreads = 256;
+__global__ void sum_pairs(const double *a, const double *b, int64_t n, double *pa, double *pb) {
+    __shared__ double sa[kSumThreads], sb[kSumThreads];
+    double x = 0.0, y = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)kSumThreads + threadIdx.x; i < n; i += (int64_t)gridDim.x * kSumThreads) {
+        x += a[i];
+        y += b[i];
+    }
+    sa[threadIdx.x] = x;
+    sb[threadIdx.x] = y;
+    __syncthreads();
+    for (int w = kSumThreads / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) {
+            sa[threadIdx.x] += sa[threadIdx.x + w];
+            sb[threadIdx.x] += sb[threadIdx.x + w];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        pa[blockIdx.x] = sa[0];
+        pb[blockIdx.x] = sb[0];
+    }
+}
+
+// undo a rejected step: u -= dt b_j k_j for j = 0..S-1, one update after the other as
+// the reference's scaleAndAddVector calls do (HpgemAPISimplified_Impl.h:843-848)
+template <typename KT>
+__global__ void rewind_update(double *u, ErrStages<KT> ks, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double v = u[i];
+        for (int j = 0; j < ks.n; ++j) v += (-ks.dt * ks.err[j]) * (double)ks.k[j][i];
+        u[i] = v;
+    }
+}
+
+namespace {
+
+template <typename KT>
+ErrStages<KT> err_stages(const hgg_handle *h, double dt, const std::vector<double> &coef) {
+    ErrStages<KT> ks{};
+    ks.n = h->S;
+    ks.dt = dt;
+    for (int i = 0; i < h->S; ++i) {
+        ks.k[i] = static_cast<const KT *>(h->k[i]);
+        ks.err[i] = coef[i];
+    }
+    return ks;
+}
+
+// error and solution norm of the step just taken (sol[cur] is the updated solution)
+int error_and_norm(hgg_handle *h, double dt, double *error, double *norm) {
+    const int64_t nE = h->op.nE;
+    const int nb = h->op.V * h->op.nB;
+    double *err2 = h->d_reduce, *nrm = h->d_reduce + nE;
+    const unsigned eb = (unsigned)((nE + 255) / 256);
+    if (h->mixed)
+        element_error_norm<float><<<eb, 256, 0, h->stream>>>(h->sol[h->cur], err_stages<float>(h, dt, h->rk_err), nb,
+                                                             nE, h->tiled, err2, nrm);
+    else
+        element_error_norm<double><<<eb, 256, 0, h->stream>>>(h->sol[h->cur], err_stages<double>(h, dt, h->rk_err),
+                                                              nb, nE, h->tiled, err2, nrm);
+    const int parts = 256;
+    double *pa = h->d_reduce + 2 * nE, *pb = pa + parts;
+    sum_pairs<<<parts, kSumThreads, 0, h->stream>>>(err2, nrm, nE, pa, pb);
+    sum_pairs<<<1, kSumThreads, 0, h->stream>>>(pa, pb, parts, pa + 2 * parts, pb + 2 * parts);
+    h->launches += 3;
+    HGG_CUDA(h, cudaGetLastError());
+    double out[2];
+    HGG_CUDA(h, cudaMemcpyAsync(&out[0], pa + 2 * parts, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    HGG_CUDA(h, cudaMemcpyAsync(&out[1], pb + 2 * parts, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    HGG_CUDA(h, cudaStreamSynchronize(h->stream));
+    *error = std::sqrt(out[0]);
+    *norm = out[1];
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int hgg_set_error_estimate(hgg_handle *h, const double *error_coefficients, int32_t order) {
+    if (!h || !error_coefficients || order < 1) return fail(h, HGG_ERR_INVALID, "error coefficients and order >= 1");
+    h->rk_err.assign(error_coefficients, error_coefficients + h->S);
+    h->rk_order = order;
+    return 0;
+}
+
+int hgg_step_adaptive(hgg_handle *h, double *time, double max_relative_error, double dt_max, double *dt_estimate,
+                      double *dt_taken, int32_t *rejections) {
+    if (!h || !time || !dt_estimate) return fail(h, HGG_ERR_INVALID, "null argument");
+    if (h->rk_err.empty()) return fail(h, HGG_ERR_INVALID, "the tableau has no error estimate (embedded pair)");
+    if (!(max_relative_error > 0.0) || !(dt_max > 0.0) || !(*dt_estimate > 0.0))
+        return fail(h, HGG_ERR_INVALID, "maximum relative error, dt_max and the dt estimate must be positive");
+    if (!h->d_reduce) {  // per-element error and norm, then the partial sums
+        int rc = alloc(h, sizeof(double) * (size_t)(2 * h->op.nE + 1024), (void **)&h->d_reduce);
+        if (rc) return rc;
+    }
+    // the error estimate needs the last stage vector
+    const bool keep = h->store_last;
+    h->store_last = true;
+    double dt = std::min(*dt_estimate, dt_max);
+    double error = std::numeric_limits<double>::infinity(), norm = 0.0;
+    int rej = 0;
+    int rc = 0;
+    while (max_relative_error * norm < error || std::isinf(error)) {
+        const int from = h->cur;
+        rc = enqueue_step(h, from, dt);
+        if (rc) break;
+        h->cur = 1 - from;
+        rc = error_and_norm(h, dt, &error, &norm);
+        if (rc) break;
+        if (max_relative_error * norm < error || std::isinf(error)) {
+            const unsigned grid = 4 * h->num_sms;
+            if (h->mixed)
+                rewind_update<float><<<grid, 256, 0, h->stream>>>(h->sol[h->cur], err_stages<float>(h, dt, h->rk_b),
+                                                                  h->N_alloc);
+            else
+                rewind_update<double><<<grid, 256, 0, h->stream>>>(h->sol[h->cur], err_stages<double>(h, dt, h->rk_b),
+                                                                   h->N_alloc);
+            h->launches++;
+            dt = 0.8 * dt * std::pow(max_relative_error / error * norm, 1. / h->rk_order);
+            ++rej;
+            if (rej > 1000) {
+                rc = fail(h, HGG_ERR_DEVICE, "adaptive step: no accepted step after 1000 tries");
+                break;
+            }
+        }
+    }
+    h->store_last = keep;
+    if (rc) return rc;
+    *dt_estimate = 0.9 * dt * std::pow(max_relative_error / error * norm, 1. / h->rk_order);
+    *time += dt;
+    if (dt_taken) *dt_taken = dt;
+    if (rejections) *rejections = rej;
+    return check_status(h);
+}
+
+}  // extern "C"
+
+extern "C" {
+
 // ---- stand-alone set-up ------------------------------------------------------
 
 namespace {
@@ -880,6 +1060,7 @@ int hgg_create_structured(const char *description, int32_t order, int32_t physic
     int rc = hgg_create(&d, &h);
     if (rc) return rc;
     h->sp = std::move(sp);
+    butcher_error_estimate(tableau, h->rk_err, h->rk_order);
     *out = h;
     return 0;
 }

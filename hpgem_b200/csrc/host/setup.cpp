@@ -399,6 +399,21 @@ bool butcher_tableau(const std::string &name, std::vector<double> &a, std::vecto
     return true;
 }
 
+bool butcher_error_estimate(const std::string &name, std::vector<double> &error, int &order) {
+    if (name == "DormandPrince") {  // the fifth-order weights minus the fourth-order ones
+        error = {35. / 384. - 5179. / 57600., 0. - 0., 500. / 1113. - 7571. / 16695., 125. / 192. - 393. / 640.,
+                 -2187. / 6784. - -92097. / 339200., 11. / 84. - 187. / 2100., 0. - 1. / 40.};
+        order = 5;
+        return true;
+    }
+    if (name == "BogackiShampine") {  // the third-order weights minus the second-order ones
+        error = {2. / 9. - 7. / 24., 1. / 3. - 1. / 4., 4. / 9. - 1. / 3., 0. - 1. / 8.};
+        order = 3;
+        return true;
+    }
+    return false;
+}
+
 // ---------------------------------------------------------------------------
 // descriptor contents for a structured mesh
 // ---------------------------------------------------------------------------

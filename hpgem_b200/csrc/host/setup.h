@@ -83,4 +83,8 @@ StructuredProblem build_structured(const std::string &description, int order, in
 bool butcher_tableau(const std::string &name, std::vector<double> &a, std::vector<double> &b,
                      std::vector<double> &c, int &stages);
 
+// Error coefficients b_i - b*_i and order of an embedded tableau (DormandPrince.cpp:75-82,
+// order 5; BogackiShampine.cpp:61-67, order 3); false for tableaux without an error estimate.
+bool butcher_error_estimate(const std::string &name, std::vector<double> &error, int &order);
+
 }  // namespace hgg

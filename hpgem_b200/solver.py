@@ -92,6 +92,21 @@ class Handle:
         self._check(self._lib.hgg_step(self._raw, ctypes.byref(t), float(dt), int(nsteps)))
         return t.value
 
+    def step_adaptive(self, time, max_relative_error, dt_max, dt_estimate):
+        """One accepted adaptive step; returns (time, next dt estimate, dt taken, rejections)."""
+        t = ctypes.c_double(time)
+        est = ctypes.c_double(dt_estimate)
+        taken = ctypes.c_double()
+        rej = ctypes.c_int32()
+        self._check(self._lib.hgg_step_adaptive(self._raw, ctypes.byref(t), float(max_relative_error),
+                                                float(dt_max), ctypes.byref(est), ctypes.byref(taken),
+                                                ctypes.byref(rej)))
+        return t.value, est.value, taken.value, rej.value
+
+    def set_error_estimate(self, error_coefficients, order):
+        e = np.ascontiguousarray(np.asarray(error_coefficients, dtype=np.float64))
+        self._check(self._lib.hgg_set_error_estimate(self._raw, _ptr(e), int(order)))
+
     def time_derivative(self, in_vec, out_vec):
         self._check(self._lib.hgg_time_derivative(self._raw, int(in_vec), int(out_vec)))
 
@@ -165,6 +180,7 @@ class HpgemAPISimplified:
             raise ValueError("physics must be 'advection' or 'wave'")
         self.handle = None
         self.n_elements = 0
+        self.dtEstimate = math.inf
 
     # -- set-up -------------------------------------------------------------
     def readMesh(self, description):
@@ -192,6 +208,39 @@ class HpgemAPISimplified:
 
     def computeTimeSteps(self, time, dt, nsteps):
         return self.handle.step(time, dt, nsteps)
+
+    def computeOneTimeStepAdaptive(self, time, maximumRelativeError, dtMax):
+        """computeOneTimeStep(time, maximumRelativeError, dtMax) (HpgemAPISimplified_Impl.h:822-861):
+        one accepted step of the embedded tableau; the next step's estimate is kept in
+        ``dtEstimate`` (the reference keeps it in a static variable initialised from dt)."""
+        time, self.dtEstimate, self.lastDt, self.lastRejections = self.handle.step_adaptive(
+            time, maximumRelativeError, dtMax, self.dtEstimate)
+        return time
+
+    def solveAdaptive(self, initialTime, finalTime, maximumRelativeError, dt=math.inf,
+                      numberOfOutputFrames=1, u0=None):
+        """The adaptive branch of HpgemAPISimplified::solve (HpgemAPISimplified_Impl.h:976-1045):
+        steps until finalTime, each limited by dt and by the next output time and the final
+        time; returns (time, number of accepted steps)."""
+        T = finalTime - initialTime
+        if math.isfinite(dt):
+            steps = int(math.ceil(T / dt))
+            if numberOfOutputFrames > 0:
+                steps += (numberOfOutputFrames - steps % numberOfOutputFrames) % numberOfOutputFrames
+                dt = T / steps
+        outputDt = T / numberOfOutputFrames
+        outputTime = outputDt + initialTime
+        if u0 is not None:
+            self.setInitialSolution(u0)
+        self.dtEstimate = dt
+        time, n = initialTime, 0
+        while time < finalTime - 1e-14:
+            n += 1
+            time = self.computeOneTimeStepAdaptive(time, maximumRelativeError,
+                                                   min(min(dt, outputTime - time), finalTime - time))
+            if time > outputTime - 1e-12:
+                outputTime += outputDt
+        return time, n
 
     def computeTimeDerivative(self, in_vec, out_vec):
         self.handle.time_derivative(in_vec, out_vec)

@@ -196,6 +196,29 @@ int hgg_set_kernel_variant(hgg_handle *h, int32_t variant);
  * returns after it (like hgg_time_derivative, whose result it reproduces). */
 int hgg_time_derivative_static(hgg_handle *h, const double *u, double *k);
 
+/* computeOneTimeStep(time, maximumRelativeError, dtMax)
+ * (HpgemAPISimplified_Impl.h:822-861): one accepted step of an embedded tableau
+ * (DormandPrince, BogackiShampine) with the reference's error control.  A trial
+ * step of dt = min(*dt_estimate, dt_max) is taken; with error = the Euclidean
+ * norm of sum_i dt err_i k_i over all coefficients and norm = the sum over
+ * elements of the Euclidean norms of the updated solution
+ * (computeErrorAndNormOfUpdate, :719-749), it is undone (u -= dt b_j k_j) and
+ * retried with dt = 0.8 dt (max_relative_error norm / error)^(1/order) while
+ * max_relative_error * norm < error.  On return *time has advanced by the
+ * accepted dt (*dt_taken), *dt_estimate holds the next estimate
+ * 0.9 dt (max_relative_error norm / error)^(1/order) (the reference keeps it in
+ * a static variable), *rejections counts the undone tries.  dt_taken and
+ * rejections may be null.  HGG_ERR_INVALID if the tableau has no error
+ * estimate. */
+int hgg_step_adaptive(hgg_handle *h, double *time, double max_relative_error, double dt_max, double *dt_estimate,
+                      double *dt_taken, int32_t *rejections);
+
+/* Error coefficients (b_i - b*_i, one per stage) and order of the handle's
+ * embedded tableau (ButcherTableau::getErrorCoefficient / getOrder,
+ * ButcherTableau.h:58-72), for handles made by hgg_create from a descriptor;
+ * hgg_create_structured sets them for DormandPrince and BogackiShampine. */
+int hgg_set_error_estimate(hgg_handle *h, const double *error_coefficients, int32_t order);
+
 /* Number of kernel launches the library issued on this handle so far. */
 int64_t hgg_launch_count(const hgg_handle *h);
 

@@ -21,6 +21,7 @@ Butcher tableaux restate kernel/Base/TimeIntegration/{RK4Methods,DormandPrince,
 ForwardEuler,MidPoint,RK2TVD,RK3TVD,BogackiShampine}.cpp.
 """
 import ctypes
+import math
 
 import numpy as np
 
@@ -58,6 +59,16 @@ TABLEAUX = {
     "BogackiShampine": dict(order=3, A=[[0, 0, 0, 0], [1. / 2., 0, 0, 0], [0., 3. / 4., 0, 0],
                                         [2. / 9., 1. / 3., 4. / 9., 0]],
                             b=[2. / 9., 1. / 3., 4. / 9., 0.], c=[0., 1. / 5., 3. / 10., 4. / 5.]),
+}
+
+
+# error coefficients b_i - b*_i of the embedded pairs (DormandPrince.cpp:75-82,
+# BogackiShampine.cpp:61-67); the order used by the step-size control is the tableau's
+ERROR_COEFFICIENTS = {
+    "DormandPrince": [35. / 384. - 5179. / 57600., 0. - 0., 500. / 1113. - 7571. / 16695.,
+                      125. / 192. - 393. / 640., -2187. / 6784. - -92097. / 339200.,
+                      11. / 84. - 187. / 2100., 0. - 1. / 40.],
+    "BogackiShampine": [2. / 9. - 7. / 24., 1. / 3. - 1. / 4., 4. / 9. - 1. / 3., 0. - 1. / 8.],
 }
 
 
@@ -251,6 +262,45 @@ class Problem:
         if rc:
             raise RuntimeError("oracle_step failed: %d" % rc)
         return (vec[0].copy(), vec[1:].copy()) if return_stages else vec[0].copy()
+
+    def error_and_norm(self, u, stages, dt, tableau):
+        """computeErrorAndNormOfUpdate (HpgemAPISimplified_Impl.h:719-749): per element the
+        deviation sum_i (k_i dt) err_i and its squared Euclidean norm, summed, square root;
+        and the sum over elements of the Euclidean norms of u."""
+        err = ERROR_COEFFICIENTS[tableau]
+        nE = len(self.absdet)
+        uu = np.asarray(u).reshape(nE, -1)
+        error = 0.0
+        norm = 0.0
+        for e in range(nE):
+            norm += math.sqrt(float(np.dot(uu[e], uu[e])))
+            dev = np.zeros(uu.shape[1])
+            for i in range(len(err)):
+                dev += (np.asarray(stages[i]).reshape(nE, -1)[e] * dt) * err[i]
+            error += float(np.dot(dev, dev))
+        return math.sqrt(error), norm
+
+    def step_adaptive(self, u, time, max_relative_error, dt_max, dt_estimate, tableau="DormandPrince"):
+        """computeOneTimeStep(time, maximumRelativeError, dtMax) (HpgemAPISimplified_Impl.h:822-861):
+        returns (u, time, next dt estimate, accepted dt, rejected tries)."""
+        tab = TABLEAUX[tableau]
+        order = tab["order"]
+        dt = min(dt_estimate, dt_max)
+        error, norm = math.inf, 0.0
+        rejections = 0
+        while max_relative_error * norm < error or math.isinf(error):
+            u_new, stages = self.step(u, dt, 1, tableau, return_stages=True)
+            error, norm = self.error_and_norm(u_new, stages, dt, tableau)
+            if max_relative_error * norm < error or math.isinf(error):
+                for j in range(len(tab["b"])):  # the reference rewinds by subtraction
+                    u_new = u_new + (-dt * tab["b"][j]) * stages[j]
+                u = u_new
+                dt = 0.8 * dt * (max_relative_error / error * norm) ** (1.0 / order)
+                rejections += 1
+            else:
+                u = u_new
+        estimate = 0.9 * dt * (max_relative_error / error * norm) ** (1.0 / order)
+        return u, time + dt, estimate, dt, rejections
 
     def l2_error(self, u, exact, t):
         """computeTotalError (HpgemAPISimplified_Impl.h:326-401): rule of order 2p+2."""
