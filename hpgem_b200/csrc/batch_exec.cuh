@@ -237,7 +237,7 @@ size_t class_item_bytes(const BatchClass &c) {
 DenseGeom dense_geom(const hgg_handle *h, int epb) {
     const HostOperators &op = h->op;
     return DenseGeom{h->d_vol, h->d_pairs, h->d_vol_f, h->d_pairs_f, h->d_nbr, h->d_self, h->d_nbrp, h->d_mode,
-                     h->d_elem_geo, h->d_face_geo, 1.0 / op.c_inv, op.nB, epb};
+                     h->d_elem_geo, h->d_face_geo, 1.0 / op.c_inv, upwind_speed(op), op.nB, epb};
 }
 
 // host copy of the items of one stage of a class
@@ -373,7 +373,7 @@ void launch_class_stage(hgg_batch *b, const BatchClass &c, int st, cudaStream_t 
         switch (c.order) { HGG_GT(1) HGG_GT(2) HGG_GT(3) HGG_GT(4) HGG_GT(5) }
 #undef HGG_GT
     } else {
-        const bool wave = c.physics == HGG_PHYSICS_WAVE;
+        const bool wave = c.physics != HGG_PHYSICS_ADVECTION;
         switch (c.shape) {
             case HGG_SHAPE_LINE: wave ? launch_grouped_dense_any<1, 2, 1>(b, c, st, grid, s) : launch_grouped_dense_any<1, 2, 0>(b, c, st, grid, s); break;
             case HGG_SHAPE_TRIANGLE: wave ? launch_grouped_dense_any<2, 3, 1>(b, c, st, grid, s) : launch_grouped_dense_any<2, 3, 0>(b, c, st, grid, s); break;
@@ -416,7 +416,7 @@ int tune_class(hgg_batch *b, BatchClass &c) {
     if (c.kind == KIND_DENSE) {
         // elements per block: the largest that fills 256 threads, and half of it
         const hgg_handle *h0 = b->handles[c.slots[0]];
-        const int wave = c.physics == HGG_PHYSICS_WAVE;
+        const int wave = c.physics != HGG_PHYSICS_ADVECTION;
         const int rows = dense_rows(c.dim, wave, h0->op.nB);
         const int nfl = c.shape == HGG_SHAPE_LINE ? 2 : (c.shape == HGG_SHAPE_TRIANGLE ? 3
                         : (c.shape == HGG_SHAPE_SQUARE || c.shape == HGG_SHAPE_TETRAHEDRON ? 4 : 6));
@@ -660,7 +660,7 @@ int hgg_batch_add(hgg_batch *b, hgg_handle *h, double dt, int32_t nsteps, int32_
         c.S = h->S;
         c.rk_a = h->rk_a;
         c.rk_b = h->rk_b;
-        c.epb = c.kind == KIND_DENSE ? std::max(1, 256 / dense_rows(h->op.dim, h->op.physics == HGG_PHYSICS_WAVE, h->op.nB)) : 1;
+        c.epb = c.kind == KIND_DENSE ? std::max(1, 256 / dense_rows(h->op.dim, h->op.physics != HGG_PHYSICS_ADVECTION, h->op.nB)) : 1;
         c.item_bytes = class_item_bytes(c);
         c.d_items.assign(c.S, nullptr);
         for (int st = 0; st < c.S; ++st)

@@ -287,6 +287,11 @@ int launch_tensor_dim(hgg_handle *h, const StageIO &io) {
     return fail(h, HGG_ERR_UNSUPPORTED, "tensor kernel: order out of range");
 }
 
+// wave speed factor of the upwind wave flux, 0 for the central flux
+double upwind_speed(const HostOperators &op) {
+    return op.physics == HGG_PHYSICS_WAVE_UPWIND ? 1.0 / std::sqrt(op.c_inv) : 0.0;
+}
+
 // dense kernel launch for the handle's shape and physics
 template <typename KT>
 int launch_dense_any(hgg_handle *h, const StageIOT<KT> &io);
@@ -322,7 +327,7 @@ int launch_dense(hgg_handle *h, const StageIOT<KT> &io) {
     if (R > 256) return fail(h, HGG_ERR_UNSUPPORTED, "dense kernel: more than 256 coefficients per element");
     int epb = std::max(1, 256 / dense_rows(DIM, WAVE, op.nB));
     DenseGeom g{h->d_vol, h->d_pairs, h->d_vol_f, h->d_pairs_f, h->d_nbr, h->d_self, h->d_nbrp, h->d_mode,
-                h->d_elem_geo, h->d_face_geo, 1.0 / op.c_inv, op.nB, epb};
+                h->d_elem_geo, h->d_face_geo, 1.0 / op.c_inv, upwind_speed(op), op.nB, epb};
     int64_t blocks = (op.nE + epb - 1) / epb;
     const int threads = dense_threads(DIM, WAVE, op.nB, epb);
     const bool ok = dense_dispatch<DIM, NFL, WAVE>(op.nB, [&](auto nbc) {
@@ -339,7 +344,7 @@ int launch_dense(hgg_handle *h, const StageIOT<KT> &io) {
 
 template <typename KT>
 int launch_dense_any(hgg_handle *h, const StageIOT<KT> &io) {
-    const bool wave = h->op.physics == HGG_PHYSICS_WAVE;
+    const bool wave = h->op.physics != HGG_PHYSICS_ADVECTION;
     switch (h->op.shape) {
         case HGG_SHAPE_LINE: return wave ? launch_dense<KT, 1, 2, 1>(h, io) : launch_dense<KT, 1, 2, 0>(h, io);
         case HGG_SHAPE_TRIANGLE: return wave ? launch_dense<KT, 2, 3, 1>(h, io) : launch_dense<KT, 2, 3, 0>(h, io);

@@ -230,6 +230,7 @@ struct DenseGeom {
     const double *elem_geo;    // advection [E][DIM]; wave [E][DIM][DIM]
     const double *face_geo;    // advection [E][NFL]; wave [E][NFL][DIM]
     double inv_cinv;           // 1 / c_inv (wave)
+    double upwind_c;           // wave: 0 for the central flux, c = 1 / sqrt(c_inv) for the upwind flux
     int nB;
     int epb;                   // elements per block
 };
@@ -335,6 +336,7 @@ __device__ __forceinline__ void dense_stage_body(const StageIOT<KT> &io, const D
         // the wave in one dimension: G and the normal are scalars
         const int v = r / nB, i = r % nB;
         const CT G = (CT)g.elem_geo[e];
+        const CT cu = (CT)g.upwind_c;
         if (v == 0) {
             const CT *op = gvol + i;
             CT s = CT(0);
@@ -349,6 +351,12 @@ __device__ __forceinline__ void dense_stage_body(const StageIOT<KT> &io, const D
 #pragma unroll
                 for (int j = 0; j < nB; ++j) t += ops[(size_t)j * nB] * w[nB + j] - opn[(size_t)j * nB] * wn[f * R + nB + j];
                 acc -= nu * t;
+                if (cu != CT(0)) {  // upwind: c |nu| times the lifted pressure jump
+                    CT b = CT(0);
+#pragma unroll
+                    for (int j = 0; j < nB; ++j) b += ops[(size_t)j * nB] * w[j] - opn[(size_t)j * nB] * wn[f * R + j];
+                    acc -= cu * (nu < CT(0) ? -nu : nu) * b;
+                }
             }
         } else {
             // k_s = (1/cInv) [ G vol q - face jumps of q ]
@@ -357,6 +365,7 @@ __device__ __forceinline__ void dense_stage_body(const StageIOT<KT> &io, const D
 #pragma unroll
             for (int j = 0; j < nB; ++j) s += op[(size_t)j * nB] * w[j];
             acc += G * s;
+            CT up = CT(0);
             for (int f = 0; f < NFL; ++f) {
                 const CT nud = (CT)g.face_geo[(size_t)e * NFL + f];
                 const CT *ops = gpairs + (size_t)g.self_pair[e * NFL + f] * nB * nB + i;
@@ -365,8 +374,16 @@ __device__ __forceinline__ void dense_stage_body(const StageIOT<KT> &io, const D
 #pragma unroll
                 for (int j = 0; j < nB; ++j) t += ops[(size_t)j * nB] * w[j] - opn[(size_t)j * nB] * wn[f * R + j];
                 acc -= nud * t;
+                if (cu != CT(0)) {  // upwind: c |nu| times the lifted velocity jump (one component)
+                    CT b = CT(0);
+#pragma unroll
+                    for (int j = 0; j < nB; ++j)
+                        b += ops[(size_t)j * nB] * w[nB + j] - opn[(size_t)j * nB] * wn[f * R + nB + j];
+                    up += cu * (nud < CT(0) ? -nud : nud) * b;
+                }
             }
             acc *= (CT)g.inv_cinv;
+            acc -= up;
         }
     }
     stage_output(io, e * R + r, u_own, (double)acc);
@@ -445,7 +462,7 @@ __device__ __forceinline__ void wave_stage_body(const StageIOT<KT> &io, const De
     __syncthreads();
     if (!active) return;
 
-    CT P = CT(0), A[DIM], B[NFL];
+    CT P = CT(0), A[DIM], B[NFL], SP[NFL];
 #pragma unroll
     for (int c = 0; c < DIM; ++c) {
         const CT *op = gvol + (size_t)c * NB * NB + i;
@@ -473,6 +490,22 @@ __device__ __forceinline__ void wave_stage_body(const StageIOT<KT> &io, const De
         }
         P -= sp;
         B[f] = sb;
+        SP[f] = sp;
+    }
+    const CT cu = (CT)g.upwind_c;
+    CT nrm[NFL];
+    if (cu != CT(0)) {
+        // upwind: the pressure row gets c |nu| times the lifted pressure jump, velocity
+        // component d gets c (nu_d / |nu|) times the lifted normal velocity jump (nu . s)
+#pragma unroll
+        for (int f = 0; f < NFL; ++f) {
+            const double *nu = g.face_geo + ((size_t)e * NFL + f) * DIM;
+            double q = 0.0;
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) q += nu[d] * nu[d];
+            nrm[f] = (CT)sqrt(q);
+            P -= cu * nrm[f] * B[f];
+        }
     }
     stage_output(io, e * R + i, u_own[0], (double)P);
     const double *G = g.elem_geo + e * DIM * DIM;
@@ -483,7 +516,11 @@ __device__ __forceinline__ void wave_stage_body(const StageIOT<KT> &io, const De
         for (int c = 0; c < DIM; ++c) acc += (CT)G[d * DIM + c] * A[c];
 #pragma unroll
         for (int f = 0; f < NFL; ++f) acc -= (CT)g.face_geo[((size_t)e * NFL + f) * DIM + d] * B[f];
-        stage_output(io, e * R + (d + 1) * NB + i, u_own[d + 1], (double)(acc * (CT)g.inv_cinv));
+        acc *= (CT)g.inv_cinv;
+        if (cu != CT(0))
+#pragma unroll
+            for (int f = 0; f < NFL; ++f) acc -= cu * ((CT)g.face_geo[((size_t)e * NFL + f) * DIM + d] / nrm[f]) * SP[f];
+        stage_output(io, e * R + (d + 1) * NB + i, u_own[d + 1], (double)acc);
     }
 }
 

@@ -277,7 +277,8 @@ HostOperators build_operators(const hgg_problem_desc &desc) {
     if (desc.shape < HGG_SHAPE_LINE || desc.shape > HGG_SHAPE_TETRAHEDRON)
         throw std::invalid_argument("unknown shape");
     if (shape_info(desc.shape).dim != d) throw std::invalid_argument("shape does not match dim");
-    if (desc.physics != HGG_PHYSICS_ADVECTION && desc.physics != HGG_PHYSICS_WAVE)
+    if (desc.physics != HGG_PHYSICS_ADVECTION && desc.physics != HGG_PHYSICS_WAVE &&
+        desc.physics != HGG_PHYSICS_WAVE_UPWIND)
         throw std::invalid_argument("unknown physics");
     const int V = desc.physics == HGG_PHYSICS_ADVECTION ? 1 : d + 1;
     if (desc.n_vars != V) throw std::invalid_argument("n_vars must be 1 (advection) or dim+1 (wave)");
@@ -288,7 +289,7 @@ HostOperators build_operators(const hgg_problem_desc &desc) {
         !desc.face_tabs || !desc.jacobians || !desc.face_elements || !desc.face_local ||
         !desc.face_tab_index || !desc.face_normals)
         throw std::invalid_argument("missing descriptor array");
-    if (desc.physics == HGG_PHYSICS_WAVE && !(desc.c_inv > 0.0))
+    if (desc.physics != HGG_PHYSICS_ADVECTION && !(desc.c_inv > 0.0))
         throw std::invalid_argument("c_inv must be positive");
     op.shape = desc.shape;
     op.dim = d;

@@ -32,7 +32,8 @@ class Server:
         """Queues a solve.  The initial condition is either coefficients `u0` (hpGEM
         order) or a function initial(x[n, dim]) -> [n] or [n, n_vars] that the server
         projects; returns the request id."""
-        code = _native.PHYSICS_ADVECTION if physics == "advection" else _native.PHYSICS_WAVE
+        code = {"advection": _native.PHYSICS_ADVECTION, "wave": _native.PHYSICS_WAVE,
+                "wave_upwind": _native.PHYSICS_WAVE_UPWIND}[physics]
         p = np.ascontiguousarray(np.asarray(params, dtype=np.float64).reshape(-1))
         keep = [p]
         u0p, n_u0 = None, 0

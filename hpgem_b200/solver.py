@@ -172,12 +172,12 @@ class HpgemAPISimplified:
                 a[:self.dim] = np.asarray(advection, dtype=float)[:self.dim]
             self.params = a[:self.dim]
             self._physics_code = _native.PHYSICS_ADVECTION
-        elif physics == "wave":
+        elif physics in ("wave", "wave_upwind"):
             self.numberOfVariables = self.dim + 1
             self.params = np.array([float(c_inv)])
-            self._physics_code = _native.PHYSICS_WAVE
+            self._physics_code = _native.PHYSICS_WAVE if physics == "wave" else _native.PHYSICS_WAVE_UPWIND
         else:
-            raise ValueError("physics must be 'advection' or 'wave'")
+            raise ValueError("physics must be 'advection', 'wave' or 'wave_upwind'")
         self.handle = None
         self.n_elements = 0
         self.dtEstimate = math.inf
@@ -301,9 +301,13 @@ def Advection(dim, order, a, tableau="DormandPrince", **kw):
     return HpgemAPISimplified(dim, order, "advection", advection=a, tableau=tableau, **kw)
 
 
-def AcousticWave(dim, order, c_inv=1.0, tableau="RK4_4", **kw):
-    """The acoustic-wave application of ExampleMultipleVariableProblem (RK4 default, main.cpp:74-75)."""
-    return HpgemAPISimplified(dim, order, "wave", c_inv=c_inv, tableau=tableau, **kw)
+def AcousticWave(dim, order, c_inv=1.0, tableau="RK4_4", flux="central", **kw):
+    """The acoustic-wave application of ExampleMultipleVariableProblem (RK4 default, main.cpp:74-75);
+    flux "central" is the reference's, "upwind" the restated Riemann flux."""
+    if flux not in ("central", "upwind"):
+        raise ValueError("flux must be 'central' or 'upwind'")
+    return HpgemAPISimplified(dim, order, "wave" if flux == "central" else "wave_upwind", c_inv=c_inv,
+                              tableau=tableau, **kw)
 
 
 def structured_description(n, lower, upper, triangular=False, periodic=True):

@@ -103,7 +103,8 @@ def make_solver(spec, precision=0, tableau="RK4_4"):
     if spec["physics"] == "advection":
         s = Advection(dim, spec["order"], spec["params"], tableau=tableau, precision=precision)
     else:
-        s = AcousticWave(dim, spec["order"], c_inv=spec["params"][0], tableau=tableau, precision=precision)
+        s = AcousticWave(dim, spec["order"], c_inv=spec["params"][0], tableau=tableau, precision=precision,
+                         flux="upwind" if spec["physics"] == "wave_upwind" else "central")
     s.readMesh(structured_description(spec["cells"], [0.0] * dim, [1.0] * dim, spec["triangular"], True))
     if spec["physics"] == "advection":
         s.setInitialSolution(spec["u0"])
@@ -122,5 +123,5 @@ def dof(spec):
         nb = (p + 1) * (p + 2) // 2 if tri else (p + 1) ** 2
     else:
         nb = (p + 1) * (p + 2) * (p + 3) // 6 if tri else (p + 1) ** 3
-    V = dim + 1 if spec["physics"] == "wave" else 1
+    V = 1 if spec["physics"] == "advection" else dim + 1
     return cells * nb * V

@@ -11,6 +11,14 @@
  *                          strong form, central flux
  *                          (applications/ExampleMultipleVariableProblem/
  *                           AcousticWave_Impl.h:102-373)
+ *   HGG_PHYSICS_WAVE_UPWIND  the same system with the upwind (Riemann) flux:
+ *                          the central flux plus the jump penalty
+ *                          (1/2) |A_n| [[U]], which for v_t = div s,
+ *                          c_inv s_t = grad v is c |n| [[v]] / 2 in the
+ *                          first equation and c c_inv n (n . [[s]]) / (2 |n|)
+ *                          in the others, c = 1 / sqrt(c_inv).  The
+ *                          reference has the central flux only; this flux
+ *                          is the one its wave benchmark names.
  *
  * Conventions shared by every entry point:
  *   - Return value 0 on success, a negative HGG_ERR_* code otherwise; the
@@ -43,7 +51,7 @@ enum hgg_shape {
     HGG_SHAPE_TETRAHEDRON = 5
 };
 
-enum hgg_physics { HGG_PHYSICS_ADVECTION = 0, HGG_PHYSICS_WAVE = 1 };
+enum hgg_physics { HGG_PHYSICS_ADVECTION = 0, HGG_PHYSICS_WAVE = 1, HGG_PHYSICS_WAVE_UPWIND = 2 };
 
 enum hgg_precision {
     HGG_PRECISION_FP64 = 0,  /* everything in FP64 (parity form) */

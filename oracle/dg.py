@@ -33,6 +33,7 @@ from .refgeom import SHAPES, vertex_shape_functions
 
 ADVECTION = 0
 WAVE = 1
+WAVE_UPWIND = 2  # the wave with the upwind flux (restated; the reference has the central flux)
 
 TABLEAUX = {
     # RK4Methods.cpp:45-63

@@ -26,6 +26,8 @@
  *   WAVE (strong form, central)    applications/ExampleMultipleVariableProblem/
  *                                  AcousticWave_Impl.h:102-129, 169-226, 289-373
  *                                  (Jacobian scaling off, AcousticWave.h:223-233)
+ *   WAVE_UPWIND                    the same with the upwind (Riemann) flux, restated:
+ *                                  the reference has the central flux only
  * Gradients are mapped as hpGEM's H1ConformingTransformation::transformDeriv
  * (kernel/Base/H1ConformingTransformation.h:64-69): solve J^T g = g_ref.
  * The textbook LU (Golub & Van Loan, Algorithm 3.4.1) stands in for dgesv;
@@ -35,7 +37,7 @@
 #include <stdlib.h>
 #include <string.h>
 
-enum { ORACLE_ADVECTION = 0, ORACLE_WAVE = 1 };
+enum { ORACLE_ADVECTION = 0, ORACLE_WAVE = 1, ORACLE_WAVE_UPWIND = 2 };
 
 typedef struct {
     int dim, nB, nQ, nQf, V, nFL, physics;
@@ -220,9 +222,18 @@ static void face_rhs(const oracle_problem *P, long f, int side, const double *wL
                 js[k] = n[k] * (uL[0] - uR[0]);
                 jv += n[k] * (uL[k + 1] - uR[k + 1]);
             }
+            /* upwind flux (ORACLE_WAVE_UPWIND): the central terms plus (1/2) |A_n| [[U]],
+             * c |n| [[v]] / 2 and c cinv n (n . [[s]]) / (2 |n|), c = 1 / sqrt(cinv), with the
+             * jump of this side minus the other (the sign flips on the right side) */
+            double upv = 0.0, ups[3] = {0.0, 0.0, 0.0};
+            if (P->physics == ORACLE_WAVE_UPWIND) {
+                double c = 1.0 / sqrt(P->cinv), sg = side == 0 ? 1.0 : -1.0;
+                upv = 0.5 * c * area * (uL[0] - uR[0]) * sg;
+                for (int k = 0; k < d; ++k) ups[k] = 0.5 * c * P->cinv * (n[k] / area) * jv * sg;
+            }
             for (int i = 0; i < nB; ++i) {
-                integrand[0 * nB + i] = -0.5 * ps[i] * jv;
-                for (int k = 0; k < d; ++k) integrand[(k + 1) * nB + i] = -0.5 * ps[i] * js[k];
+                integrand[0 * nB + i] = -0.5 * ps[i] * jv - ps[i] * upv;
+                for (int k = 0; k < d; ++k) integrand[(k + 1) * nB + i] = -0.5 * ps[i] * js[k] - ps[i] * ups[k];
             }
             accumulate(res, integrand, V * nB, P->wqf[q], q == 0);
         }
@@ -237,7 +248,7 @@ static int mass_solve(const oracle_problem *P, long e, double *x, double *M, int
         const double *ph = P->phi + (long)q * nB;
         double s = P->wq[q] * absJ;
         for (int iv = 0; iv < V; ++iv) {
-            double c = (P->physics == ORACLE_WAVE && iv > 0) ? P->cinv : 1.0;
+            double c = (P->physics != ORACLE_ADVECTION && iv > 0) ? P->cinv : 1.0;
             for (int ib = 0; ib < nB; ++ib)
                 for (int jb = 0; jb < nB; ++jb) {
                     double val = ph[ib] * ph[jb] * c;
@@ -373,12 +384,12 @@ int oracle_project(const oracle_problem *P, const double *values, double *out) {
             const double *u0 = values + (e * P->nQ + q) * V;
             for (int v = 0; v < V; ++v)
                 for (int i = 0; i < nB; ++i) {
-                    double c = (P->physics == ORACLE_WAVE && v > 0) ? P->cinv : 1.0;
+                    double c = (P->physics != ORACLE_ADVECTION && v > 0) ? P->cinv : 1.0;
                     double val = ph[i] * u0[v] * c;
-                    if (P->physics == ORACLE_WAVE) val *= absJ;
+                    if (P->physics != ORACLE_ADVECTION) val *= absJ;
                     s.tmp[v * nB + i] = val;
                 }
-            accumulate(r, s.tmp, N, P->wq[q] * (P->physics == ORACLE_WAVE ? 1.0 : absJ), q == 0);
+            accumulate(r, s.tmp, N, P->wq[q] * (P->physics != ORACLE_ADVECTION ? 1.0 : absJ), q == 0);
         }
         if (mass_solve(P, e, r, s.M, s.piv)) { scratch_free(&s); return -3; }
     }

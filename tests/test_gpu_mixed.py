@@ -13,7 +13,7 @@ Tolerances (FP32 unit round-off 6e-8):
 import numpy as np
 import pytest
 
-from oracle.dg import ADVECTION, WAVE, Problem
+from oracle.dg import ADVECTION, WAVE, WAVE_UPWIND, Problem
 from oracle.mesh import mesh_from_description
 
 import hpgem_b200
@@ -76,6 +76,7 @@ MIXED_CASES = [
     ([2, 2, 2], True, 2, "wave", [1.0], "RK4_4", 1e-3, 8),
     ([6, 6], True, 2, "wave", [1.0], "DormandPrince", 1e-3, 5),
     ([16], False, 3, "wave", [2.0], "RK4_4", 1e-3, 10),
+    ([2, 2, 2], True, 2, "wave_upwind", [1.0], "RK4_4", 1e-3, 8),
     # above 20 basis functions the mixed form contracts in FP64 (FP32 stage vectors):
     # triangles at p = 5, 100 steps at the batched set's CFL dt = 0.2 h / (2p + 1)
     ([16, 16], True, 5, "advection", [0.6, 0.8], "RK4_4", 0.2 / 16 / 11, 100),
@@ -91,7 +92,8 @@ def test_mixed_form_on_tensor_and_dense_kernels(case):
         prob = Problem(mesh_from_description(description), p, ADVECTION, a=params)
         u0 = prob.project(lambda x: np.sin(2 * np.pi * x).prod(axis=1)[:, None])
     else:
-        prob = Problem(mesh_from_description(description), p, WAVE, cinv=params[0])
+        prob = Problem(mesh_from_description(description), p, WAVE_UPWIND if physics == "wave_upwind" else WAVE,
+                       cinv=params[0])
         u0 = prob.project(lambda x: np.concatenate([np.sin(2 * np.pi * x[:, :1]), 0.3 * np.cos(2 * np.pi * x)], axis=1))
     ref = prob.step(u0, dt, steps, tableau)
     res = {}
@@ -99,7 +101,8 @@ def test_mixed_form_on_tensor_and_dense_kernels(case):
         if physics == "advection":
             s = hpgem_b200.Advection(d, p, params, tableau=tableau, precision=prec)
         else:
-            s = hpgem_b200.AcousticWave(d, p, c_inv=params[0], tableau=tableau, precision=prec)
+            s = hpgem_b200.AcousticWave(d, p, c_inv=params[0], tableau=tableau, precision=prec,
+                                        flux="upwind" if physics == "wave_upwind" else "central")
         s.readMesh(description)
         s.setTimeIntegrationVector(0, u0)
         s.computeTimeSteps(0.0, dt, steps)

@@ -24,7 +24,7 @@ import math
 import numpy as np
 import pytest
 
-from oracle.dg import ADVECTION, WAVE, Problem
+from oracle.dg import ADVECTION, WAVE, WAVE_UPWIND, Problem
 from oracle.mesh import mesh_from_description
 
 import hpgem_b200
@@ -66,13 +66,14 @@ def run_pair(description, p, physics, params, tableau, dt, nsteps, seed=0, stage
         u0 = prob.project(lambda x: sine_field(x)[:, None])
         solver = hpgem_b200.Advection(dim, p, params, tableau=tableau)
     else:
-        prob = Problem(mesh, p, WAVE, cinv=params[0])
+        prob = Problem(mesh, p, WAVE_UPWIND if physics == "wave_upwind" else WAVE, cinv=params[0])
         rng = np.random.default_rng(seed)
         k = rng.integers(1, 3, size=(dim,))
         u0 = prob.project(lambda x: np.stack(
             [np.sin(2 * np.pi * (x @ k))] + [0.3 * np.cos(2 * np.pi * x[:, i]) for i in range(dim)],
             axis=1))
-        solver = hpgem_b200.AcousticWave(dim, p, c_inv=params[0], tableau=tableau)
+        solver = hpgem_b200.AcousticWave(dim, p, c_inv=params[0], tableau=tableau,
+                                         flux="upwind" if physics == "wave_upwind" else "central")
     solver.readMesh(description)
     solver.handle.set_kernel_variant(variant)
     solver.setTimeIntegrationVector(0, u0)
@@ -301,3 +302,25 @@ def test_invalid_inputs_fail_loudly():
         hpgem_b200.Advection(2, 6, [1.0, 0.5]).readMesh(desc([4, 4]))
     with pytest.raises(_native.NativeError):
         hpgem_b200.Advection(2, 2, [1.0, 0.5], tableau="NoSuchTableau").readMesh(desc([4, 4]))
+
+
+UPWIND_CASES = [
+    # cells, triangular, order, c_inv: every dense wave body (1D rows, 2D/3D shared rows)
+    ([2, 2, 2], True, 2, 1.0),
+    ([4, 4], True, 3, 0.5),
+    ([4, 3], False, 2, 2.0),
+    ([6], False, 3, 1.5),
+]
+
+
+@pytest.mark.parametrize("case", UPWIND_CASES, ids=lambda c: "%dD-%s-p%d" % (len(c[0]), "tri" if c[1] else "box", c[2]))
+def test_wave_upwind_flux_against_oracle(case):
+    """The upwind (Riemann) flux of the acoustic wave, restated (the reference has the
+    central flux): solution and stage derivatives against the oracle's restatement."""
+    cells, tri, p, cinv = case
+    got, ref, solver, gk, rk = run_pair(desc(cells, triangular=tri), p, "wave_upwind", [cinv], "RK4_4",
+                                        2e-3, 4, stages=True)
+    assert solver.handle.kernel_kind == "dense"
+    assert rel_err(got, ref) < solver.solution_rtol
+    for a, b in zip(gk, rk):
+        assert rel_err(a, b) < solver.stage_rtol
