@@ -23,7 +23,7 @@ EXPORTED = ["hgg_create", "hgg_destroy", "hgg_last_error", "hgg_set_state", "hgg
             "hgg_kernel_kind", "hgg_set_store_last_stage", "hgg_set_stream", "hgg_set_kernel_variant", "hgg_launch_count",
             "hgg_create_structured", "hgg_structured_descriptor", "hgg_free_descriptor",
             "hgg_quadrature_points", "hgg_num_quadrature_points",
-            "hgg_project", "hgg_num_error_points", "hgg_error_points", "hgg_l2_error",
+            "hgg_project", "hgg_num_error_points", "hgg_error_points", "hgg_l2_error", "hgg_max_error",
             "hgg_time_derivative_static", "hgg_step_adaptive", "hgg_set_error_estimate",
             "hgg_batch_create", "hgg_batch_destroy", "hgg_batch_last_error", "hgg_batch_add",
             "hgg_batch_remove", "hgg_batch_step", "hgg_batch_synchronize", "hgg_batch_remaining",
@@ -136,6 +136,7 @@ def load():
         "hgg_num_error_points": (ctypes.c_int32, [H]),
         "hgg_error_points": (ctypes.c_int, [H, P]),
         "hgg_l2_error": (ctypes.c_int, [H, ctypes.c_int32, P, ctypes.POINTER(ctypes.c_double)]),
+        "hgg_max_error": (ctypes.c_int, [H, ctypes.c_int32, P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -64,7 +64,11 @@ struct hgg_handle {
     bool tensor_layout = false;       // device vectors in tensor order (signs folded)
     bool tiled = false;               // ... and in tiles of 32 elements, coefficient-major (slice kernel)
     double *d_scratch = nullptr;      // one vector, for layout conversion of set/get_state
-    double *d_reduce = nullptr;       // adaptive steps: per-element error and norm, partial sums
+    double *d_reduce = nullptr;       // adaptive steps and error norms: per-element values, partial sums
+    double *d_exact = nullptr;        // error norms: the caller's exact values on the device
+    size_t exact_cap = 0;
+    double *d_maxbuf = nullptr;
+    double *d_err_basis = nullptr, *d_err_w = nullptr, *d_elem_basis = nullptr, *d_absdet = nullptr;
     int32_t *d_tpos = nullptr;        // hpGEM index -> tensor position
     double *d_tsign = nullptr;
     // slice kernel (hexahedra, p = 3): per-element records of SliceShape::GR doubles
@@ -1120,33 +1124,181 @@ int hgg_project(hgg_handle *h, const double *values, int32_t vec) {
     return hgg_set_state(h, vec, out.data());
 }
 
+}  // extern "C"
+
+// ---- error norms on the device -------------------------------------------------
+// computeTotalError (HpgemAPISimplified_Impl.h:370-401, rule of order 2p+2) and
+// computeMaxError (:499-530, the element rule): the caller gives the exact
+// solution's values at the points (hgg_error_points / hgg_quadrature_points); one
+// thread per element evaluates the discrete solution there and accumulates, then
+// the elements' results are summed in a fixed order (L2) or maximised (max).
+
+// per element: sum_q w_q |J_e| sum_v (exact - u_h)^2, the host loop's order
+__global__ void element_l2_error(const double *u, const double *exact, const double *basis, const double *w,
+                                 const double *absdet, int nq, int nb, int V, int64_t n_elements, double *out) {
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= n_elements) return;
+    double loc = 0.0;
+    for (int q = 0; q < nq; ++q) {
+        double s = 0.0;
+        for (int v = 0; v < V; ++v) {
+            double uh = 0.0;
+            for (int j = 0; j < nb; ++j) uh += basis[q * nb + j] * u[(e * V + v) * nb + j];
+            const double diff = exact[(e * nq + q) * V + v] - uh;
+            s += diff * diff;
+        }
+        loc += w[q] * absdet[e] * s;
+    }
+    out[e] = loc;
+}
+
+// per element and variable: max_q |u_h - exact| at the element rule's points
+__global__ void element_max_error(const double *u, const double *exact, const double *basis, int nq, int nb, int V,
+                                  int64_t n_elements, double *out) {
+    const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= n_elements) return;
+    for (int v = 0; v < V; ++v) {
+        double m = 0.0;
+        for (int q = 0; q < nq; ++q) {
+            double uh = 0.0;
+            for (int j = 0; j < nb; ++j) uh += u[(e * V + v) * nb + j] * basis[q * nb + j];
+            const double d = fabs(uh - exact[(e * nq + q) * V + v]);
+            if (d > m) m = d;
+        }
+        out[v * n_elements + e] = m;
+    }
+}
+
+// out[v] = max over rows of a[v][:], one block per variable
+__global__ void max_per_row(const double *a, int64_t n, double *out) {
+    __shared__ double sm[kSumThreads];
+    const double *row = a + blockIdx.x * n;
+    double m = 0.0;
+    for (int64_t i = threadIdx.x; i < n; i += kSumThreads) m = fmax(m, row[i]);
+    sm[threadIdx.x] = m;
+    __syncthreads();
+    for (int w = kSumThreads / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) sm[threadIdx.x] = fmax(sm[threadIdx.x], sm[threadIdx.x + w]);
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[blockIdx.x] = sm[0];
+}
+
+namespace {
+
+// a device view of vector `vec` in hpGEM order (element-major, FP64): the vector itself
+// when it is stored that way, else its conversion in the scratch vector
+int hpgem_order_view(hgg_handle *h, int vec, const double **view) {
+    void *d = vector_ptr(h, vec);
+    if (!d) return fail(h, HGG_ERR_INVALID, "vector id out of range");
+    const bool f = vector_is_float(h, vec);
+    if (!h->tensor_layout && !f) {
+        *view = static_cast<const double *>(d);
+        return 0;
+    }
+    const unsigned grid = 4 * h->num_sms;
+    if (h->tensor_layout && f)
+        from_tensor_order<float><<<grid, 256, 0, h->stream>>>(static_cast<const float *>(d), h->d_scratch, h->d_tpos,
+                                                               h->d_tsign, h->op.nB, h->N, h->tiled);
+    else if (h->tensor_layout)
+        from_tensor_order<double><<<grid, 256, 0, h->stream>>>(static_cast<const double *>(d), h->d_scratch,
+                                                                h->d_tpos, h->d_tsign, h->op.nB, h->N, h->tiled);
+    else
+        convert_vector<<<grid, 256, 0, h->stream>>>(static_cast<const float *>(d), h->d_scratch, h->N);
+    h->launches++;
+    HGG_CUDA(h, cudaGetLastError());
+    *view = h->d_scratch;
+    return 0;
+}
+
+// device copy of the caller's exact values (kept for the next call of the same size)
+int exact_on_device(hgg_handle *h, const double *exact, size_t count, const double **out) {
+    if (count > h->exact_cap) {
+        if (h->d_exact) {
+            cudaStreamSynchronize(h->stream);
+            for (auto it = h->bufs.begin(); it != h->bufs.end(); ++it)
+                if (it->p == h->d_exact) {
+                    cudaFree(it->p);
+                    h->bufs.erase(it);
+                    break;
+                }
+            h->d_exact = nullptr;
+        }
+        int rc = alloc(h, sizeof(double) * count, (void **)&h->d_exact);
+        if (rc) return rc;
+        h->exact_cap = count;
+    }
+    HGG_CUDA(h, cudaMemcpyAsync(h->d_exact, exact, sizeof(double) * count, cudaMemcpyHostToDevice, h->stream));
+    *out = h->d_exact;
+    return 0;
+}
+
+int error_tables(hgg_handle *h) {
+    if (h->d_err_basis) return 0;
+    const StructuredProblem &P = *h->sp;
+    int rc;
+    if ((rc = upload(h, P.error_basis, &h->d_err_basis)) || (rc = upload(h, P.error_rule.weights, &h->d_err_w)) ||
+        (rc = upload(h, P.basis_values, &h->d_elem_basis)) || (rc = upload(h, h->op.abs_det, &h->d_absdet)))
+        return rc;
+    if (!h->d_reduce) {
+        rc = alloc(h, sizeof(double) * (size_t)(2 * h->op.nE + 1024), (void **)&h->d_reduce);
+        if (rc) return rc;
+    }
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
 int hgg_l2_error(hgg_handle *h, int32_t vec, const double *exact, double *error) {
     if (!h || !exact || !error) return fail(h, HGG_ERR_INVALID, "null argument");
     if (!h->sp) return fail(h, HGG_ERR_UNSUPPORTED, "error norms need a handle built from a structured mesh");
     if (h->sp->error_rule.size() == 0)
         return fail(h, HGG_ERR_UNSUPPORTED, "no quadrature rule of order 2p+2 for this shape");
-    std::vector<double> u((size_t)h->N);
-    int rc = hgg_get_state(h, vec, u.data());
-    if (rc) return rc;
-    const StructuredProblem &P = *h->sp;
+    int rc = error_tables(h);
+    const double *u = nullptr, *ex = nullptr;
     const HostOperators &op = h->op;
-    const int nB = op.nB, V = op.V, nQ = P.error_rule.size();
+    const int nQ = h->sp->error_rule.size();
+    if (rc || (rc = hpgem_order_view(h, vec, &u)) ||
+        (rc = exact_on_device(h, exact, (size_t)op.nE * nQ * op.V, &ex)))
+        return rc;
+    double *per = h->d_reduce, *pa = h->d_reduce + 2 * op.nE, *pb = pa + 256;
+    element_l2_error<<<(unsigned)((op.nE + 255) / 256), 256, 0, h->stream>>>(u, ex, h->d_err_basis, h->d_err_w,
+                                                                            h->d_absdet, nQ, op.nB, op.V, op.nE, per);
+    sum_pairs<<<256, kSumThreads, 0, h->stream>>>(per, per, op.nE, pa, pb);
+    sum_pairs<<<1, kSumThreads, 0, h->stream>>>(pa, pa, 256, pa + 512, pb + 512);
+    h->launches += 3;
+    HGG_CUDA(h, cudaGetLastError());
     double total = 0.0;
-    for (int64_t e = 0; e < op.nE; ++e) {
-        double loc = 0.0;
-        for (int q = 0; q < nQ; ++q) {
-            double s = 0.0;
-            for (int v = 0; v < V; ++v) {
-                double uh = 0.0;
-                for (int j = 0; j < nB; ++j) uh += P.error_basis[q * nB + j] * u[(e * V + v) * nB + j];
-                double diff = exact[(e * nQ + q) * V + v] - uh;
-                s += diff * diff;
-            }
-            loc += P.error_rule.weights[q] * op.abs_det[e] * s;
-        }
-        total += loc;
-    }
+    HGG_CUDA(h, cudaMemcpyAsync(&total, pa + 512, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    HGG_CUDA(h, cudaStreamSynchronize(h->stream));
     *error = std::sqrt(std::fabs(total));
+    return 0;
+}
+
+int hgg_max_error(hgg_handle *h, int32_t vec, const double *exact, double *max_error) {
+    if (!h || !exact || !max_error) return fail(h, HGG_ERR_INVALID, "null argument");
+    if (!h->sp) return fail(h, HGG_ERR_UNSUPPORTED, "error norms need a handle built from a structured mesh");
+    int rc = error_tables(h);
+    const double *u = nullptr, *ex = nullptr;
+    const HostOperators &op = h->op;
+    const int nQ = h->sp->rule.size();
+    if (rc || (rc = hpgem_order_view(h, vec, &u)) ||
+        (rc = exact_on_device(h, exact, (size_t)op.nE * nQ * op.V, &ex)))
+        return rc;
+    if (!h->d_maxbuf) {  // per element and variable, then per variable
+        rc = alloc(h, sizeof(double) * ((size_t)op.V * op.nE + op.V), (void **)&h->d_maxbuf);
+        if (rc) return rc;
+    }
+    double *per = h->d_maxbuf, *res = h->d_maxbuf + (int64_t)op.V * op.nE;
+    element_max_error<<<(unsigned)((op.nE + 255) / 256), 256, 0, h->stream>>>(u, ex, h->d_elem_basis, nQ, op.nB,
+                                                                             op.V, op.nE, per);
+    max_per_row<<<op.V, kSumThreads, 0, h->stream>>>(per, op.nE, res);
+    h->launches += 2;
+    HGG_CUDA(h, cudaGetLastError());
+    HGG_CUDA(h, cudaMemcpyAsync(max_error, res, sizeof(double) * op.V, cudaMemcpyDeviceToHost, h->stream));
+    HGG_CUDA(h, cudaStreamSynchronize(h->stream));
     return 0;
 }
 

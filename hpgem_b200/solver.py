@@ -140,6 +140,13 @@ class Handle:
         self._check(self._lib.hgg_error_points(self._raw, _ptr(out)))
         return out.reshape(n_elements, n, dim)
 
+    def max_error(self, vec, exact_values, n_vars):
+        """Per variable, max |u_h - exact| at the element quadrature points (exact given there)."""
+        a = np.ascontiguousarray(np.asarray(exact_values, dtype=np.float64).reshape(-1))
+        out = np.zeros(int(n_vars), dtype=np.float64)
+        self._check(self._lib.hgg_max_error(self._raw, int(vec), _ptr(a), _ptr(out)))
+        return out
+
     def l2_error(self, vec, exact_values):
         a = np.ascontiguousarray(exact_values, dtype=np.float64).reshape(-1)
         err = ctypes.c_double()
@@ -285,6 +292,13 @@ class HpgemAPISimplified:
         x = self.handle.error_points(self.n_elements, self.dim)
         vals = np.asarray(exact(x.reshape(-1, self.dim), time), dtype=float)
         return self.handle.l2_error(vec, vals.reshape(-1, self.numberOfVariables))
+
+    def computeMaxError(self, exact, time, vec=0):
+        """computeMaxError (HpgemAPISimplified_Impl.h:499-530): per variable, the largest
+        |u_h - exact| at the element quadrature points; exact(x[n, dim], t) -> [n] or [n, V]."""
+        x = self.quadraturePoints()
+        vals = np.asarray(exact(x.reshape(-1, self.dim), time), dtype=float)
+        return self.handle.max_error(vec, vals.reshape(-1, self.numberOfVariables), self.numberOfVariables)
 
 
 def _basis_count(dim, description, p):

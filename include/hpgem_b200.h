@@ -266,6 +266,13 @@ int32_t hgg_num_error_points(const hgg_handle *h);
 int hgg_error_points(const hgg_handle *h, double *xyz);
 int hgg_l2_error(hgg_handle *h, int32_t vec, const double *exact, double *error);
 
+/* computeMaxError (HpgemAPISimplified_Impl.h:499-530 with :406-463): per
+ * variable, the largest |u_h - exact| over every element's quadrature points
+ * (the element rule of hgg_quadrature_points), exact values given there as
+ * exact[n_elements][n_quad][n_vars]; max_error receives n_vars values.  Both
+ * norms are evaluated on the device; only the exact values cross to it. */
+int hgg_max_error(hgg_handle *h, int32_t vec, const double *exact, double *max_error);
+
 /* ---- many problems at once ------------------------------------------------
  * No counterpart in the reference (hpGEM advances one mesh per process).  A
  * batch advances many independent problems, each an existing handle with its
