@@ -22,6 +22,7 @@ EXPORTED = ["hgg_create", "hgg_destroy", "hgg_last_error", "hgg_set_state", "hgg
             "hgg_step", "hgg_time_derivative", "hgg_synchronize", "hgg_vector_length",
             "hgg_kernel_kind", "hgg_set_store_last_stage", "hgg_set_stream", "hgg_set_kernel_variant", "hgg_launch_count",
             "hgg_create_structured", "hgg_structured_descriptor", "hgg_free_descriptor",
+            "hgg_create_mesh_file", "hgg_mesh_file_descriptor",
             "hgg_quadrature_points", "hgg_num_quadrature_points",
             "hgg_project", "hgg_num_error_points", "hgg_error_points", "hgg_l2_error", "hgg_max_error",
             "hgg_time_derivative_static", "hgg_step_adaptive", "hgg_set_error_estimate",
@@ -130,6 +131,11 @@ def load():
                                                      ctypes.c_char_p, ctypes.c_int32,
                                                      ctypes.POINTER(ProblemDesc), ctypes.POINTER(H)]),
         "hgg_free_descriptor": (None, [H]),
+        "hgg_create_mesh_file": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int32, ctypes.c_int32, P,
+                                                ctypes.c_char_p, ctypes.c_int32, ctypes.POINTER(H)]),
+        "hgg_mesh_file_descriptor": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int32, ctypes.c_int32, P,
+                                                    ctypes.c_char_p, ctypes.c_int32,
+                                                    ctypes.POINTER(ProblemDesc), ctypes.POINTER(H)]),
         "hgg_quadrature_points": (ctypes.c_int, [H, P]),
         "hgg_num_quadrature_points": (ctypes.c_int32, [H]),
         "hgg_project": (ctypes.c_int, [H, P, ctypes.c_int32]),

@@ -6,7 +6,9 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <fstream>
 #include <limits>
+#include <sstream>
 #include <memory>
 #include <mutex>
 #include <stdexcept>
@@ -1052,6 +1054,58 @@ int hgg_structured_descriptor(const char *description, int32_t order, int32_t ph
 }
 
 void hgg_free_descriptor(void *owner) { delete static_cast<StructuredProblem *>(owner); }
+
+}  // extern "C"
+
+namespace {
+// the problem of a mesh file (text read here, parsed by read_mesh2)
+int mesh_file_problem(const char *path, int32_t order, int32_t physics, const double *params, const char *tableau,
+                      StructuredProblem &P) {
+    std::ifstream in(path, std::ios::binary);
+    if (!in) return fail(nullptr, HGG_ERR_INVALID, std::string("cannot open mesh file ") + path);
+    std::stringstream text;
+    text << in.rdbuf();
+    try {
+        P = build_problem(read_mesh2(text.str()), order, physics, params, tableau);
+    } catch (const std::exception &ex) {
+        return fail(nullptr, HGG_ERR_INVALID, ex.what());
+    }
+    return 0;
+}
+}  // namespace
+
+extern "C" {
+
+int hgg_mesh_file_descriptor(const char *path, int32_t order, int32_t physics, const double *params,
+                             const char *tableau, int32_t precision, hgg_problem_desc *out, void **owner) {
+    if (!path || !tableau || !out || !owner) return fail(nullptr, HGG_ERR_INVALID, "null argument");
+    *owner = nullptr;
+    std::unique_ptr<StructuredProblem> sp(new (std::nothrow) StructuredProblem());
+    if (!sp) return fail(nullptr, HGG_ERR_NOMEM, "host allocation failed");
+    int rc = mesh_file_problem(path, order, physics, params, tableau, *sp);
+    if (rc) return rc;
+    fill_descriptor(*sp, precision, *out);
+    *owner = sp.release();
+    return 0;
+}
+
+int hgg_create_mesh_file(const char *path, int32_t order, int32_t physics, const double *params,
+                         const char *tableau, int32_t precision, hgg_handle **out) {
+    if (!path || !out || !tableau) return fail(nullptr, HGG_ERR_INVALID, "null argument");
+    *out = nullptr;
+    std::unique_ptr<StructuredProblem> sp(new StructuredProblem());
+    int rc = mesh_file_problem(path, order, physics, params, tableau, *sp);
+    if (rc) return rc;
+    hgg_problem_desc d;
+    fill_descriptor(*sp, precision, d);
+    hgg_handle *h = nullptr;
+    rc = hgg_create(&d, &h);
+    if (rc) return rc;
+    h->sp = std::move(sp);
+    butcher_error_estimate(tableau, h->rk_err, h->rk_order);
+    *out = h;
+    return 0;
+}
 
 int hgg_create_structured(const char *description, int32_t order, int32_t physics, const double *params,
                           const char *tableau, int32_t precision, hgg_handle **out) {

@@ -289,7 +289,15 @@ Mesh structured_mesh(const StructuredDescription &d) {
         }
     }
 
-    // pair faces by their node sets
+    pair_faces(m);
+    return m;
+}
+
+// Pairs the elements' faces by their (global) node sets, in order of first
+// appearance; periodic copies of a node share its number, so periodic faces pair.
+void pair_faces(Mesh &m) {
+    const ShapeInfo &si = shape_info(m.shape);
+    const int dim = m.dim;
     const int fv = dim == 1 ? 1 : si.face_vertices;
     std::unordered_map<FaceKey, int64_t, FaceKeyHash> open;
     open.reserve((size_t)(m.n_elements * si.n_faces / 2 + 16));
@@ -324,6 +332,88 @@ Mesh structured_mesh(const StructuredDescription &d) {
             }
         }
     }
+}
+
+// A "mesh 2" file as the Preprocessor writes it and MeshManipulator::readMesh
+// reads it: "mesh 2"; "nNodes nElements dim [nFaces [nEdges]]"; a partition
+// line; "zones", their count and names; "nodes", then per node a partition line
+// and "k x_1 ... x_{k dim}" (k coordinate copies, hexadecimal floating point;
+// periodic nodes have several); "elements", then per element
+// "n node_1 copy_1 ... node_n copy_n zone ..." and a shadow line.  Faces are
+// paired from the element nodes as for the structured generator.
+Mesh read_mesh2(const std::string &text) {
+    std::vector<std::string> lines;
+    {
+        std::istringstream in(text);
+        std::string ln;
+        while (std::getline(in, ln)) {
+            const size_t a = ln.find_first_not_of(" \t\r"), b = ln.find_last_not_of(" \t\r");
+            lines.push_back(a == std::string::npos ? std::string() : ln.substr(a, b - a + 1));
+        }
+    }
+    auto bad = [](const std::string &what) { return std::invalid_argument("mesh file: " + what); };
+    if (lines.size() < 3 || lines[0] != "mesh 2") throw bad("first line is not \"mesh 2\"");
+    std::istringstream head(lines[1]);
+    int64_t n_nodes = -1, n_elem = -1;
+    int dim = -1;
+    head >> n_nodes >> n_elem >> dim;
+    if (n_nodes <= 0 || n_elem <= 0 || dim < 1 || dim > 3) throw bad("bad header \"" + lines[1] + "\"");
+    size_t i = 2;
+    while (i < lines.size() && lines[i] != "zones") ++i;
+    if (i + 1 >= lines.size()) throw bad("no zones section");
+    const int n_zones = std::stoi(lines[i + 1]);
+    i += 2 + n_zones;
+    if (i >= lines.size() || lines[i] != "nodes") throw bad("no nodes section");
+    ++i;
+    std::vector<std::vector<double>> node_coords((size_t)n_nodes);
+    for (int64_t nd = 0; nd < n_nodes; ++nd) {
+        ++i;  // partition line
+        if (i >= lines.size()) throw bad("truncated nodes section");
+        const char *c = lines[i].c_str();
+        char *end = nullptr;
+        const long k = std::strtol(c, &end, 10);
+        if (k < 1) throw bad("node without coordinates");
+        c = end;
+        for (long j = 0; j < k * dim; ++j) {
+            const double v = std::strtod(c, &end);  // reads hexadecimal floating point
+            if (end == c) throw bad("node coordinate");
+            node_coords[nd].push_back(v);
+            c = end;
+        }
+        ++i;
+    }
+    if (i >= lines.size() || lines[i] != "elements") throw bad("no elements section");
+    ++i;
+    Mesh m;
+    m.dim = dim;
+    m.n_elements = n_elem;
+    for (int64_t e = 0; e < n_elem; ++e, i += 2) {
+        if (i >= lines.size()) throw bad("truncated elements section");
+        std::istringstream el(lines[i]);
+        int nv = 0;
+        el >> nv;
+        const int shape = dim == 1 ? (nv == 2 ? LINE : -1)
+                        : dim == 2 ? (nv == 3 ? TRIANGLE : nv == 4 ? SQUARE : -1)
+                                   : (nv == 4 ? TETRAHEDRON : nv == 8 ? CUBE : -1);
+        if (shape < 0) throw bad("element with " + std::to_string(nv) + " vertices in " + std::to_string(dim) + "D");
+        if (e == 0) {
+            m.shape = shape;
+            m.n_vertices = nv;
+            m.nodes.resize((size_t)n_elem * nv);
+            m.coords.resize((size_t)n_elem * nv * dim);
+        } else if (shape != m.shape) {
+            throw bad("mixed element shapes are not supported");
+        }
+        for (int v = 0; v < nv; ++v) {
+            int64_t nd = -1, copy = -1;
+            el >> nd >> copy;
+            if (!el || nd < 0 || nd >= n_nodes || copy < 0 || (copy + 1) * dim > (int64_t)node_coords[nd].size())
+                throw bad("element vertex out of range");
+            m.nodes[e * nv + v] = nd;
+            for (int k = 0; k < dim; ++k) m.coords[(e * nv + v) * dim + k] = node_coords[nd][copy * dim + k];
+        }
+    }
+    pair_faces(m);
     return m;
 }
 
@@ -419,8 +509,12 @@ bool butcher_error_estimate(const std::string &name, std::vector<double> &error,
 // ---------------------------------------------------------------------------
 StructuredProblem build_structured(const std::string &description, int order, int physics,
                                    const double *params, const std::string &tableau) {
+    return build_problem(structured_mesh(parse_structured(description)), order, physics, params, tableau);
+}
+
+StructuredProblem build_problem(Mesh mesh, int order, int physics, const double *params, const std::string &tableau) {
     StructuredProblem P;
-    P.mesh = structured_mesh(parse_structured(description));
+    P.mesh = std::move(mesh);
     const Mesh &m = P.mesh;
     const ShapeInfo &si = shape_info(m.shape);
     const int d = m.dim;

@@ -52,6 +52,12 @@ struct Mesh {
 // StructuredReader (applications/Preprocessor/lib/hpgem.cpp:55-265) + face pairing.
 Mesh structured_mesh(const StructuredDescription &d);
 
+// Face pairing by global node sets (periodic copies of a node share its number).
+void pair_faces(Mesh &m);
+
+// A Preprocessor "mesh 2" file's text (MeshManipulator::readMesh's input) -> Mesh.
+Mesh read_mesh2(const std::string &text);
+
 // Element reference point -> physical point through the vertex map.
 void reference_to_physical(const Mesh &m, int64_t e, const double *xi, double *x);
 
@@ -79,6 +85,7 @@ struct StructuredProblem {
 
 StructuredProblem build_structured(const std::string &description, int order, int physics,
                                    const double *params, const std::string &tableau);
+StructuredProblem build_problem(Mesh mesh, int order, int physics, const double *params, const std::string &tableau);
 
 bool butcher_tableau(const std::string &name, std::vector<double> &a, std::vector<double> &b,
                      std::vector<double> &c, int &stages);

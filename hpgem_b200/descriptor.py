@@ -18,13 +18,22 @@ def _arr(ptr, shape, dtype):
 
 
 def structured_descriptor(description, order, physics, params, tableau="RK4_4"):
+    return _descriptor("hgg_structured_descriptor", description, order, physics, params, tableau)
+
+
+def mesh_file_descriptor(path, order, physics, params, tableau="RK4_4"):
+    """The descriptor of a Preprocessor "mesh 2" file (hgg_mesh_file_descriptor)."""
+    return _descriptor("hgg_mesh_file_descriptor", path, order, physics, params, tableau)
+
+
+def _descriptor(entry, source, order, physics, params, tableau):
     lib = _native.load()
     desc = _native.ProblemDesc()
     owner = ctypes.c_void_p()
     p = np.ascontiguousarray(np.asarray(params, dtype=np.float64).reshape(-1))
-    _native.check(lib.hgg_structured_descriptor(description.encode(), order, physics,
-                                                ctypes.c_void_p(p.ctypes.data), tableau.encode(), 0,
-                                                ctypes.byref(desc), ctypes.byref(owner)))
+    _native.check(getattr(lib, entry)(source.encode(), order, physics,
+                                      ctypes.c_void_p(p.ctypes.data), tableau.encode(), 0,
+                                      ctypes.byref(desc), ctypes.byref(owner)))
     try:
         d, nB, nQ, nQf = desc.dim, desc.n_basis, desc.n_quad, desc.n_face_quad
         E, F, S = desc.n_elements, desc.n_faces, desc.n_stages

@@ -43,6 +43,15 @@ class Handle:
                                                 ctypes.byref(h)))
         return cls(h)
 
+    @classmethod
+    def mesh_file(cls, path, order, physics, params, tableau="RK4_4", precision=_native.PRECISION_FP64):
+        lib = _native.load()
+        h = ctypes.c_void_p()
+        p = np.ascontiguousarray(np.asarray(params, dtype=np.float64).reshape(-1))
+        _native.check(lib.hgg_create_mesh_file(str(path).encode(), int(order), int(physics), _ptr(p),
+                                               tableau.encode(), int(precision), ctypes.byref(h)))
+        return cls(h)
+
     def close(self):
         if self._raw is not None and self._raw.value:
             self._lib.hgg_destroy(self._raw)
@@ -200,6 +209,19 @@ class HpgemAPISimplified:
         self.n_elements = self.handle.vector_length // (self.numberOfVariables * self.n_basis)
         return self
 
+    def readMeshFile(self, path):
+        """readMesh(fileName): creates the device problem from a Preprocessor "mesh 2" file."""
+        from .descriptor import mesh_file_descriptor
+        D = mesh_file_descriptor(str(path), self.polynomialOrder, self._physics_code, self.params, self.tableau)
+        self.handle = Handle.mesh_file(path, self.polynomialOrder, self._physics_code, self.params,
+                                       self.tableau, self.precision)
+        self._description = None
+        self._mesh_file = str(path)
+        self._mass = None
+        self.n_basis = D["n_basis"]
+        self.n_elements = D["n_elements"]
+        return self
+
     def quadraturePoints(self):
         return self.handle.quadrature_points(self.n_elements, self.dim)
 
@@ -277,9 +299,13 @@ class HpgemAPISimplified:
         mesh: sqrt(sum_e |J_e| d_e^T Mhat d_e), exact on affine elements (the element
         rule of order 2p+1 integrates the degree-2p mass integrand exactly)."""
         if getattr(self, "_mass", None) is None:
-            from .descriptor import structured_descriptor
-            D = structured_descriptor(self._description, self.polynomialOrder, self._physics_code,
-                                      self.params, self.tableau)
+            from .descriptor import mesh_file_descriptor, structured_descriptor
+            if self._description is not None:
+                D = structured_descriptor(self._description, self.polynomialOrder, self._physics_code,
+                                          self.params, self.tableau)
+            else:
+                D = mesh_file_descriptor(self._mesh_file, self.polynomialOrder, self._physics_code,
+                                         self.params, self.tableau)
             phi = D["basis_values"]
             self._mass = np.einsum("q,qi,qj->ij", D["quad_weights"], phi, phi)
             self._absdet = np.abs(np.linalg.det(D["jacobians"]))

@@ -249,6 +249,19 @@ int hgg_structured_descriptor(const char *description, int32_t order, int32_t ph
                               hgg_problem_desc *out, void **owner);
 void hgg_free_descriptor(void *owner);
 
+/* readMesh(fileName) (kernel/Base/MeshManipulator_Impl.h:1505-) for a
+ * Preprocessor "mesh 2" file (applications/Preprocessor/lib/hpgem.cpp writes
+ * it; version 1 files are rejected), then the same set-up as hgg_create_structured: the mesh goes from the
+ * file straight to the descriptor's arrays (no per-element objects).  Element
+ * shapes must be uniform and every face must have two elements (periodic
+ * meshes); the element order and vertex order are the file's. */
+int hgg_create_mesh_file(const char *path, int32_t order, int32_t physics, const double *params,
+                         const char *tableau, int32_t precision, hgg_handle **out);
+
+/* The same descriptor, host only (like hgg_structured_descriptor). */
+int hgg_mesh_file_descriptor(const char *path, int32_t order, int32_t physics, const double *params,
+                             const char *tableau, int32_t precision, hgg_problem_desc *out, void **owner);
+
 /* Element quadrature points in physical coordinates, [n_elements][n_quad][dim]
  * (PhysicalElement::getPointPhysical at each point of the element rule). */
 int hgg_quadrature_points(const hgg_handle *h, double *xyz);

@@ -21,6 +21,10 @@ need nothing but this repository.  What it extracts, and from where:
   reference shape, as an if/else chain on the basis-function index.
 * ``advection_goldens.json``: the L2-error tables of
   ``tests/self/Basic/090Advection_SelfTest.cpp:303-337``.
+* ``mesh_files/*.hpgem``: three of those Preprocessor outputs as they are
+  (the fully periodic 1D line, 2D triangle and 3D cube meshes), for the tests
+  of the library's "mesh 2" reader; their structured descriptions are in
+  ``meshes.json``.
 """
 import json
 import math
@@ -107,6 +111,10 @@ MESHES = [
     ("3Dtriangular1", "3Dtriangular1mesh.hpgem", "3Dtriangular1source.hpgem"),
     ("3Dtriangular2", "3Dtriangular2mesh.hpgem", "3Dtriangular2source.hpgem"),
 ]
+
+
+# Preprocessor outputs kept as files for the mesh reader's tests (fully periodic)
+MESH_FILES = ["unitLineN4Per.hpgem", "unitSquareTrianglesN4Per.hpgem", "unitCubeN4Per.hpgem"]
 
 
 def extract_meshes(ref):
@@ -258,6 +266,12 @@ def main():
         with open(os.path.join(HERE, name), "w") as f:
             json.dump(blob, f, separators=(",", ":"))
         print(name, os.path.getsize(os.path.join(HERE, name)), "bytes")
+    os.makedirs(os.path.join(HERE, "mesh_files"), exist_ok=True)
+    for fname in MESH_FILES:
+        dst = os.path.join(HERE, "mesh_files", fname)
+        with open(os.path.join(ref, "tests", "files", fname)) as fi, open(dst, "w") as fo:
+            fo.write(fi.read())
+        print(os.path.join("mesh_files", fname), os.path.getsize(dst), "bytes")
 
 
 if __name__ == "__main__":
