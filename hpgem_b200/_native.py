@@ -23,6 +23,8 @@ EXPORTED = ["hgg_create", "hgg_destroy", "hgg_last_error", "hgg_set_state", "hgg
             "hgg_kernel_kind", "hgg_set_store_last_stage", "hgg_set_stream", "hgg_set_kernel_variant", "hgg_launch_count",
             "hgg_create_structured", "hgg_structured_descriptor", "hgg_free_descriptor",
             "hgg_create_mesh_file", "hgg_mesh_file_descriptor",
+            "hgg_create_linear", "hgg_linear_descriptor", "hgg_free_linear_descriptor",
+            "hgg_create_linear_structured",
             "hgg_quadrature_points", "hgg_num_quadrature_points",
             "hgg_project", "hgg_num_error_points", "hgg_error_points", "hgg_l2_error", "hgg_max_error",
             "hgg_time_derivative_static", "hgg_step_adaptive", "hgg_set_error_estimate",
@@ -54,6 +56,17 @@ class ProblemDesc(ctypes.Structure):
         ("n_faces", ctypes.c_int64), ("face_elements", ctypes.c_void_p),
         ("face_local", ctypes.c_void_p), ("face_tab_index", ctypes.c_void_p),
         ("face_normals", ctypes.c_void_p),
+        ("n_stages", ctypes.c_int32), ("rk_a", ctypes.c_void_p), ("rk_b", ctypes.c_void_p),
+        ("rk_c", ctypes.c_void_p),
+    ]
+
+
+class LinearDesc(ctypes.Structure):
+    """Mirror of struct hgg_linear_desc."""
+    _fields_ = [
+        ("n_rows", ctypes.c_int32), ("precision", ctypes.c_int32), ("n_elements", ctypes.c_int64),
+        ("mass", ctypes.c_void_p), ("element_stiffness", ctypes.c_void_p),
+        ("n_faces", ctypes.c_int64), ("face_elements", ctypes.c_void_p), ("face_stiffness", ctypes.c_void_p),
         ("n_stages", ctypes.c_int32), ("rk_a", ctypes.c_void_p), ("rk_b", ctypes.c_void_p),
         ("rk_c", ctypes.c_void_p),
     ]
@@ -136,6 +149,13 @@ def load():
         "hgg_mesh_file_descriptor": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int32, ctypes.c_int32, P,
                                                     ctypes.c_char_p, ctypes.c_int32,
                                                     ctypes.POINTER(ProblemDesc), ctypes.POINTER(H)]),
+        "hgg_create_linear": (ctypes.c_int, [ctypes.POINTER(LinearDesc), ctypes.POINTER(H)]),
+        "hgg_linear_descriptor": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int32, ctypes.c_int32, P,
+                                                 ctypes.c_char_p, ctypes.c_int32,
+                                                 ctypes.POINTER(LinearDesc), ctypes.POINTER(H)]),
+        "hgg_free_linear_descriptor": (None, [H]),
+        "hgg_create_linear_structured": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int32, ctypes.c_int32, P,
+                                                        ctypes.c_char_p, ctypes.c_int32, ctypes.POINTER(H)]),
         "hgg_quadrature_points": (ctypes.c_int, [H, P]),
         "hgg_num_quadrature_points": (ctypes.c_int32, [H]),
         "hgg_project": (ctypes.c_int, [H, P, ctypes.c_int32]),

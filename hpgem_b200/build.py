@@ -16,11 +16,13 @@ LIB_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIB_DIR, "libhpgem_b200.so")
 SOURCES = [os.path.join(CSRC, "capi.cu"),
            os.path.join(CSRC, "host", "setup.cpp"),
-           os.path.join(CSRC, "host", "operators.cpp")]
+           os.path.join(CSRC, "host", "operators.cpp"),
+           os.path.join(CSRC, "host", "linear.cpp")]
 DEPS = SOURCES + sorted(glob.glob(os.path.join(CSRC, "*.cuh"))) + [
                   os.path.join(CSRC, "host", "refshapes.h"),
                   os.path.join(CSRC, "host", "setup.h"),
                   os.path.join(CSRC, "host", "operators.h"),
+                  os.path.join(CSRC, "host", "linear.h"),
                   os.path.join(CSRC, "host", "simplex_rules.inc"),
                   os.path.join(os.path.dirname(HERE), "include", "hpgem_b200.h")]
 

@@ -642,6 +642,7 @@ int hgg_batch_add(hgg_batch *b, hgg_handle *h, double dt, int32_t nsteps, int32_
         if (free_slot < 0 && !b->handles[i]) free_slot = i;
     }
     if (free_slot < 0) return bfail(b, HGG_ERR_INVALID, "batch is full");
+    if (h->linear) return bfail(b, HGG_ERR_UNSUPPORTED, "stored-matrix handles are stepped on their own");
     if (!h->slice_ok && !h->op.tensor && dense_R(h) > 256)
         return bfail(b, HGG_ERR_UNSUPPORTED, "dense kernel: more than 256 coefficients per element");
     // the handle's own work must be finished before the batch uses its buffers

@@ -17,8 +17,10 @@
 
 #include "../../include/hpgem_b200.h"
 #include "dg_kernels.cuh"
+#include "linear_stage.cuh"
 #include "tensor_pipe.cuh"
 #include "tensor_slice.cuh"
+#include "host/linear.h"
 #include "host/operators.h"
 #include "host/setup.h"
 
@@ -76,6 +78,12 @@ struct hgg_handle {
     // slice kernel (hexahedra, p = 3): per-element records of SliceShape::GR doubles
     bool slice_ok = false;
     double *d_slice_geo = nullptr;
+    // stored-matrix form (HpgemAPILinear): distinct folded matrices, transposed
+    bool linear = false;
+    int lin_R = 0, lin_slots = 0, lin_mats = 0;
+    double *d_lin_table = nullptr;
+    float *d_lin_table_f = nullptr;  // FP32-mixed form with FP32 contractions (R <= kMixedFp32MaxBasis)
+    int32_t *d_lin_self = nullptr, *d_lin_nbr = nullptr, *d_lin_mat = nullptr;
     int num_sms = 148;
     int *d_status = nullptr;
     bool store_last = true;
@@ -361,10 +369,32 @@ int launch_dense_any(hgg_handle *h, const StageIOT<KT> &io) {
     return fail(h, HGG_ERR_UNSUPPORTED, "shape");
 }
 
+template <typename KT>
+int launch_linear(hgg_handle *h, const StageIOT<KT> &io) {
+    const int R = h->lin_R;
+    const int epb = std::max(1, 256 / R);
+    LinearGeom g{h->d_lin_table, h->d_lin_table_f, h->d_lin_self, h->d_lin_nbr, h->d_lin_mat,
+                 R, h->lin_slots, epb, h->lin_mats};
+    const unsigned blocks = (unsigned)((h->op.nE + epb - 1) / epb);
+    const int threads = linear_threads(R, epb);
+    auto go = [&](auto ct) {
+        using CT = decltype(ct);
+        const size_t smem = linear_smem(R, h->lin_slots, epb, sizeof(CT));
+        if (smem > 48 * 1024)
+            cudaFuncSetAttribute(linear_stage<KT, CT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        linear_stage<KT, CT><<<blocks, threads, smem, h->stream>>>(io, g);
+    };
+    if (std::is_same_v<KT, float> && h->d_lin_table_f) go(float{});
+    else go(double{});
+    return 0;
+}
+
 int launch_stage(hgg_handle *h, const StageIO &io) {
     const HostOperators &op = h->op;
     int rc;
-    if (h->slice_ok) {
+    if (h->linear) {
+        rc = launch_linear<double>(h, io);
+    } else if (h->slice_ok) {
         rc = launch_slice<double>(h, io);
     } else if (op.tensor) {
         rc = op.dim == 2 ? launch_tensor_dim<2>(h, io)
@@ -383,7 +413,8 @@ int launch_stage(hgg_handle *h, const StageIO &io) {
 // FP32-mixed form: the stage kernels that have it
 int launch_stage(hgg_handle *h, const StageIOT<float> &io) {
     int rc;
-    if (h->slice_ok) rc = launch_slice(h, io);
+    if (h->linear) rc = launch_linear<float>(h, io);
+    else if (h->slice_ok) rc = launch_slice(h, io);
     else if (h->op.tensor)
         rc = h->op.dim == 2 ? launch_tensor_oneshot_f<2>(h, io)
                             : (h->op.dim == 3 ? launch_tensor_oneshot_f<3>(h, io)
@@ -459,37 +490,29 @@ int check_status(hgg_handle *h) {
     int st = 0;
     HGG_CUDA(h, cudaMemcpyAsync(&st, h->d_status, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
     HGG_CUDA(h, cudaStreamSynchronize(h->stream));
-    if (st) return fail(h, HGG_ERR_DEVICE, "kernel status word " + std::to_string(st) + " (bad neighbour index)");
+    if (st)
+        return fail(h, HGG_ERR_DEVICE,
+                    "kernel status word " + std::to_string(st) + " (bit 0: bad neighbour index, bit 1: bad matrix index)");
     return 0;
 }
 
-int create_from_desc(const hgg_problem_desc *desc, hgg_handle *h) {
-    try {
-        h->op = build_operators(*desc);
-    } catch (const std::exception &ex) {
-        return fail(h, HGG_ERR_INVALID, ex.what());
-    }
-    if (desc->n_stages < 1 || desc->n_stages > kMaxStages || !desc->rk_a || !desc->rk_b)
+// Butcher tableau and precision shared by both descriptors
+int set_tableau(hgg_handle *h, int32_t n_stages, const double *a, const double *b, const double *c,
+                int32_t precision) {
+    if (n_stages < 1 || n_stages > kMaxStages || !a || !b)
         return fail(h, HGG_ERR_INVALID, "Butcher tableau must have 1..8 stages");
-    h->S = desc->n_stages;
-    h->rk_a.assign(desc->rk_a, desc->rk_a + h->S * h->S);
-    h->rk_b.assign(desc->rk_b, desc->rk_b + h->S);
-    h->rk_c = desc->rk_c ? std::vector<double>(desc->rk_c, desc->rk_c + h->S) : std::vector<double>(h->S, 0.0);
-    if (desc->precision != HGG_PRECISION_FP64 && desc->precision != HGG_PRECISION_FP32)
+    h->S = n_stages;
+    h->rk_a.assign(a, a + h->S * h->S);
+    h->rk_b.assign(b, b + h->S);
+    h->rk_c = c ? std::vector<double>(c, c + h->S) : std::vector<double>(h->S, 0.0);
+    if (precision != HGG_PRECISION_FP64 && precision != HGG_PRECISION_FP32)
         return fail(h, HGG_ERR_INVALID, "precision must be HGG_PRECISION_FP64 or HGG_PRECISION_FP32");
-    h->mixed = desc->precision == HGG_PRECISION_FP32;
-    const HostOperators &op = h->op;
-    h->N = op.nE * op.V * op.nB;
-    h->tile_elems = op.tensor ? pipe_tile_elems(op.order, op.dim) : 1;
-    h->tensor_layout = op.tensor;
-    h->slice_ok = op.tensor && op.dim == 3 && op.order == 3 && op.trace_pos[0] == 0 && op.trace_pos[1] == 1;
-    h->tiled = h->slice_ok;
-    if (h->slice_ok) h->tile_elems = SliceShape::TE;
-    if (h->mixed && !mixed_supported(h))
-        return fail(h, HGG_ERR_UNSUPPORTED, "the FP32-mixed form has no kernel for this shape and order");
-    const int64_t n_pad = (op.nE + h->tile_elems - 1) / h->tile_elems * h->tile_elems;
-    h->N_alloc = n_pad * op.V * op.nB;
+    h->mixed = precision == HGG_PRECISION_FP32;
+    return 0;
+}
 
+// device, stream, solution and stage vectors (N_alloc doubles each), status word
+int init_device_vectors(hgg_handle *h) {
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
         return fail(h, HGG_ERR_NOT_LOADED, "no CUDA device available");
@@ -508,6 +531,32 @@ int create_from_desc(const hgg_problem_desc *desc, hgg_handle *h) {
         HGG_CUDA(h, cudaMemsetAsync(h->k[i], 0, (h->mixed ? sizeof(float) : sizeof(double)) * h->N_alloc, h->stream));
     if ((rc = alloc(h, sizeof(int), (void **)&h->d_status))) return rc;
     HGG_CUDA(h, cudaMemsetAsync(h->d_status, 0, sizeof(int), h->stream));
+    return 0;
+}
+
+// linear: the handle will run the stored-matrix kernel (attach_linear), so the
+// vectors stay in hpGEM order and the matrix-free operators are not uploaded
+int create_from_desc(const hgg_problem_desc *desc, hgg_handle *h, bool linear = false) {
+    try {
+        h->op = build_operators(*desc);
+    } catch (const std::exception &ex) {
+        return fail(h, HGG_ERR_INVALID, ex.what());
+    }
+    if (linear) h->op.tensor = false;
+    int rc = set_tableau(h, desc->n_stages, desc->rk_a, desc->rk_b, desc->rk_c, desc->precision);
+    if (rc) return rc;
+    const HostOperators &op = h->op;
+    h->N = op.nE * op.V * op.nB;
+    h->tile_elems = op.tensor ? pipe_tile_elems(op.order, op.dim) : 1;
+    h->tensor_layout = op.tensor;
+    h->slice_ok = op.tensor && op.dim == 3 && op.order == 3 && op.trace_pos[0] == 0 && op.trace_pos[1] == 1;
+    h->tiled = h->slice_ok;
+    if (h->slice_ok) h->tile_elems = SliceShape::TE;
+    if (h->mixed && !mixed_supported(h))
+        return fail(h, HGG_ERR_UNSUPPORTED, "the FP32-mixed form has no kernel for this shape and order");
+    const int64_t n_pad = (op.nE + h->tile_elems - 1) / h->tile_elems * h->tile_elems;
+    h->N_alloc = n_pad * op.V * op.nB;
+    if ((rc = init_device_vectors(h))) return rc;
     if (op.tensor) {
         if ((rc = upload(h, op.elem_geo, &h->d_ahat)) || (rc = upload(h, op.t_nbr, &h->d_tnbr)) ||
             (rc = upload(h, op.t_mode, &h->d_tmode)) || (rc = upload(h, op.t_sigma, &h->d_tsigma)))
@@ -551,6 +600,10 @@ int create_from_desc(const hgg_problem_desc *desc, hgg_handle *h) {
         if ((rc = alloc(h, sizeof(double) * h->N_alloc, (void **)&h->d_scratch))) return rc;
     } else {
         if (h->mixed && (rc = alloc(h, sizeof(double) * h->N_alloc, (void **)&h->d_scratch))) return rc;
+        if (linear) {
+            HGG_CUDA(h, cudaStreamSynchronize(h->stream));
+            return 0;
+        }
         // the dense kernel reads its operators transposed ([..][j][i]): coalesced across rows i
         auto transposed = [&](const std::vector<double> &m) {
             std::vector<double> t(m.size());
@@ -572,6 +625,37 @@ int create_from_desc(const hgg_problem_desc *desc, hgg_handle *h) {
             (rc = upload(h, op.elem_geo, &h->d_elem_geo)) || (rc = upload(h, op.face_geo, &h->d_face_geo)))
             return rc;
     }
+    HGG_CUDA(h, cudaStreamSynchronize(h->stream));
+    return 0;
+}
+
+// Folds the stored matrices (fold_linear) and uploads them: the handle's
+// stages then run the stored-matrix kernel.
+int attach_linear(hgg_handle *h, const LinearSystem &sys) {
+    LinearOperators lo;
+    try {
+        lo = fold_linear(sys);
+    } catch (const std::exception &ex) {
+        return fail(h, HGG_ERR_INVALID, ex.what());
+    }
+    const int R = lo.R;
+    const size_t RR = (size_t)R * R;
+    std::vector<double> t(lo.table.size());
+    for (int m = 0; m < lo.n_mats(); ++m)
+        for (int i = 0; i < R; ++i)
+            for (int j = 0; j < R; ++j) t[m * RR + (size_t)j * R + i] = lo.table[m * RR + (size_t)i * R + j];
+    int rc;
+    if ((rc = upload(h, t, &h->d_lin_table)) || (rc = upload(h, lo.self_mat, &h->d_lin_self))) return rc;
+    if (lo.slots > 0 && ((rc = upload(h, lo.nbr, &h->d_lin_nbr)) || (rc = upload(h, lo.nbr_mat, &h->d_lin_mat))))
+        return rc;
+    if (h->mixed && R <= kMixedFp32MaxBasis) {
+        std::vector<float> tf(t.begin(), t.end());
+        if ((rc = upload(h, tf, &h->d_lin_table_f))) return rc;
+    }
+    h->lin_R = R;
+    h->lin_slots = lo.slots;
+    h->lin_mats = lo.n_mats();
+    h->linear = true;
     HGG_CUDA(h, cudaStreamSynchronize(h->stream));
     return 0;
 }
@@ -730,7 +814,7 @@ int hgg_synchronize(hgg_handle *h) {
 
 int64_t hgg_vector_length(const hgg_handle *h) { return h ? h->N : -1; }
 
-int hgg_kernel_kind(const hgg_handle *h) { return h ? (h->op.tensor ? 1 : 0) : -1; }
+int hgg_kernel_kind(const hgg_handle *h) { return h ? (h->linear ? 2 : (h->op.tensor ? 1 : 0)) : -1; }
 
 int hgg_set_store_last_stage(hgg_handle *h, int32_t enable) {
     if (!h) return fail(h, HGG_ERR_INVALID, "null handle");
@@ -1122,6 +1206,137 @@ int hgg_create_structured(const char *description, int32_t order, int32_t physic
     hgg_handle *h = nullptr;
     int rc = hgg_create(&d, &h);
     if (rc) return rc;
+    h->sp = std::move(sp);
+    butcher_error_estimate(tableau, h->rk_err, h->rk_order);
+    *out = h;
+    return 0;
+}
+
+}  // extern "C"
+
+namespace {
+// HpgemAPILinear's matrices of a structured mesh (host), with the problem they came from
+int linear_structured_system(const char *description, int32_t order, int32_t physics, const double *params,
+                             const char *tableau, StructuredProblem &P, LinearSystem &sys) {
+    if (physics != HGG_PHYSICS_ADVECTION && physics != HGG_PHYSICS_WAVE)
+        return fail(nullptr, HGG_ERR_UNSUPPORTED,
+                    "the stored-matrix form has the reference's linear advection and central-flux wave");
+    try {
+        P = build_structured(description, order, physics, params, tableau);
+        hgg_problem_desc d;
+        fill_descriptor(P, HGG_PRECISION_FP64, d);
+        sys = assemble_linear(d);
+    } catch (const std::exception &ex) {
+        return fail(nullptr, HGG_ERR_INVALID, ex.what());
+    }
+    return 0;
+}
+
+// arrays behind an hgg_linear_desc from hgg_linear_descriptor
+struct LinearDescOwner {
+    std::vector<double> mass, stiffness, faces, rk_a, rk_b, rk_c;
+    std::vector<int64_t> face_elements;
+};
+}  // namespace
+
+extern "C" {
+
+int hgg_create_linear(const hgg_linear_desc *desc, hgg_handle **out) {
+    if (!desc || !out) return fail(nullptr, HGG_ERR_INVALID, "null argument");
+    *out = nullptr;
+    LinearSystem sys;
+    try {
+        sys = linear_from_desc(*desc);
+    } catch (const std::exception &ex) {
+        return fail(nullptr, HGG_ERR_INVALID, ex.what());
+    }
+    hgg_handle *h = new (std::nothrow) hgg_handle();
+    if (!h) return fail(nullptr, HGG_ERR_NOMEM, "host allocation failed");
+    auto bail = [&](int rc) {
+        g_create_error = h->err;
+        destroy_handle(h);
+        return rc;
+    };
+    int rc = set_tableau(h, desc->n_stages, desc->rk_a, desc->rk_b, desc->rk_c, desc->precision);
+    if (rc) return bail(rc);
+    // one "variable" of R coefficients per element: the layout is hpGEM's either way
+    h->op.nE = desc->n_elements;
+    h->op.V = 1;
+    h->op.nB = desc->n_rows;
+    h->N = h->N_alloc = desc->n_elements * desc->n_rows;
+    if ((rc = init_device_vectors(h))) return bail(rc);
+    if (h->mixed && (rc = alloc(h, sizeof(double) * h->N_alloc, (void **)&h->d_scratch))) return bail(rc);
+    if ((rc = attach_linear(h, sys))) return bail(rc);
+    *out = h;
+    return 0;
+}
+
+int hgg_linear_descriptor(const char *description, int32_t order, int32_t physics, const double *params,
+                          const char *tableau, int32_t precision, hgg_linear_desc *out, void **owner) {
+    if (!description || !tableau || !out || !owner) return fail(nullptr, HGG_ERR_INVALID, "null argument");
+    *owner = nullptr;
+    StructuredProblem P;
+    LinearSystem sys;
+    int rc = linear_structured_system(description, order, physics, params, tableau, P, sys);
+    if (rc) return rc;
+    std::unique_ptr<LinearDescOwner> o(new (std::nothrow) LinearDescOwner());
+    if (!o) return fail(nullptr, HGG_ERR_NOMEM, "host allocation failed");
+    const size_t RR = (size_t)sys.R * sys.R;
+    try {
+        o->mass.resize(sys.E * RR);
+        o->stiffness.resize(sys.E * RR);
+        o->faces.assign(sys.F * 4 * RR, 0.0);
+    } catch (const std::bad_alloc &) {
+        return fail(nullptr, HGG_ERR_NOMEM, "host allocation failed");
+    }
+    for (int64_t e = 0; e < sys.E; ++e) {
+        std::memcpy(&o->mass[e * RR], sys.pool.get(sys.mass_id[e]), RR * sizeof(double));
+        std::memcpy(&o->stiffness[e * RR], sys.pool.get(sys.stiffness_id[e]), RR * sizeof(double));
+    }
+    for (int64_t f = 0; f < sys.F; ++f)
+        for (int b = 0; b < 4; ++b)
+            if (sys.face_id[4 * f + b] >= 0)
+                std::memcpy(&o->faces[(4 * f + b) * RR], sys.pool.get(sys.face_id[4 * f + b]), RR * sizeof(double));
+    o->face_elements = sys.face_elements;
+    o->rk_a = P.rk_a;
+    o->rk_b = P.rk_b;
+    o->rk_c = P.rk_c;
+    *out = hgg_linear_desc{};
+    out->n_rows = sys.R;
+    out->precision = precision;
+    out->n_elements = sys.E;
+    out->mass = o->mass.data();
+    out->element_stiffness = o->stiffness.data();
+    out->n_faces = sys.F;
+    out->face_elements = o->face_elements.data();
+    out->face_stiffness = o->faces.data();
+    out->n_stages = P.n_stages;
+    out->rk_a = o->rk_a.data();
+    out->rk_b = o->rk_b.data();
+    out->rk_c = o->rk_c.data();
+    *owner = o.release();
+    return 0;
+}
+
+void hgg_free_linear_descriptor(void *owner) { delete static_cast<LinearDescOwner *>(owner); }
+
+int hgg_create_linear_structured(const char *description, int32_t order, int32_t physics, const double *params,
+                                 const char *tableau, int32_t precision, hgg_handle **out) {
+    if (!description || !out || !tableau) return fail(nullptr, HGG_ERR_INVALID, "null argument");
+    *out = nullptr;
+    std::unique_ptr<StructuredProblem> sp(new StructuredProblem());
+    LinearSystem sys;
+    int rc = linear_structured_system(description, order, physics, params, tableau, *sp, sys);
+    if (rc) return rc;
+    hgg_problem_desc d;
+    fill_descriptor(*sp, precision, d);
+    hgg_handle *h = new (std::nothrow) hgg_handle();
+    if (!h) return fail(nullptr, HGG_ERR_NOMEM, "host allocation failed");
+    if ((rc = create_from_desc(&d, h, true)) || (rc = attach_linear(h, sys))) {
+        g_create_error = h->err;
+        destroy_handle(h);
+        return rc;
+    }
     h->sp = std::move(sp);
     butcher_error_estimate(tableau, h->rk_err, h->rk_order);
     *out = h;

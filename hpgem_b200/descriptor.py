@@ -55,3 +55,29 @@ def _descriptor(entry, source, order, physics, params, tableau):
     finally:
         lib.hgg_free_descriptor(owner)
     return out
+
+
+def linear_descriptor(description, order, physics, params, tableau="RK4_4"):
+    """The stored matrices hgg_linear_descriptor assembles (HpgemAPILinear's
+    createMassMatrices / createStiffnessMatrices for the reference's linear
+    advection and wave applications) as numpy arrays."""
+    lib = _native.load()
+    desc = _native.LinearDesc()
+    owner = ctypes.c_void_p()
+    p = np.ascontiguousarray(np.asarray(params, dtype=np.float64).reshape(-1))
+    _native.check(lib.hgg_linear_descriptor(description.encode(), order, physics,
+                                            ctypes.c_void_p(p.ctypes.data), tableau.encode(), 0,
+                                            ctypes.byref(desc), ctypes.byref(owner)))
+    try:
+        R, E, F, S = desc.n_rows, desc.n_elements, desc.n_faces, desc.n_stages
+        out = dict(
+            n_rows=R, n_elements=E, n_faces=F,
+            mass=_arr(desc.mass, (E, R, R), np.float64),
+            element_stiffness=_arr(desc.element_stiffness, (E, R, R), np.float64),
+            face_elements=_arr(desc.face_elements, (F, 2), np.int64),
+            face_stiffness=_arr(desc.face_stiffness, (F, 4, R, R), np.float64),
+            rk_a=_arr(desc.rk_a, (S, S), np.float64), rk_b=_arr(desc.rk_b, (S,), np.float64),
+            rk_c=_arr(desc.rk_c, (S,), np.float64))
+    finally:
+        lib.hgg_free_linear_descriptor(owner)
+    return out

@@ -52,6 +52,42 @@ class Handle:
                                                tableau.encode(), int(precision), ctypes.byref(h)))
         return cls(h)
 
+    @classmethod
+    def linear_structured(cls, description, order, physics, params, tableau="RK4_4",
+                          precision=_native.PRECISION_FP64):
+        """HpgemAPILinear on a structured mesh: the stored matrices of the reference's
+        linear advection / central-flux wave applications (hgg_create_linear_structured)."""
+        lib = _native.load()
+        h = ctypes.c_void_p()
+        p = np.ascontiguousarray(np.asarray(params, dtype=np.float64).reshape(-1))
+        _native.check(lib.hgg_create_linear_structured(description.encode(), int(order), int(physics),
+                                                       _ptr(p), tableau.encode(), int(precision),
+                                                       ctypes.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def linear(cls, mass, element_stiffness, face_elements, face_stiffness, rk_a, rk_b, rk_c=None,
+               precision=_native.PRECISION_FP64):
+        """HpgemAPILinear from the matrices hpGEM stored (hgg_create_linear): mass and
+        element stiffness [E][R][R], face_elements [F][2] (right -1 on a boundary face),
+        face_stiffness [F][4][R][R] (LL, LR, RL, RR blocks), Butcher tableau arrays."""
+        lib = _native.load()
+        mass = np.ascontiguousarray(mass, dtype=np.float64)
+        E, R = mass.shape[0], mass.shape[1]
+        K = np.ascontiguousarray(element_stiffness, dtype=np.float64).reshape(E, R, R)
+        fe = np.ascontiguousarray(face_elements, dtype=np.int64).reshape(-1, 2)
+        fs = np.ascontiguousarray(face_stiffness, dtype=np.float64).reshape(len(fe), 4, R, R)
+        a = np.ascontiguousarray(rk_a, dtype=np.float64)
+        b = np.ascontiguousarray(rk_b, dtype=np.float64)
+        c = np.ascontiguousarray(rk_c if rk_c is not None else np.zeros(len(b)), dtype=np.float64)
+        d = _native.LinearDesc(n_rows=R, precision=int(precision), n_elements=E, mass=mass.ctypes.data,
+                               element_stiffness=K.ctypes.data, n_faces=len(fe), face_elements=fe.ctypes.data,
+                               face_stiffness=fs.ctypes.data, n_stages=len(b), rk_a=a.ctypes.data,
+                               rk_b=b.ctypes.data, rk_c=c.ctypes.data)
+        h = ctypes.c_void_p()
+        _native.check(lib.hgg_create_linear(ctypes.byref(d), ctypes.byref(h)))
+        return cls(h)
+
     def close(self):
         if self._raw is not None and self._raw.value:
             self._lib.hgg_destroy(self._raw)
@@ -72,7 +108,7 @@ class Handle:
 
     @property
     def kernel_kind(self):
-        return "tensor" if self._lib.hgg_kernel_kind(self._raw) == 1 else "dense"
+        return {1: "tensor", 2: "linear"}.get(self._lib.hgg_kernel_kind(self._raw), "dense")
 
     @property
     def launch_count(self):
@@ -325,6 +361,34 @@ class HpgemAPISimplified:
         x = self.quadraturePoints()
         vals = np.asarray(exact(x.reshape(-1, self.dim), time), dtype=float)
         return self.handle.max_error(vec, vals.reshape(-1, self.numberOfVariables), self.numberOfVariables)
+
+
+class HpgemAPILinear(HpgemAPISimplified):
+    """HpgemAPILinear<DIM> (kernel/Base/HpgemAPILinear.h): the element and face
+    matrices are built once before the time loop (createMassMatrices,
+    createStiffnessMatrices) and every stage multiplies them
+    (multiplyStiffnessMatrices) and solves with the stored mass matrix.
+    ``physics`` "advection" has the integrands of
+    tests/self/Basic/080AdvectionLinear_SelfTest.cpp, "wave" those of
+    applications/ExampleMultipleVariableProblem/AcousticWaveLinear_Impl.h.
+    Everything after readMesh is the inherited time loop."""
+
+    def __init__(self, dim, order, physics="advection", advection=None, c_inv=1.0,
+                 tableau="RK4_4", precision=_native.PRECISION_FP64):
+        if physics not in ("advection", "wave"):
+            raise ValueError("the linear applications are 'advection' and 'wave' (central flux)")
+        super().__init__(dim, order, physics, advection=advection, c_inv=c_inv, tableau=tableau,
+                         precision=precision)
+
+    def readMesh(self, description):
+        """readMesh + tasksBeforeSolving (HpgemAPILinear_Impl.h:107-129, :500-506)."""
+        self.handle = Handle.linear_structured(description, self.polynomialOrder, self._physics_code,
+                                               self.params, self.tableau, self.precision)
+        self._description = description
+        self._mass = None
+        self.n_basis = _basis_count(self.dim, description, self.polynomialOrder)
+        self.n_elements = self.handle.vector_length // (self.numberOfVariables * self.n_basis)
+        return self
 
 
 def _basis_count(dim, description, p):

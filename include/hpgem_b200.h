@@ -163,7 +163,8 @@ int hgg_synchronize(hgg_handle *h);
 int64_t hgg_vector_length(const hgg_handle *h);
 
 /* 1 when the sum-factorised tensor-product kernel drives this handle,
- * 0 when the dense reference-operator kernel does. */
+ * 0 when the dense reference-operator kernel does, 2 for the stored-matrix
+ * kernel of a handle from hgg_create_linear*. */
 int hgg_kernel_kind(const hgg_handle *h);
 
 /* When enabled (default), the last stage derivative k_S is stored like the
@@ -251,8 +252,9 @@ void hgg_free_descriptor(void *owner);
 
 /* readMesh(fileName) (kernel/Base/MeshManipulator_Impl.h:1505-) for a
  * Preprocessor "mesh 2" file (applications/Preprocessor/lib/hpgem.cpp writes
- * it; version 1 files are rejected), then the same set-up as hgg_create_structured: the mesh goes from the
- * file straight to the descriptor's arrays (no per-element objects).  Element
+ * it; version 1 files are rejected), then the same set-up as
+ * hgg_create_structured: the mesh goes from the file straight to the
+ * descriptor's arrays (no per-element objects).  Element
  * shapes must be uniform and every face must have two elements (periodic
  * meshes); the element order and vertex order are the file's. */
 int hgg_create_mesh_file(const char *path, int32_t order, int32_t physics, const double *params,
@@ -285,6 +287,61 @@ int hgg_l2_error(hgg_handle *h, int32_t vec, const double *exact, double *error)
  * exact[n_elements][n_quad][n_vars]; max_error receives n_vars values.  Both
  * norms are evaluated on the device; only the exact values cross to it. */
 int hgg_max_error(hgg_handle *h, int32_t vec, const double *exact, double *max_error);
+
+/* ---- HpgemAPILinear: stored element and face matrices ---------------------
+ * HpgemAPILinear<DIM> (kernel/Base/HpgemAPILinear_Impl.h) builds, before its
+ * time loop, per element a mass matrix (createMassMatrices, :131-139) and a
+ * stiffness matrix, and per face the four blocks of a face stiffness matrix
+ * (createStiffnessMatrices, :250-288).  Every stage it multiplies them with
+ * the stage input (multiplyStiffnessMatrices, :291-434) and solves with the
+ * stored mass matrix (solveMassMatrixEquations, :143-156).  The library takes
+ * those matrices as hpGEM built them, so any linear application's integrands
+ * run unchanged; on the device each element's stage is
+ *   k_e = D_e w_e + sum_s N_{e,s} w_{n(e,s)},
+ *   D_e = M_e^{-1} (K_e + its own-side face blocks),
+ *   N_{e,s} = M_e^{-1} (the block coupling to neighbour n(e,s)),
+ * with every distinct matrix stored once (structured meshes repeat a few).
+ * Rows and columns use hpGEM's element index iV * n_basis + iB. */
+typedef struct hgg_linear_desc {
+    int32_t n_rows;                   /* R: coefficients per element (n_vars * n_basis) */
+    int32_t precision;                /* enum hgg_precision */
+    int64_t n_elements;
+    const double *mass;               /* [n_elements][R][R], row-major */
+    const double *element_stiffness;  /* [n_elements][R][R] */
+    int64_t n_faces;
+    const int64_t *face_elements;     /* [n_faces][2]: left, right element; right = -1 on a boundary face */
+    const double *face_stiffness;     /* [n_faces][4][R][R]: FaceMatrix::getElementMatrix(iSide, jSide)
+                                         for (LEFT,LEFT), (LEFT,RIGHT), (RIGHT,LEFT), (RIGHT,RIGHT);
+                                         on a boundary face only (LEFT,LEFT) is read */
+    int32_t n_stages;                 /* Butcher tableau, as in hgg_problem_desc */
+    const double *rk_a;
+    const double *rk_b;
+    const double *rk_c;
+} hgg_linear_desc;
+
+/* HpgemAPILinear::readMesh + tasksBeforeSolving: a handle whose stages apply
+ * the stored matrices.  Every time-loop entry point (hgg_set_state,
+ * hgg_step, hgg_time_derivative, hgg_step_adaptive after
+ * hgg_set_error_estimate, hgg_get_state, ...) works on it unchanged; at most
+ * 256 rows per element. */
+int hgg_create_linear(const hgg_linear_desc *desc, hgg_handle **out);
+
+/* The matrices of the reference's two linear applications on a structured
+ * mesh: physics HGG_PHYSICS_ADVECTION assembles the integrands of
+ * tests/self/Basic/080AdvectionLinear_SelfTest.cpp:108-168 (weak form, upwind
+ * flux), HGG_PHYSICS_WAVE those of applications/ExampleMultipleVariableProblem/
+ * AcousticWaveLinear_Impl.h:98-284 (strong form, central flux).  Host only:
+ * fills *out with arrays owned by *owner (hgg_free_linear_descriptor). */
+int hgg_linear_descriptor(const char *description, int32_t order, int32_t physics, const double *params,
+                          const char *tableau, int32_t precision, hgg_linear_desc *out, void **owner);
+void hgg_free_linear_descriptor(void *owner);
+
+/* The same matrices, assembled without the per-element arrays (identical
+ * matrices kept once) and handed to the device; the handle also has the
+ * structured mesh's projection, quadrature points and error norms. */
+int hgg_create_linear_structured(const char *description, int32_t order, int32_t physics,
+                                 const double *params, const char *tableau, int32_t precision,
+                                 hgg_handle **out);
 
 /* ---- many problems at once ------------------------------------------------
  * No counterpart in the reference (hpGEM advances one mesh per process).  A

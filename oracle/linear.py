@@ -1,0 +1,128 @@
+"""Oracle for HpgemAPILinear's stored-matrix time stepping (test infrastructure only).
+
+Restates kernel/Base/HpgemAPILinear_Impl.h:
+* createMassMatrices (:131-139) and createStiffnessMatrices (:250-288): per
+  element a mass and a stiffness matrix, per face the four blocks
+  (LEFT,LEFT), (LEFT,RIGHT), (RIGHT,LEFT), (RIGHT,RIGHT) of the face matrix;
+  ``assemble`` builds them in numpy from an oracle ``Problem`` with the
+  integrands of the reference's two linear applications:
+  - advection, tests/self/Basic/080AdvectionLinear_SelfTest.cpp:108-168
+    (element: phi_i (a . grad phi_j) in row j, column i; face: the upwind
+    side's trial functions, -(a . n_j) phi_j phi_i with n_j the unit normal
+    out of the test function's side, halved for flow parallel to the face,
+    integrated with the face weight times |n|);
+  - wave, applications/ExampleMultipleVariableProblem/AcousticWaveLinear_Impl.h:
+    98-284 (mass c_inv on the s variables; element grad_d phi_j phi_i in the
+    (p, s_d) and (s_d, p) blocks; face -0.5 n_d phi_j phi_i with the scaled
+    normal out of the basis function's side, no |n| factor);
+* multiplyStiffnessMatrices (:360-434) + solveMassMatrixEquations (:143-156):
+  ``time_derivative`` multiplies the element matrix, then adds both sides of
+  every face in face order, then solves with the element's mass matrix;
+* the Runge-Kutta loop of HpgemAPISimplified::computeOneTimeStep
+  (HpgemAPISimplified_Impl.h:788-820), which HpgemAPILinear inherits.
+"""
+import numpy as np
+
+from .dg import ADVECTION, TABLEAUX, WAVE
+
+
+def assemble(prob):
+    """(mass [E][R][R], stiffness [E][R][R], face_elements [F][2], faces [F][4][R][R])."""
+    if prob.physics not in (ADVECTION, WAVE):
+        raise ValueError("the reference's linear applications are advection and the central-flux wave")
+    d, nB, E = prob.dim, prob.nB, prob.mesh.n_elements
+    wave = prob.physics == WAVE
+    V = d + 1 if wave else 1
+    R = V * nB
+    w = np.asarray(prob.rule.weights, dtype=float)
+    phi = prob.phi                                   # [nQ][nB]
+    Jinv = np.linalg.inv(prob.J)                     # [E][d][d]
+    grad = np.einsum("ecr,qbc->eqbr", Jinv, prob.dphi)  # J^{-T} grad_ref: [E][nQ][nB][d]
+    wq = w[None, :] * prob.absdet[:, None]           # [E][nQ]
+    mass1 = np.einsum("eq,qi,qj->eij", wq, phi, phi)
+    mass = np.zeros((E, R, R))
+    K = np.zeros((E, R, R))
+    a = prob.a[:d]
+    if not wave:
+        mass[:] = mass1
+        ag = np.einsum("eqjr,r->eqj", grad, a)
+        K[:] = np.einsum("eq,qi,eqj->eji", wq, phi, ag)
+    else:
+        for v in range(V):
+            mass[:, v * nB:(v + 1) * nB, v * nB:(v + 1) * nB] = mass1 * (prob.cinv if v > 0 else 1.0)
+        for c in range(d):
+            blk = np.einsum("eq,eqj,qi->eij", wq, grad[..., c], phi)  # [E][test i][basis j]
+            K[:, 0:nB, (c + 1) * nB:(c + 2) * nB] = blk
+            K[:, (c + 1) * nB:(c + 2) * nB, 0:nB] = blk
+    table = prob.faces_c
+    F = len(table)
+    faces = np.zeros((F, 4, R, R))
+    wf = np.asarray(prob.face_rule.weights, dtype=float)
+    for f in range(F):
+        L, Rt, fL, combo = (int(x) for x in table[f])
+        ph = (prob.phiF[fL], prob.phiR[combo])      # [nQf][nB] per side
+        n = prob.normals[f]
+        area = float(np.sqrt(np.dot(n, n)))
+        for ts in range(2):
+            for tr in range(2):
+                pp = np.einsum("q,qa,qb->ab", wf, ph[ts], ph[tr])  # [test function][trial function]
+                blk = faces[f, 2 * ts + tr]
+                if not wave:
+                    A = float(np.dot(a, n / area))
+                    if A > 1e-12:
+                        factor = 1.0 if tr == 0 else 0.0
+                    elif A < -1e-12:
+                        factor = 1.0 if tr == 1 else 0.0
+                    else:
+                        factor = 0.5
+                    an = A if ts == 0 else -A
+                    blk[:] = -an * area * factor * pp
+                else:
+                    sgn = -1.0 if tr == 1 else 1.0
+                    for c in range(d):
+                        t = -0.5 * sgn * n[c] * pp
+                        blk[0:nB, (c + 1) * nB:(c + 2) * nB] = t
+                        blk[(c + 1) * nB:(c + 2) * nB, 0:nB] = t
+    return mass, K, table[:, :2].astype(np.int64), faces
+
+
+class LinearOracle:
+    """Stored matrices of one mesh; faces with right element -1 are boundary faces
+    (only their (LEFT, LEFT) block is used, HpgemAPILinear_Impl.h:410-430)."""
+
+    def __init__(self, mass, stiffness, face_elements, faces):
+        self.mass = np.asarray(mass, dtype=float)
+        self.K = np.asarray(stiffness, dtype=float)
+        self.fe = np.asarray(face_elements, dtype=np.int64).reshape(-1, 2)
+        self.faces = np.asarray(faces, dtype=float)
+        self.E, self.R = self.mass.shape[0], self.mass.shape[1]
+
+    def time_derivative(self, u):
+        u = np.asarray(u, dtype=float).reshape(self.E, self.R)
+        r = np.einsum("eij,ej->ei", self.K, u)
+        for f, (L, Rt) in enumerate(self.fe):
+            if Rt >= 0:
+                r[L] += self.faces[f, 0] @ u[L] + self.faces[f, 1] @ u[Rt]
+                r[Rt] += self.faces[f, 2] @ u[L] + self.faces[f, 3] @ u[Rt]
+            else:
+                r[L] += self.faces[f, 0] @ u[L]
+        k = np.linalg.solve(self.mass, r[..., None])[..., 0]   # LU with partial pivoting per element
+        return k.reshape(-1)
+
+    def step(self, u, dt, nsteps, tableau="RK4_4"):
+        tab = TABLEAUX[tableau]
+        A, b = np.asarray(tab["A"], dtype=float), np.asarray(tab["b"], dtype=float)
+        S = len(b)
+        u = np.asarray(u, dtype=float).reshape(-1).copy()
+        for _ in range(nsteps):
+            ks = []
+            for i in range(S):
+                w = u.copy()
+                for j in range(i):
+                    if A[i][j] != 0.0:
+                        w += dt * A[i][j] * ks[j]
+                ks.append(self.time_derivative(w))
+            for j in range(S):
+                if b[j] != 0.0:
+                    u += dt * b[j] * ks[j]
+        return u
