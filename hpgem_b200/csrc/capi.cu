@@ -84,6 +84,10 @@ struct hgg_handle {
     double *d_lin_table = nullptr;
     float *d_lin_table_f = nullptr;  // FP32-mixed form with FP32 contractions (R <= kMixedFp32MaxBasis)
     int32_t *d_lin_self = nullptr, *d_lin_nbr = nullptr, *d_lin_mat = nullptr;
+    // grouped DMMA kernel: tiles of elements with identical matrices (0 tiles: not used)
+    double *d_lin_table_rm = nullptr;
+    int32_t *d_lin_tile_elems = nullptr, *d_lin_tile_mats = nullptr;
+    int64_t lin_tiles = 0;
     int num_sms = 148;
     int *d_status = nullptr;
     bool store_last = true;
@@ -373,8 +377,13 @@ template <typename KT>
 int launch_linear(hgg_handle *h, const StageIOT<KT> &io) {
     const int R = h->lin_R;
     const int epb = std::max(1, 256 / R);
-    LinearGeom g{h->d_lin_table, h->d_lin_table_f, h->d_lin_self, h->d_lin_nbr, h->d_lin_mat,
+    LinearGeom g{h->d_lin_table, h->d_lin_table_rm, h->d_lin_table_f, h->d_lin_self, h->d_lin_nbr, h->d_lin_mat,
                  R, h->lin_slots, epb, h->lin_mats};
+    if (h->lin_tiles > 0) {
+        LinearTiles t{h->d_lin_tile_elems, h->d_lin_tile_mats};
+        linear_tile_stage<KT><<<(unsigned)h->lin_tiles, 256, 0, h->stream>>>(io, g, t);
+        return 0;
+    }
     const unsigned blocks = (unsigned)((h->op.nE + epb - 1) / epb);
     const int threads = linear_threads(R, epb);
     auto go = [&](auto ct) {
@@ -651,6 +660,48 @@ int attach_linear(hgg_handle *h, const LinearSystem &sys) {
     if (h->mixed && R <= kMixedFp32MaxBasis) {
         std::vector<float> tf(t.begin(), t.end());
         if ((rc = upload(h, tf, &h->d_lin_table_f))) return rc;
+    }
+    // Tiles of the grouped kernel: elements ordered by their matrix tuple (self,
+    // slot 1, ..., slot S), cut into tiles of kLinTileN within each group.  Used
+    // when the tiles are at least half full on average (few distinct tuples, as
+    // on structured meshes) and an element has at least kLinTileMinRows rows
+    // (below that the padding of the 8-row fragments and the per-chunk
+    // synchronisation cost more than the row kernel: measured on quadrilaterals
+    // at p = 2, 9 rows, 0.82 ms per RK4 step against 0.46 ms on 512^2 cells).
+    {
+        const int S = lo.slots, W = S + 1;
+        auto tuple = [&](int64_t e, int k) { return k == 0 ? lo.self_mat[e] : lo.nbr_mat[(size_t)e * S + k - 1]; };
+        std::vector<int64_t> order(lo.E);
+        for (int64_t e = 0; e < lo.E; ++e) order[e] = e;
+        std::stable_sort(order.begin(), order.end(), [&](int64_t x, int64_t y) {
+            for (int k = 0; k < W; ++k)
+                if (tuple(x, k) != tuple(y, k)) return tuple(x, k) < tuple(y, k);
+            return false;
+        });
+        std::vector<int32_t> tel, tmat;
+        int fill = kLinTileN;
+        for (size_t i = 0; i < order.size(); ++i) {
+            const int64_t e = order[i];
+            const bool same = i > 0 && [&] {
+                for (int k = 0; k < W; ++k)
+                    if (tuple(e, k) != tuple(order[i - 1], k)) return false;
+                return true;
+            }();
+            if (!same || fill == kLinTileN) {
+                tel.insert(tel.end(), kLinTileN, -1);
+                for (int k = 0; k < W; ++k) tmat.push_back(tuple(e, k));
+                fill = 0;
+            }
+            tel[tel.size() - kLinTileN + fill++] = (int32_t)e;
+        }
+        const int64_t n_tiles = (int64_t)(tel.size() / kLinTileN);
+        if (n_tiles * kLinTileN <= 2 * lo.E && R >= kLinTileMinRows) {
+            std::vector<double> rm(lo.table);
+            if ((rc = upload(h, rm, &h->d_lin_table_rm)) || (rc = upload(h, tel, &h->d_lin_tile_elems)) ||
+                (rc = upload(h, tmat, &h->d_lin_tile_mats)))
+                return rc;
+            h->lin_tiles = n_tiles;
+        }
     }
     h->lin_R = R;
     h->lin_slots = lo.slots;

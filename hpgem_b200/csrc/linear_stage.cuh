@@ -17,6 +17,7 @@ namespace hgg {
 
 struct LinearGeom {
     const double *table;      // [n_mats][R][R] transposed: table[m][j][i] = (matrix m)_{ij}
+    const double *table_rm;   // [n_mats][R][R] row-major (the grouped kernel's copy), or null
     const float *table_f;     // the same in FP32 (FP32-mixed form with FP32 contractions), else null
     const int32_t *self_mat;  // [E]
     const int32_t *nbr;       // [E][slots], -1: unused slot
@@ -98,6 +99,118 @@ __global__ void __launch_bounds__(256) linear_stage(const StageIOT<KT> io, const
         for (int j = 0; j < R; ++j) acc += op[(size_t)j * R] * wn[j];
     }
     stage_output(io, e * R + r, u_own, (double)acc);
+}
+
+// ---------------------------------------------------------------------------
+// grouped form: tiles of kLinTileN elements that share all their matrices
+// ---------------------------------------------------------------------------
+// On a structured mesh the elements fall into a few groups with identical
+// matrices (one group on a hexahedral mesh, ten on the five-tetrahedron split),
+// so a tile's stage is a dense product Out[R][64] = sum_s A_s[R][R] W_s[R][64]
+// with W_s the stage inputs of the tile's elements (s = 0) or of their
+// neighbours in slot s.  It runs on the FP64 tensor cores (DMMA, m8n8k4):
+// 8 warps, warp w owns elements 8w..8w+7, each warp all row bands of 8.
+constexpr int kLinTileN = 64;            // elements per tile
+constexpr int kLinKC = 32;               // k (column) chunk staged in shared memory
+constexpr int kLinRows = 64;             // output rows per pass
+constexpr int kLinStride = kLinKC + 4;   // padded row stride (doubles): fragment loads conflict-free
+constexpr int kLinOutStride = kLinRows + 1;
+constexpr int kLinTileMinRows = 24;      // smaller elements run the row kernel
+
+struct LinearTiles {
+    const int32_t *elems;  // [n_tiles][kLinTileN] element ids, -1: padding
+    const int32_t *mats;   // [n_tiles][1 + slots] the tile's matrices (-1: unused slot)
+};
+
+__device__ __forceinline__ void dmma_m8n8k4(double &d0, double &d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+template <typename KT>
+__global__ void __launch_bounds__(256) linear_tile_stage(const StageIOT<KT> io, const LinearGeom g,
+                                                          const LinearTiles t) {
+    // A chunk [kLinRows][kLinStride] and B chunk [kLinTileN][kLinStride]; the
+    // output tile [kLinTileN][kLinOutStride] reuses the same memory
+    __shared__ __align__(16) double sm[(kLinRows + kLinTileN) * kLinStride];
+    __shared__ int32_t tel[kLinTileN], src[kLinTileN];
+    static_assert(kLinTileN * kLinOutStride <= (kLinRows + kLinTileN) * kLinStride, "output staging fits");
+    double *As = sm, *Bs = sm + kLinRows * kLinStride;
+    const int R = g.R, S = g.slots;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, gid = lane >> 2, tig = lane & 3;
+    const int64_t tile = blockIdx.x;
+    if (tid < kLinTileN) tel[tid] = t.elems[tile * kLinTileN + tid];
+    const int passes = (R + kLinRows - 1) / kLinRows;
+    for (int pass = 0; pass < passes; ++pass) {
+        const int r0 = pass * kLinRows;
+        const int rows = min(kLinRows, R - r0);
+        double acc[8][2];
+#pragma unroll
+        for (int b = 0; b < 8; ++b) acc[b][0] = acc[b][1] = 0.0;
+        for (int s = 0; s <= S; ++s) {
+            const int32_t m = t.mats[tile * (S + 1) + s];  // the same for the whole block
+            if (m < 0) continue;
+            if (m >= g.n_mats) {
+                if (tid == 0) atomicOr(io.status, 2);
+                continue;
+            }
+            __syncthreads();  // tel written; src, As, Bs free
+            if (tid < kLinTileN) {
+                const int32_t e = tel[tid];
+                int32_t se = -1;
+                if (e >= 0 && e < io.n_elements) se = s == 0 ? e : g.nbr[(int64_t)e * S + (s - 1)];
+                if (se >= io.n_elements || se < -1) {
+                    atomicOr(io.status, 1);
+                    se = -1;
+                }
+                src[tid] = se;
+            }
+            const double *A = g.table_rm + (size_t)m * R * R;
+            for (int kc = 0; kc < R; kc += kLinKC) {
+                __syncthreads();  // src written; the previous chunk's fragments read
+                for (int i = tid; i < kLinRows * kLinKC; i += blockDim.x) {
+                    const int r = i / kLinKC, k = i % kLinKC;
+                    double v = 0.0;
+                    if (r < rows && kc + k < R) v = A[(size_t)(r0 + r) * R + kc + k];
+                    As[r * kLinStride + k] = v;
+                }
+                for (int i = tid; i < kLinTileN * kLinKC; i += blockDim.x) {
+                    const int n = i / kLinKC, k = i % kLinKC;
+                    const int32_t se = src[n];
+                    double v = 0.0;
+                    if (se >= 0 && kc + k < R) v = stage_input(io, (int64_t)se * R + kc + k);
+                    Bs[n * kLinStride + k] = v;
+                }
+                __syncthreads();
+                const int kmax = min(kLinKC, R - kc);
+                for (int k4 = 0; k4 < kmax; k4 += 4) {
+                    const double b = Bs[(warp * 8 + gid) * kLinStride + k4 + tig];
+#pragma unroll
+                    for (int band = 0; band < 8; ++band)
+                        if (band * 8 < rows) dmma_m8n8k4(acc[band][0], acc[band][1],
+                                                         As[(band * 8 + gid) * kLinStride + k4 + tig], b);
+                }
+            }
+        }
+        __syncthreads();  // fragments read: stage the outputs as [element][row]
+        double *Os = sm;
+#pragma unroll
+        for (int band = 0; band < 8; ++band)
+            if (band * 8 < rows) {
+                const int n = warp * 8 + tig * 2;
+                Os[n * kLinOutStride + band * 8 + gid] = acc[band][0];
+                Os[(n + 1) * kLinOutStride + band * 8 + gid] = acc[band][1];
+            }
+        __syncthreads();
+        for (int i = tid; i < kLinTileN * kLinRows; i += blockDim.x) {
+            const int n = i / kLinRows, r = i % kLinRows;
+            const int32_t e = tel[n];
+            if (e < 0 || e >= io.n_elements || r >= rows) continue;
+            const int64_t idx = (int64_t)e * R + r0 + r;
+            stage_output(io, idx, io.u[idx], Os[n * kLinOutStride + r]);
+        }
+    }
 }
 
 }  // namespace hgg

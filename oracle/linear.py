@@ -17,7 +17,7 @@ Restates kernel/Base/HpgemAPILinear_Impl.h:
     normal out of the basis function's side, no |n| factor);
 * multiplyStiffnessMatrices (:360-434) + solveMassMatrixEquations (:143-156):
   ``time_derivative`` multiplies the element matrix, then adds both sides of
-  every face in face order, then solves with the element's mass matrix;
+  every face, then solves with the element's mass matrix;
 * the Runge-Kutta loop of HpgemAPISimplified::computeOneTimeStep
   (HpgemAPISimplified_Impl.h:788-820), which HpgemAPILinear inherits.
 """
@@ -100,12 +100,17 @@ class LinearOracle:
     def time_derivative(self, u):
         u = np.asarray(u, dtype=float).reshape(self.E, self.R)
         r = np.einsum("eij,ej->ei", self.K, u)
-        for f, (L, Rt) in enumerate(self.fe):
-            if Rt >= 0:
-                r[L] += self.faces[f, 0] @ u[L] + self.faces[f, 1] @ u[Rt]
-                r[Rt] += self.faces[f, 2] @ u[L] + self.faces[f, 3] @ u[Rt]
-            else:
-                r[L] += self.faces[f, 0] @ u[L]
+        # both sides of every face (the reference adds them face by face; the sums
+        # here differ from that order by rounding only)
+        L, Rt = self.fe[:, 0], self.fe[:, 1]
+        inner = Rt >= 0
+        uR = u[np.where(inner, Rt, 0)]
+        left = np.einsum("fij,fj->fi", self.faces[:, 0], u[L])
+        left[inner] += np.einsum("fij,fj->fi", self.faces[inner, 1], uR[inner])
+        np.add.at(r, L, left)
+        right = (np.einsum("fij,fj->fi", self.faces[inner, 2], u[L[inner]]) +
+                 np.einsum("fij,fj->fi", self.faces[inner, 3], uR[inner]))
+        np.add.at(r, Rt[inner], right)
         k = np.linalg.solve(self.mass, r[..., None])[..., 0]   # LU with partial pivoting per element
         return k.reshape(-1)
 

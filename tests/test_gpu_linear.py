@@ -49,6 +49,12 @@ CASES = [
     ("triangles p2 wave", [4, 4], True, 2, "wave", [1.0], 2e-3, 20),
     ("tetrahedra p2 wave", [2, 2, 2], True, 2, "wave", [1.3], 1e-3, 10),
     ("hexahedra p3 wave", [2, 2, 2], False, 3, "wave", [1.0], 1e-3, 5),
+    # large enough for the grouped tensor-core kernel (64-element tiles of equal matrices):
+    # one 64-row pass, several groups, four passes (256 rows), two passes (75 rows)
+    ("hexahedra p3 advection tiles", [8, 8, 8], False, 3, "advection", [1.0, 0.7, 0.3], 1e-3, 4),
+    ("tetrahedra p2 wave tiles", [4, 4, 4], True, 2, "wave", [1.3], 1e-3, 4),
+    ("hexahedra p3 wave tiles", [4, 4, 4], False, 3, "wave", [1.0], 1e-3, 2),
+    ("quads p4 wave tiles", [8, 8], False, 4, "wave", [0.7], 1e-3, 4),
 ]
 
 
