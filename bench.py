@@ -484,7 +484,8 @@ def run_tet_wave(args, stream):
     out["fp32_mixed"]["max_rel_coef_diff_vs_fp64"] = float(np.abs(u32 - u64).max() / np.abs(u64).max())
     res = {"workload": "3D acoustic wave, 32^3 x 5 periodic tetrahedra, p = 2, upwind flux, RK4, "
                        "dt = 5e-4, seeded 3-mode pressure, 23 steps", "dtype": "f64",
-           "kernel": "dense_stage<KT,3,4,1,10> (wave rows)"}
+           "kernel": "dense_group_stage<double,3,4,10> (FP64: 32-element tiles of equal operators, "
+                     "lane = element); dense_stage<float,3,4,1,10> (FP32-mixed: one thread per element row)"}
     res.update(out["fp64"])
     res["forms"] = {"fp32_mixed": out["fp32_mixed"]}
     res["central_flux_fp64"] = out["fp64_central"]
@@ -522,9 +523,10 @@ def run_linear(args, stream):
 
     import hpgem_b200
 
-    d = hpgem_b200.structured_description([64, 64, 64], [0, 0, 0], [1, 1, 1])
+    nc = args.linear_cells
+    d = hpgem_b200.structured_description([nc, nc, nc], [0, 0, 0], [1, 1, 1])
     a = [1.0, 0.7, 0.3]
-    warm, steps = 3, 20
+    warm, steps = (args.warmup, args.steps) if args.only else (3, 20)
     out, sols = {}, {}
     for name, prec in (("fp64", 0), ("fp32_mixed", 1)):
         t0 = time.time()
@@ -559,8 +561,8 @@ def run_linear(args, stream):
     flop = 2.0 * rows * (1 + slots) * 4  # per DoF-update: 1 + 6 matrices of 64 x 64, 4 stages
     peak = measured_fp64_gemm_tflops()
     achieved = out["fp64"]["value"] * flop / 1e12
-    res = {"workload": "HpgemAPILinear advection, 64^3 periodic hexahedra, p = 3, RK4, dt = 2e-4, "
-                       "Gaussian bump, %d timed steps after %d" % (steps, warm),
+    res = {"workload": "HpgemAPILinear advection, %d^3 periodic hexahedra, p = 3, RK4, dt = 2e-4, "
+                       "Gaussian bump, %d timed steps after %d" % (nc, steps, warm),
            "dtype": "f64", "kernel": "linear_tile_stage (FP64 DMMA m8n8k4, 64-element tiles)"}
     res.update(out["fp64"])
     res["l2_distance_to_matrix_free"] = s64.l2Distance(u64, u_free)
@@ -640,7 +642,18 @@ def main():
     ap.add_argument("--served-requests", type=int, default=500,
                     help="requests of the seeded stream to serve (the stream has 2000; the first 500 "
                          "keep the default run within a few minutes)")
+    ap.add_argument("--only", choices=["linear", "tet_wave"],
+                    help="run one secondary leg alone (profiling): --steps / --warmup set its timed loop")
+    ap.add_argument("--linear-cells", type=int, default=64,
+                    help="cells per direction of the stored-matrix leg's hexahedral mesh")
     args = ap.parse_args()
+    if args.only:
+        import torch
+
+        stream = torch.cuda.Stream()
+        leg = run_linear(args, stream) if args.only == "linear" else run_tet_wave(args, stream)
+        print(json.dumps(leg), flush=True)
+        return
     if args.impl == "reference":
         if int(os.environ.get("RANK", "0")) != 0:
             return

@@ -548,6 +548,261 @@ __global__ void __launch_bounds__(256) dense_stage(const StageIOT<KT> io, const 
     dense_any_body<KT, DIM, NFL, WAVE, NB>(io, g, blockIdx.x);
 }
 
+// ---------------------------------------------------------------------------
+// grouped dense kernels: lane = element, warp = basis row
+// ---------------------------------------------------------------------------
+// The elements of a structured mesh fall into a few groups with the same
+// operator signature (the pair operators of every face; for the wave, whose
+// per-element work is the largest).  A
+// tile holds kGroupTile elements of one group; a block of kGroupTile * rows
+// threads runs it with lane = element and warp = output row, so every operator
+// entry a warp reads is the same address for all its lanes (one broadcast
+// instead of one sector per element), and the per-element staging arrays have
+// odd strides (in elements of CT), so the lanes' reads hit distinct banks.  The
+// stage inputs are staged and the outputs written through shared memory, both
+// coalesced along an element's coefficients.
+constexpr int kGroupTile = 32;
+
+// odd stride (in CT elements) at least n
+__host__ __device__ constexpr int odd_stride(int n) { return n | 1; }
+
+// Per-tile set-up: the tile's element ids, its
+// operator signature (the same for all its elements: taken from the first) and
+// every element's geometry record, staged coalesced; lanes then read their
+// element's record from shared memory (odd stride) instead of 32 scattered
+// global addresses per load.
+template <int NFL>
+struct GroupTileInfo {
+    int32_t tel[kGroupTile];
+    int32_t self_pair[NFL], nbr_pair[NFL];
+    int8_t mode[NFL];
+};
+
+template <int NFL>
+__device__ __forceinline__ void group_tile_setup(const DenseGeom &g, const int32_t *tiles, int64_t tile,
+                                                 int64_t n_elements, GroupTileInfo<NFL> &ti) {
+    const int tid = threadIdx.x;
+    if (tid < kGroupTile) ti.tel[tid] = tiles[tile * kGroupTile + tid];
+    if (tid < NFL) {
+        const int32_t e0 = tiles[tile * kGroupTile];  // the first slot of a tile is never padding
+        const bool ok = e0 >= 0 && e0 < n_elements;
+        ti.self_pair[tid] = ok ? g.self_pair[(int64_t)e0 * NFL + tid] : 0;
+        ti.nbr_pair[tid] = ok ? g.nbr_pair[(int64_t)e0 * NFL + tid] : 0;
+        ti.mode[tid] = ok ? g.mode[(int64_t)e0 * NFL + tid] : 0;
+    }
+    __syncthreads();
+}
+
+// geometry record of tile element l: elem_geo (EG values) then face_geo (FG values)
+template <typename CT, int EG, int FG>
+__device__ __forceinline__ void group_stage_geometry(const DenseGeom &g, const int32_t *tel, int64_t n_elements,
+                                                     double *GE, int GS) {
+    for (int k = threadIdx.x; k < kGroupTile * (EG + FG); k += blockDim.x) {
+        const int l = k / (EG + FG), q = k % (EG + FG);
+        const int32_t e = tel[l];
+        double v = 0.0;
+        if (e >= 0 && e < n_elements) v = q < EG ? g.elem_geo[(int64_t)e * EG + q] : g.face_geo[(int64_t)e * FG + q - EG];
+        GE[l * GS + q] = v;
+    }
+}
+
+// The tile's operators in shared memory, transposed as in global memory
+// ([..][j][i]): the DIM volume operators, then per face the self-pair and the
+// neighbour-pair operator of the tile's signature (faces whose upwind mode
+// does not use one get zeros there; they are not read).
+template <typename CT, int DIM, int NFL, int NB>
+__device__ __forceinline__ void group_stage_operators(const DenseGeom &g, const int32_t *self_pair,
+                                                      const int32_t *nbr_pair, CT *OP) {
+    const CT *gvol = dense_vol<CT>(g), *gpairs = dense_pairs<CT>(g);
+    constexpr int NN = NB * NB, TOT = (DIM + 2 * NFL) * NN;
+    for (int k = threadIdx.x; k < TOT; k += blockDim.x) {
+        const int m = k / NN, q = k % NN;
+        CT v;
+        if (m < DIM) v = gvol[(size_t)m * NN + q];
+        else {
+            const int f = (m - DIM) >> 1;
+            const int32_t pair = ((m - DIM) & 1) ? nbr_pair[f] : self_pair[f];
+            v = gpairs[(size_t)pair * NN + q];
+        }
+        OP[k] = v;
+    }
+}
+
+// Acoustic wave in 2D and 3D (the arithmetic of wave_stage_body).  Shared:
+// W [tile][R] stage inputs (then the outputs), WN [tile][NFL][2 NB] neighbour
+// pressure and n . s_n per face, X [tile][DIM + NFL][NB] t_c and n . s, GE
+// [tile][DIM^2 + NFL DIM] geometry (FP64).
+template <int DIM, int NFL, int NB>
+struct WaveGroupShape {
+    static constexpr int V = DIM + 1, R = V * NB, EG = DIM * DIM, FG = NFL * DIM;
+    static constexpr int WS = odd_stride(R), WNS = odd_stride(NFL * 2 * NB), XS = odd_stride((DIM + NFL) * NB);
+    static constexpr int GS = odd_stride(EG + FG);
+    static constexpr int OPS = (DIM + 2 * NFL) * NB * NB;
+    static constexpr int ELEMS = kGroupTile * (WS + WNS + XS) + OPS;  // CT elements after GE (doubles)
+    static constexpr int GEO = kGroupTile * GS;
+};
+
+template <typename KT, int DIM, int NFL, int NB>
+__device__ __forceinline__ void wave_group_body(const StageIOT<KT> &io, const DenseGeom &g, const int32_t *tiles,
+                                                int64_t tile) {
+    using CT = DenseCT<KT, NB>;
+    using SH = WaveGroupShape<DIM, NFL, NB>;
+    constexpr int R = SH::R, WS = SH::WS, WNS = SH::WNS, XS = SH::XS, GS = SH::GS, EG = SH::EG, TE = kGroupTile;
+    extern __shared__ __align__(16) unsigned char dense_shared[];
+    double *GE = reinterpret_cast<double *>(dense_shared);
+    CT *W = reinterpret_cast<CT *>(GE + SH::GEO);
+    CT *WN = W + TE * WS;
+    CT *X = WN + TE * WNS;
+    CT *OP = X + TE * XS;  // [DIM + 2 NFL][NB][NB]
+    __shared__ GroupTileInfo<NFL> ti;
+    const int tid = threadIdx.x, el = tid & (TE - 1), i = tid / TE;
+    group_tile_setup<NFL>(g, tiles, tile, io.n_elements, ti);
+    group_stage_geometry<CT, EG, NFL * DIM>(g, ti.tel, io.n_elements, GE, GS);
+    group_stage_operators<CT, DIM, NFL, NB>(g, ti.self_pair, ti.nbr_pair, OP);
+    for (int k = tid; k < TE * R; k += blockDim.x) {
+        const int l = k / R, rr = k % R;
+        const int32_t ee = ti.tel[l];
+        double v = 0.0;
+        if (ee >= 0 && ee < io.n_elements) v = stage_input(io, (int64_t)ee * R + rr);
+        W[l * WS + rr] = (CT)v;
+    }
+    __syncthreads();  // GE staged (the neighbour loop reads the normals)
+    // neighbours: pressure and n . s (this element's normal) per face and basis row
+    for (int k = tid; k < TE * NFL * NB; k += blockDim.x) {
+        const int l = k / (NFL * NB), f = (k / NB) % NFL, j = k % NB;
+        const int32_t ee = ti.tel[l];
+        double pn = 0.0, jn = 0.0;
+        if (ee >= 0 && ee < io.n_elements) {
+            const int32_t n = g.nbr[(int64_t)ee * NFL + f];
+            if (n >= 0 && n < io.n_elements) {
+                const double *nu = GE + l * GS + EG + f * DIM;
+                pn = stage_input(io, (int64_t)n * R + j);
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) jn += nu[d] * (double)(CT)stage_input(io, (int64_t)n * R + (d + 1) * NB + j);
+            } else {
+                atomicOr(io.status, 1);
+            }
+        }
+        WN[l * WNS + f * 2 * NB + j] = (CT)pn;
+        WN[l * WNS + f * 2 * NB + NB + j] = (CT)jn;
+    }
+    __syncthreads();
+    const int32_t e = ti.tel[el];
+    const bool active = e >= 0 && e < io.n_elements && i < NB;
+    const CT *w = W + el * WS;
+    const CT *wn = WN + el * WNS;
+    const double *G = GE + el * GS;        // G[d][c] = (J^{-T})_{dc}
+    const double *nus = GE + el * GS + EG;  // [NFL][DIM]
+    CT *x = X + el * XS;
+    if (active) {
+#pragma unroll
+        for (int c = 0; c < DIM; ++c) {
+            CT t = CT(0);
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) t += (CT)G[d * DIM + c] * w[(d + 1) * NB + i];
+            x[c * NB + i] = t;
+        }
+#pragma unroll
+        for (int f = 0; f < NFL; ++f) {
+            CT a = CT(0);
+#pragma unroll
+            for (int d = 0; d < DIM; ++d) a += (CT)nus[f * DIM + d] * w[(d + 1) * NB + i];
+            x[(DIM + f) * NB + i] = a;
+        }
+    }
+    __syncthreads();
+    CT P = CT(0), A[DIM], B[NFL], SP[NFL], nrm[NFL];
+    const CT cu = (CT)g.upwind_c;
+    if (active) {
+#pragma unroll
+        for (int c = 0; c < DIM; ++c) {
+            const CT *op = OP + c * NB * NB + i;
+            CT sp = CT(0), sa = CT(0);
+#pragma unroll
+            for (int j = 0; j < NB; ++j) {
+                const CT o = op[j * NB];
+                sp += o * x[c * NB + j];
+                sa += o * w[j];
+            }
+            P += sp;
+            A[c] = sa;
+        }
+#pragma unroll
+        for (int f = 0; f < NFL; ++f) {
+            const CT *ops = OP + (DIM + 2 * f) * NB * NB + i;
+            const CT *opn = OP + (DIM + 2 * f + 1) * NB * NB + i;
+            const CT *js = x + (DIM + f) * NB, *jn = wn + f * 2 * NB + NB, *pn = wn + f * 2 * NB;
+            CT sp = CT(0), sb = CT(0);
+#pragma unroll
+            for (int j = 0; j < NB; ++j) {
+                const CT os = ops[j * NB], on = opn[j * NB];
+                sp += os * js[j] - on * jn[j];
+                sb += os * w[j] - on * pn[j];
+            }
+            P -= sp;
+            B[f] = sb;
+            SP[f] = sp;
+        }
+        if (cu != CT(0)) {
+#pragma unroll
+            for (int f = 0; f < NFL; ++f) {
+                double q = 0.0;
+#pragma unroll
+                for (int d = 0; d < DIM; ++d) q += nus[f * DIM + d] * nus[f * DIM + d];
+                nrm[f] = (CT)sqrt(q);
+                P -= cu * nrm[f] * B[f];
+            }
+        }
+    }
+    __syncthreads();  // W, WN, X read: stage the outputs in W as [element][R]
+    if (active) {
+        W[el * WS + i] = P;
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+            CT acc = CT(0);
+#pragma unroll
+            for (int c = 0; c < DIM; ++c) acc += (CT)G[d * DIM + c] * A[c];
+#pragma unroll
+            for (int f = 0; f < NFL; ++f) acc -= (CT)nus[f * DIM + d] * B[f];
+            acc *= (CT)g.inv_cinv;
+            if (cu != CT(0))
+#pragma unroll
+                for (int f = 0; f < NFL; ++f) acc -= cu * ((CT)nus[f * DIM + d] / nrm[f]) * SP[f];
+            W[el * WS + (d + 1) * NB + i] = acc;
+        }
+    }
+    __syncthreads();
+    for (int k = tid; k < TE * R; k += blockDim.x) {
+        const int l = k / R, rr = k % R;
+        const int32_t ee = ti.tel[l];
+        if (ee < 0 || ee >= io.n_elements) continue;
+        const int64_t idx = (int64_t)ee * R + rr;
+        stage_output(io, idx, io.u[idx], (double)W[l * WS + rr]);
+    }
+}
+
+// rows (warps) of a grouped block; 0: no grouped kernel (the wave in 2D and
+// 3D only).  One warp per basis row; above kGroupMaxRows rows the register
+// budget of the large block (65536 / (32 rows) per thread) makes the compiler
+// spill, and the per-element-row kernel runs instead.
+constexpr int kGroupMaxRows = 24;
+__host__ __device__ inline int group_rows(int dim, int wave, int nb) {
+    if (dim < 2 || !wave) return 0;
+    return nb <= kGroupMaxRows ? nb : 0;
+}
+template <typename CT, int DIM, int NFL, int NB>
+constexpr size_t group_smem() {
+    using SH = WaveGroupShape<DIM, NFL, NB>;
+    return sizeof(double) * SH::GEO + sizeof(CT) * SH::ELEMS;
+}
+
+template <typename KT, int DIM, int NFL, int NB>
+__global__ void __launch_bounds__(kGroupTile *(NB < kGroupMaxRows ? NB : kGroupMaxRows),
+                                  1024 / (kGroupTile * NB) > 0 ? 1024 / (kGroupTile * NB) : 1)
+    dense_group_stage(const StageIOT<KT> io, const DenseGeom g, const int32_t *tiles) {
+    wave_group_body<KT, DIM, NFL, NB>(io, g, tiles, blockIdx.x);
+}
+
 // basis sizes of the shapes the dense kernel serves, orders 1..5
 template <int DIM, int NFL> struct DenseSizes;
 template <> struct DenseSizes<1, 2> { static constexpr int nb[5] = {2, 3, 4, 5, 6}; };

@@ -176,12 +176,13 @@ int hgg_set_store_last_stage(hgg_handle *h, int32_t enable);
  * device; NULL restores the handle's own stream). */
 int hgg_set_stream(hgg_handle *h, void *stream);
 
-/* Selects the kernel organisation of the sum-factorised path: 0 (default)
- * automatic, 1 one block per small group of elements, 2 the pipelined kernel.
- * Both compute the same result; the choice exists for comparison and
- * profiling.  Hexahedra of order 3 keep their vectors in a tiled layout that
- * only their slice kernel reads: any variant but 0 returns
- * HGG_ERR_UNSUPPORTED there.  Ignored by the dense path. */
+/* Selects the kernel organisation: 0 (default) automatic; on the
+ * sum-factorised path 1 is one block per small group of elements and 2 the
+ * pipelined kernel; on the dense path 1 and 2 run one thread per element row
+ * instead of the grouped kernel (tiles of elements with equal operators).  All
+ * compute the same result; the choice exists for comparison and profiling.
+ * Hexahedra of order 3 keep their vectors in a tiled layout that only their
+ * slice kernel reads: any variant but 0 returns HGG_ERR_UNSUPPORTED there. */
 int hgg_set_kernel_variant(hgg_handle *h, int32_t variant);
 
 /* Right-hand side k = M^{-1} R(u) of caller-owned DEVICE vectors u and k, both
