@@ -355,7 +355,7 @@ int launch_dense(hgg_handle *h, const StageIOT<KT> &io) {
     const bool ok = dense_dispatch<DIM, NFL, WAVE>(op.nB, [&](auto nbc) {
         constexpr int NB = decltype(nbc)::value;
         // the grouped kernel where it measured faster: the wave with FP64 contractions
-        // (32^3 x 5 tetrahedra, p = 2, RK4: 1.29 against 2.01 ms per step upwind, 1.18
+        // (32^3 x 5 tetrahedra, p = 2, RK4: 1.12 against 2.01 ms per step upwind, 1.00
         // against 1.71 central); with FP32 contractions, and for advection, the
         // per-row kernel was as fast or faster (0.97 against 1.09 ms; 0.38 both)
         if constexpr (DIM >= 2 && NB <= kGroupMaxRows && WAVE && std::is_same_v<DenseCT<KT, NB>, double>) {
@@ -675,6 +675,19 @@ int create_from_desc(const hgg_problem_desc *desc, hgg_handle *h, bool linear = 
                 tiles[tiles.size() - kGroupTile + fill++] = (int32_t)order[i];
             }
             const int64_t n_tiles = (int64_t)(tiles.size() / kGroupTile);
+            // run the tiles in the order of their first element, not group by group:
+            // the neighbours a tile gathers then belong to tiles of the other groups
+            // that run at about the same time, while they are still in L2
+            std::vector<int64_t> torder(n_tiles);
+            for (int64_t t = 0; t < n_tiles; ++t) torder[t] = t;
+            std::stable_sort(torder.begin(), torder.end(), [&](int64_t x, int64_t y) {
+                return tiles[x * kGroupTile] < tiles[y * kGroupTile];
+            });
+            std::vector<int32_t> sorted(tiles.size());
+            for (int64_t t = 0; t < n_tiles; ++t)
+                std::copy(tiles.begin() + torder[t] * kGroupTile, tiles.begin() + (torder[t] + 1) * kGroupTile,
+                          sorted.begin() + t * kGroupTile);
+            tiles.swap(sorted);
             if (n_tiles * kGroupTile <= 2 * op.nE) {
                 if ((rc = upload(h, tiles, &h->d_group_tiles))) return rc;
                 h->group_tiles = n_tiles;
@@ -747,6 +760,21 @@ int attach_linear(hgg_handle *h, const LinearSystem &sys) {
             tel[tel.size() - kLinTileN + fill++] = (int32_t)e;
         }
         const int64_t n_tiles = (int64_t)(tel.size() / kLinTileN);
+        {
+            // tiles in the order of their first element (see the grouped dense kernel)
+            std::vector<int64_t> torder(n_tiles);
+            for (int64_t t = 0; t < n_tiles; ++t) torder[t] = t;
+            std::stable_sort(torder.begin(), torder.end(),
+                             [&](int64_t x, int64_t y) { return tel[x * kLinTileN] < tel[y * kLinTileN]; });
+            std::vector<int32_t> el2(tel.size()), mat2(tmat.size());
+            for (int64_t t = 0; t < n_tiles; ++t) {
+                std::copy(tel.begin() + torder[t] * kLinTileN, tel.begin() + (torder[t] + 1) * kLinTileN,
+                          el2.begin() + t * kLinTileN);
+                std::copy(tmat.begin() + torder[t] * W, tmat.begin() + (torder[t] + 1) * W, mat2.begin() + t * W);
+            }
+            tel.swap(el2);
+            tmat.swap(mat2);
+        }
         if (n_tiles * kLinTileN <= 2 * lo.E && R >= kLinTileMinRows) {
             std::vector<double> rm(lo.table);
             if ((rc = upload(h, rm, &h->d_lin_table_rm)) || (rc = upload(h, tel, &h->d_lin_tile_elems)) ||
