@@ -91,7 +91,6 @@ struct hgg_handle {
     // grouped dense kernel: tiles of kGroupTile elements with the same operator signature
     int32_t *d_group_tiles = nullptr;
     int64_t group_tiles = 0;
-    bool grouped = true;  // hgg_set_kernel_variant can turn it off
     int num_sms = 148;
     int *d_status = nullptr;
     bool store_last = true;
@@ -358,8 +357,9 @@ int launch_dense(hgg_handle *h, const StageIOT<KT> &io) {
         // (32^3 x 5 tetrahedra, p = 2, RK4: 1.12 against 2.01 ms per step upwind, 1.00
         // against 1.71 central); with FP32 contractions, and for advection, the
         // per-row kernel was as fast or faster (0.97 against 1.09 ms; 0.38 both)
-        if constexpr (DIM >= 2 && NB <= kGroupMaxRows && WAVE && std::is_same_v<DenseCT<KT, NB>, double>) {
-            if (h->group_tiles > 0 && h->grouped) {
+        if constexpr (DIM >= 2 && NB <= kGroupMaxRows && WAVE) {
+            const bool want = h->variant == 2 || (h->variant == 0 && std::is_same_v<DenseCT<KT, NB>, double>);
+            if (h->group_tiles > 0 && want) {
                 constexpr size_t gsmem = group_smem<DenseCT<KT, NB>, DIM, NFL, NB>();
                 if (gsmem > 48 * 1024)
                     cudaFuncSetAttribute(dense_group_stage<KT, DIM, NFL, NB>,
@@ -973,7 +973,6 @@ int hgg_set_kernel_variant(hgg_handle *h, int32_t variant) {
     if (variant != h->variant) {
         release_graphs(h);
         h->variant = variant;
-        h->grouped = variant == 0;
     }
     return 0;
 }

@@ -178,9 +178,11 @@ int hgg_set_stream(hgg_handle *h, void *stream);
 
 /* Selects the kernel organisation: 0 (default) automatic; on the
  * sum-factorised path 1 is one block per small group of elements and 2 the
- * pipelined kernel; on the dense path 1 and 2 run one thread per element row
- * instead of the grouped kernel (tiles of elements with equal operators).  All
- * compute the same result; the choice exists for comparison and profiling.
+ * pipelined kernel; on the dense path 1 runs one thread per element row and 2
+ * the grouped kernel (tiles of elements with equal operators) wherever the
+ * mesh has such tiles, whatever the contraction type (automatic takes it for
+ * the wave with FP64 contractions).  All compute the same result; the choice
+ * exists for comparison and profiling.
  * Hexahedra of order 3 keep their vectors in a tiled layout that only their
  * slice kernel reads: any variant but 0 returns HGG_ERR_UNSUPPORTED there. */
 int hgg_set_kernel_variant(hgg_handle *h, int32_t variant);
