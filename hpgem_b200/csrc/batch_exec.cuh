@@ -49,6 +49,15 @@ struct SliceItem {
     int slot;
 };
 
+template <typename KT>
+struct LinearItem {
+    StageIOT<KT> io[2];
+    LinearGeom g;
+    LinearTiles t;
+    int64_t block0;  // first virtual block (= tile)
+    int slot;
+};
+
 // item whose virtual blocks contain vb (items sorted by block0, block0[0] = 0)
 template <typename Item>
 __device__ __forceinline__ int find_item(const Item *items, int n, int64_t vb) {
@@ -106,6 +115,21 @@ __global__ void __launch_bounds__(SliceShape::THREADS, sizeof(KT) == 4 ? 5 : (NF
     }
 }
 
+template <typename KT>
+__global__ void __launch_bounds__(256)
+    grouped_linear(const LinearItem<KT> *items, const int *n_items, const int64_t *total, const int *parity,
+                   const int *remaining) {
+    const int n = *n_items;
+    const int64_t nb = *total;
+    for (int64_t vb = blockIdx.x; vb < nb; vb += gridDim.x) {
+        const int i = find_item(items, n, vb);
+        const int slot = items[i].slot;
+        __syncthreads();
+        if (remaining[slot] <= 0) continue;
+        linear_tile_body<KT>(items[i].io[parity[slot]], items[i].g, items[i].t, vb - items[i].block0);
+    }
+}
+
 // end of one step of every member: flip the current buffer, count the step
 __global__ void batch_advance(int *parity, int *remaining, int cap) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -119,7 +143,7 @@ __global__ void batch_advance(int *parity, int *remaining, int cap) {
 
 namespace {
 
-enum BatchKind { KIND_DENSE = 0, KIND_TENSOR = 1, KIND_SLICE = 2 };
+enum BatchKind { KIND_DENSE = 0, KIND_TENSOR = 1, KIND_SLICE = 2, KIND_LINEAR = 3 };
 
 struct BatchClass {
     // key
@@ -200,6 +224,7 @@ int bfail(hgg_batch *b, int code, const std::string &msg) {
     } while (0)
 
 int batch_kind(const hgg_handle *h) {
+    if (h->linear) return KIND_LINEAR;
     if (h->slice_ok) return KIND_SLICE;
     if (h->op.tensor) return KIND_TENSOR;
     return KIND_DENSE;
@@ -220,6 +245,7 @@ int tensor_epb(int order, int dim) {
 
 int64_t item_blocks(const BatchClass &c, const hgg_handle *h) {
     const int64_t nE = h->op.nE;
+    if (c.kind == KIND_LINEAR) return h->lin_tiles;
     if (c.kind == KIND_SLICE) return (nE + SliceShape::TE - 1) / SliceShape::TE;
     if (c.kind == KIND_TENSOR) {
         const int epb = tensor_epb(c.order, c.dim);
@@ -231,6 +257,7 @@ int64_t item_blocks(const BatchClass &c, const hgg_handle *h) {
 size_t class_item_bytes(const BatchClass &c) {
     if (c.kind == KIND_DENSE) return c.mixed ? sizeof(DenseItem<float>) : sizeof(DenseItem<double>);
     if (c.kind == KIND_TENSOR) return c.mixed ? sizeof(TensorItem<float>) : sizeof(TensorItem<double>);
+    if (c.kind == KIND_LINEAR) return c.mixed ? sizeof(LinearItem<float>) : sizeof(LinearItem<double>);
     return c.mixed ? sizeof(SliceItem<float>) : sizeof(SliceItem<double>);
 }
 
@@ -255,6 +282,16 @@ void fill_items(const hgg_batch *b, const BatchClass &c, int stage, std::vector<
             for (int par = 0; par < 2; ++par)
                 it.io[par] = make_stage_io<KT>(h, par ? 1 - base : base, b->dt[slot], stage, b->d_status);
             it.g = dense_geom(h, c.epb);
+            it.block0 = block0;
+            it.slot = slot;
+            std::memcpy(dst, &it, sizeof(it));
+        } else if (c.kind == KIND_LINEAR) {
+            LinearItem<KT> it{};
+            for (int par = 0; par < 2; ++par)
+                it.io[par] = make_stage_io<KT>(h, par ? 1 - base : base, b->dt[slot], stage, b->d_status);
+            it.g = LinearGeom{h->d_lin_table, h->d_lin_table_rm, h->d_lin_table_f, h->d_lin_self, h->d_lin_nbr,
+                              h->d_lin_mat, h->lin_R, h->lin_slots, std::max(1, 256 / h->lin_R), h->lin_mats};
+            it.t = LinearTiles{h->d_lin_tile_elems, h->d_lin_tile_mats};
             it.block0 = block0;
             it.slot = slot;
             std::memcpy(dst, &it, sizeof(it));
@@ -361,7 +398,14 @@ void launch_grouped_slice(const hgg_batch *b, const BatchClass &c, int st, unsig
 void launch_class_stage(hgg_batch *b, const BatchClass &c, int st, cudaStream_t s) {
     // a fixed persistent grid: membership changes leave the launch (and the graph) as it is
     const unsigned grid = (unsigned)(c.ctas_per_sm * b->num_sms);
-    if (c.kind == KIND_SLICE) {
+    if (c.kind == KIND_LINEAR) {
+        if (c.mixed)
+            grouped_linear<float><<<grid, 256, 0, s>>>(static_cast<const LinearItem<float> *>(c.d_items[st]), c.d_n,
+                                                       c.d_total, b->d_parity, b->d_remaining);
+        else
+            grouped_linear<double><<<grid, 256, 0, s>>>(static_cast<const LinearItem<double> *>(c.d_items[st]),
+                                                        c.d_n, c.d_total, b->d_parity, b->d_remaining);
+    } else if (c.kind == KIND_SLICE) {
         if (c.mixed) launch_grouped_slice<float>(b, c, st, grid, s);
         else launch_grouped_slice<double>(b, c, st, grid, s);
     } else if (c.kind == KIND_TENSOR) {
@@ -642,7 +686,8 @@ int hgg_batch_add(hgg_batch *b, hgg_handle *h, double dt, int32_t nsteps, int32_
         if (free_slot < 0 && !b->handles[i]) free_slot = i;
     }
     if (free_slot < 0) return bfail(b, HGG_ERR_INVALID, "batch is full");
-    if (h->linear) return bfail(b, HGG_ERR_UNSUPPORTED, "stored-matrix handles are stepped on their own");
+    if (h->linear && h->lin_tiles == 0)
+        return bfail(b, HGG_ERR_UNSUPPORTED, "stored-matrix handles without tiles are stepped on their own");
     if (!h->slice_ok && !h->op.tensor && dense_R(h) > 256)
         return bfail(b, HGG_ERR_UNSUPPORTED, "dense kernel: more than 256 coefficients per element");
     // the handle's own work must be finished before the batch uses its buffers

@@ -88,6 +88,7 @@ struct hgg_handle {
     double *d_lin_table_rm = nullptr;
     int32_t *d_lin_tile_elems = nullptr, *d_lin_tile_mats = nullptr;
     int64_t lin_tiles = 0;
+    int lin_min_rows = kLinTileMinRows;  // fewer rows per element: the row kernel
     // grouped dense kernel: tiles of kGroupTile elements with the same operator signature
     int32_t *d_group_tiles = nullptr;
     int64_t group_tiles = 0;
@@ -562,6 +563,8 @@ int init_device_vectors(hgg_handle *h) {
     return 0;
 }
 
+int attach_linear(hgg_handle *h, const LinearSystem &sys, bool tiles_only = false);
+
 // linear: the handle will run the stored-matrix kernel (attach_linear), so the
 // vectors stay in hpGEM order and the matrix-free operators are not uploaded
 int create_from_desc(const hgg_problem_desc *desc, hgg_handle *h, bool linear = false) {
@@ -631,6 +634,30 @@ int create_from_desc(const hgg_problem_desc *desc, hgg_handle *h, bool linear = 
         if (linear) {
             HGG_CUDA(h, cudaStreamSynchronize(h->stream));
             return 0;
+        }
+        // Folded operator: for advection on triangles of order >= 4 (>= 5 in the
+        // mixed form) the element's whole stage is one small dense operator per
+        // matrix slot (the reference's integrands assembled once, the mass inverse
+        // folded in: the same operator as the matrix-free kernel to rounding), and
+        // the grouped FP64 tensor-core kernel of the stored-matrix path applies it
+        // faster than the per-row dense kernel (256^2 cells, RK4: 0.34 against 0.46
+        // ms per step at p = 4, 0.49 against 0.87 at p = 5; in the mixed form p = 4
+        // measured 0.33 against 0.29 and stays on the dense kernel).  Only when the
+        // mesh forms tiles (structured meshes); otherwise the dense kernel runs.
+        if (op.physics == HGG_PHYSICS_ADVECTION && op.shape == HGG_SHAPE_TRIANGLE &&
+            (op.nB >= 21 || (op.nB >= 15 && !h->mixed))) {
+            LinearSystem sys;
+            bool assembled = true;
+            try {
+                sys = assemble_linear(*desc);
+            } catch (const std::exception &) {
+                assembled = false;
+            }
+            if (assembled) {
+                h->lin_min_rows = 1;
+                if ((rc = attach_linear(h, sys, true))) return rc;
+                if (h->linear) return 0;
+            }
         }
         // the dense kernel reads its operators transposed ([..][j][i]): coalesced across rows i
         auto transposed = [&](const std::vector<double> &m) {
@@ -704,8 +731,9 @@ int create_from_desc(const hgg_problem_desc *desc, hgg_handle *h, bool linear = 
 }
 
 // Folds the stored matrices (fold_linear) and uploads them: the handle's
-// stages then run the stored-matrix kernel.
-int attach_linear(hgg_handle *h, const LinearSystem &sys) {
+// stages then run the stored-matrix kernel.  With tiles_only, nothing is
+// attached (and 0 returned) unless the grouped tensor-core kernel will run.
+int attach_linear(hgg_handle *h, const LinearSystem &sys, bool tiles_only) {
     LinearOperators lo;
     try {
         lo = fold_linear(sys);
@@ -714,18 +742,7 @@ int attach_linear(hgg_handle *h, const LinearSystem &sys) {
     }
     const int R = lo.R;
     const size_t RR = (size_t)R * R;
-    std::vector<double> t(lo.table.size());
-    for (int m = 0; m < lo.n_mats(); ++m)
-        for (int i = 0; i < R; ++i)
-            for (int j = 0; j < R; ++j) t[m * RR + (size_t)j * R + i] = lo.table[m * RR + (size_t)i * R + j];
     int rc;
-    if ((rc = upload(h, t, &h->d_lin_table)) || (rc = upload(h, lo.self_mat, &h->d_lin_self))) return rc;
-    if (lo.slots > 0 && ((rc = upload(h, lo.nbr, &h->d_lin_nbr)) || (rc = upload(h, lo.nbr_mat, &h->d_lin_mat))))
-        return rc;
-    if (h->mixed && R <= kMixedFp32MaxBasis) {
-        std::vector<float> tf(t.begin(), t.end());
-        if ((rc = upload(h, tf, &h->d_lin_table_f))) return rc;
-    }
     // Tiles of the grouped kernel: elements ordered by their matrix tuple (self,
     // slot 1, ..., slot S), cut into tiles of kLinTileN within each group.  Used
     // when the tiles are at least half full on average (few distinct tuples, as
@@ -733,6 +750,8 @@ int attach_linear(hgg_handle *h, const LinearSystem &sys) {
     // (below that the padding of the 8-row fragments and the per-chunk
     // synchronisation cost more than the row kernel: measured on quadrilaterals
     // at p = 2, 9 rows, 0.82 ms per RK4 step against 0.46 ms on 512^2 cells).
+    std::vector<int32_t> tel, tmat;
+    int64_t n_tiles = 0;
     {
         const int S = lo.slots, W = S + 1;
         auto tuple = [&](int64_t e, int k) { return k == 0 ? lo.self_mat[e] : lo.nbr_mat[(size_t)e * S + k - 1]; };
@@ -743,7 +762,6 @@ int attach_linear(hgg_handle *h, const LinearSystem &sys) {
                 if (tuple(x, k) != tuple(y, k)) return tuple(x, k) < tuple(y, k);
             return false;
         });
-        std::vector<int32_t> tel, tmat;
         int fill = kLinTileN;
         for (size_t i = 0; i < order.size(); ++i) {
             const int64_t e = order[i];
@@ -759,29 +777,40 @@ int attach_linear(hgg_handle *h, const LinearSystem &sys) {
             }
             tel[tel.size() - kLinTileN + fill++] = (int32_t)e;
         }
-        const int64_t n_tiles = (int64_t)(tel.size() / kLinTileN);
-        {
-            // tiles in the order of their first element (see the grouped dense kernel)
-            std::vector<int64_t> torder(n_tiles);
-            for (int64_t t = 0; t < n_tiles; ++t) torder[t] = t;
-            std::stable_sort(torder.begin(), torder.end(),
-                             [&](int64_t x, int64_t y) { return tel[x * kLinTileN] < tel[y * kLinTileN]; });
-            std::vector<int32_t> el2(tel.size()), mat2(tmat.size());
-            for (int64_t t = 0; t < n_tiles; ++t) {
-                std::copy(tel.begin() + torder[t] * kLinTileN, tel.begin() + (torder[t] + 1) * kLinTileN,
-                          el2.begin() + t * kLinTileN);
-                std::copy(tmat.begin() + torder[t] * W, tmat.begin() + (torder[t] + 1) * W, mat2.begin() + t * W);
-            }
-            tel.swap(el2);
-            tmat.swap(mat2);
+        n_tiles = (int64_t)(tel.size() / kLinTileN);
+        // tiles in the order of their first element (see the grouped dense kernel)
+        std::vector<int64_t> torder(n_tiles);
+        for (int64_t t2 = 0; t2 < n_tiles; ++t2) torder[t2] = t2;
+        std::stable_sort(torder.begin(), torder.end(),
+                         [&](int64_t x, int64_t y) { return tel[x * kLinTileN] < tel[y * kLinTileN]; });
+        std::vector<int32_t> el2(tel.size()), mat2(tmat.size());
+        for (int64_t t2 = 0; t2 < n_tiles; ++t2) {
+            std::copy(tel.begin() + torder[t2] * kLinTileN, tel.begin() + (torder[t2] + 1) * kLinTileN,
+                      el2.begin() + t2 * kLinTileN);
+            std::copy(tmat.begin() + torder[t2] * W, tmat.begin() + (torder[t2] + 1) * W, mat2.begin() + t2 * W);
         }
-        if (n_tiles * kLinTileN <= 2 * lo.E && R >= kLinTileMinRows) {
-            std::vector<double> rm(lo.table);
-            if ((rc = upload(h, rm, &h->d_lin_table_rm)) || (rc = upload(h, tel, &h->d_lin_tile_elems)) ||
-                (rc = upload(h, tmat, &h->d_lin_tile_mats)))
-                return rc;
-            h->lin_tiles = n_tiles;
-        }
+        tel.swap(el2);
+        tmat.swap(mat2);
+    }
+    const bool use_tiles = n_tiles * kLinTileN <= 2 * lo.E && R >= h->lin_min_rows;
+    if (tiles_only && !use_tiles) return 0;
+    std::vector<double> t(lo.table.size());
+    for (int m = 0; m < lo.n_mats(); ++m)
+        for (int i = 0; i < R; ++i)
+            for (int j = 0; j < R; ++j) t[m * RR + (size_t)j * R + i] = lo.table[m * RR + (size_t)i * R + j];
+    if ((rc = upload(h, t, &h->d_lin_table)) || (rc = upload(h, lo.self_mat, &h->d_lin_self))) return rc;
+    if (lo.slots > 0 && ((rc = upload(h, lo.nbr, &h->d_lin_nbr)) || (rc = upload(h, lo.nbr_mat, &h->d_lin_mat))))
+        return rc;
+    if (h->mixed && R <= kMixedFp32MaxBasis) {
+        std::vector<float> tf(t.begin(), t.end());
+        if ((rc = upload(h, tf, &h->d_lin_table_f))) return rc;
+    }
+    if (use_tiles) {
+        std::vector<double> rm(lo.table);
+        if ((rc = upload(h, rm, &h->d_lin_table_rm)) || (rc = upload(h, tel, &h->d_lin_tile_elems)) ||
+            (rc = upload(h, tmat, &h->d_lin_tile_mats)))
+            return rc;
+        h->lin_tiles = n_tiles;
     }
     h->lin_R = R;
     h->lin_slots = lo.slots;

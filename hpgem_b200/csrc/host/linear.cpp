@@ -7,6 +7,7 @@
 #include <cstring>
 #include <exception>
 #include <map>
+#include <utility>
 #include <stdexcept>
 #include <string>
 #include <thread>
@@ -57,6 +58,26 @@ void parallel_for(int64_t n, F &&f) {
     for (auto &th : pool) th.join();
     for (auto &e : errors)
         if (e) std::rethrow_exception(e);
+}
+
+// Key of a small geometry record (a Jacobian, a normal): every value rounded to
+// 2^-40 of the record's largest magnitude, so that records which differ only by
+// the rounding of the mesh coordinates (cells of width 1/6, say, whose
+// Jacobians carry entries of 1e-17 where a zero belongs) share their matrices;
+// the matrices of such records differ by ~1e-16 relative.
+std::string geometry_key(const double *v, int n, const int32_t *ints = nullptr, int ni = 0) {
+    std::string key;
+    for (int i = 0; i < ni; ++i) key.append(reinterpret_cast<const char *>(&ints[i]), sizeof(int32_t));
+    double big = 0.0;
+    for (int i = 0; i < n; ++i) big = std::max(big, std::fabs(v[i]));
+    int e = 0;
+    std::frexp(big, &e);
+    key.append(reinterpret_cast<const char *>(&e), sizeof(e));
+    for (int i = 0; i < n; ++i) {
+        const int64_t q = big == 0.0 ? 0 : (int64_t)std::nearbyint(std::ldexp(v[i], 40 - e));
+        key.append(reinterpret_cast<const char *>(&q), sizeof(q));
+    }
+    return key;
 }
 
 }  // namespace
@@ -121,11 +142,11 @@ LinearSystem assemble_linear(const hgg_problem_desc &desc) {
     std::vector<double> M(RR), K(RR), grad((size_t)nQ * nB * d), Jinv(9);
     const double *a = desc.advection;
     // the matrices depend on the element only through its Jacobian (affine
-    // elements): elements with the same Jacobian, bit for bit, share them
+    // elements): elements with the same Jacobian (geometry_key) share them
     std::map<std::string, std::pair<int32_t, int32_t>> by_jacobian;
     for (int64_t e = 0; e < s.E; ++e) {
         const double *J = desc.jacobians + e * d * d;
-        const std::string jkey(reinterpret_cast<const char *>(J), sizeof(double) * d * d);
+        const std::string jkey = geometry_key(J, d * d);
         auto known = by_jacobian.find(jkey);
         if (known != by_jacobian.end()) {
             s.mass_id[e] = known->second.first;
@@ -188,8 +209,7 @@ LinearSystem assemble_linear(const hgg_problem_desc &desc) {
         if (tab[0] < 0 || tab[1] < 0 || tab[0] >= desc.n_face_tabs || tab[1] >= desc.n_face_tabs)
             throw std::invalid_argument("bad face tabulation index");
         const double *n = desc.face_normals + f * d;
-        std::string fkey(reinterpret_cast<const char *>(tab), sizeof(tab));
-        fkey.append(reinterpret_cast<const char *>(n), sizeof(double) * d);
+        std::string fkey = geometry_key(n, d, tab, 2);
         auto known = by_face.find(fkey);
         if (known != by_face.end()) {
             for (int b = 0; b < 4; ++b) s.face_id[4 * f + b] = s.face_id[4 * known->second + b];
@@ -284,11 +304,22 @@ LinearOperators fold_linear(const LinearSystem &s) {
     out.nbr_mat.assign((size_t)s.E * out.slots, -1);
     for (int64_t e = 0; e < s.E; ++e) {
         std::vector<int32_t> key{s.mass_id[e], s.stiffness_id[e]};
+        std::sort(own[e].begin(), own[e].end());  // the same blocks give the same key in any face order
         key.insert(key.end(), own[e].begin(), own[e].end());
         out.self_mat[e] = product_id(std::move(key));
-        for (size_t k = 0; k < nb[e].size(); ++k) {
-            out.nbr[(size_t)e * out.slots + k] = nb[e][k].first;
-            out.nbr_mat[(size_t)e * out.slots + k] = product_id({s.mass_id[e], nb[e][k].second});
+        // neighbour slots ordered by their matrix: elements whose neighbour blocks
+        // are the same matrices get the same tuple whatever the order of their
+        // faces in the face list (periodic boundaries list them differently)
+        std::vector<std::pair<int32_t, int32_t>> slots_e;  // (matrix, neighbour)
+        for (size_t k = 0; k < nb[e].size(); ++k)
+            slots_e.push_back({product_id({s.mass_id[e], nb[e][k].second}), nb[e][k].first});
+        std::stable_sort(slots_e.begin(), slots_e.end(),
+                         [](const std::pair<int32_t, int32_t> &x, const std::pair<int32_t, int32_t> &y) {
+                             return x.first < y.first;
+                         });
+        for (size_t k = 0; k < slots_e.size(); ++k) {
+            out.nbr[(size_t)e * out.slots + k] = slots_e[k].second;
+            out.nbr_mat[(size_t)e * out.slots + k] = slots_e[k].first;
         }
     }
 

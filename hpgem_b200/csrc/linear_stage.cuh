@@ -128,9 +128,11 @@ __device__ __forceinline__ void dmma_m8n8k4(double &d0, double &d1, double a, do
                  : "d"(a), "d"(b));
 }
 
+// One tile (256 threads).  Called by the one-problem launch (tile = blockIdx.x)
+// and by the batch's persistent launch (tile = the block's index in its problem).
 template <typename KT>
-__global__ void __launch_bounds__(256) linear_tile_stage(const StageIOT<KT> io, const LinearGeom g,
-                                                          const LinearTiles t) {
+__device__ __forceinline__ void linear_tile_body(const StageIOT<KT> &io, const LinearGeom &g, const LinearTiles &t,
+                                                 int64_t tile) {
     // A chunk [kLinRows][kLinStride] and B chunk [kLinTileN][kLinStride]; the
     // output tile [kLinTileN][kLinOutStride] reuses the same memory
     __shared__ __align__(16) double sm[(kLinRows + kLinTileN) * kLinStride];
@@ -139,7 +141,6 @@ __global__ void __launch_bounds__(256) linear_tile_stage(const StageIOT<KT> io, 
     double *As = sm, *Bs = sm + kLinRows * kLinStride;
     const int R = g.R, S = g.slots;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, gid = lane >> 2, tig = lane & 3;
-    const int64_t tile = blockIdx.x;
     if (tid < kLinTileN) tel[tid] = t.elems[tile * kLinTileN + tid];
     const int passes = (R + kLinRows - 1) / kLinRows;
     for (int pass = 0; pass < passes; ++pass) {
@@ -168,22 +169,24 @@ __global__ void __launch_bounds__(256) linear_tile_stage(const StageIOT<KT> io, 
             }
             const double *A = g.table_rm + (size_t)m * R * R;
             for (int kc = 0; kc < R; kc += kLinKC) {
+                // only the fragments' extent is staged: rows up to the next band of 8,
+                // columns up to the next multiple of 4 (zeros beyond R)
+                const int kmax = min(kLinKC, R - kc), kw = (kmax + 3) & ~3, rw = (rows + 7) & ~7;
                 __syncthreads();  // src written; the previous chunk's fragments read
-                for (int i = tid; i < kLinRows * kLinKC; i += blockDim.x) {
-                    const int r = i / kLinKC, k = i % kLinKC;
+                for (int i = tid; i < rw * kw; i += blockDim.x) {
+                    const int r = i / kw, k = i % kw;
                     double v = 0.0;
-                    if (r < rows && kc + k < R) v = A[(size_t)(r0 + r) * R + kc + k];
+                    if (r < rows && k < kmax) v = A[(size_t)(r0 + r) * R + kc + k];
                     As[r * kLinStride + k] = v;
                 }
-                for (int i = tid; i < kLinTileN * kLinKC; i += blockDim.x) {
-                    const int n = i / kLinKC, k = i % kLinKC;
+                for (int i = tid; i < kLinTileN * kw; i += blockDim.x) {
+                    const int n = i / kw, k = i % kw;
                     const int32_t se = src[n];
                     double v = 0.0;
-                    if (se >= 0 && kc + k < R) v = stage_input(io, (int64_t)se * R + kc + k);
+                    if (se >= 0 && k < kmax) v = stage_input(io, (int64_t)se * R + kc + k);
                     Bs[n * kLinStride + k] = v;
                 }
                 __syncthreads();
-                const int kmax = min(kLinKC, R - kc);
                 for (int k4 = 0; k4 < kmax; k4 += 4) {
                     const double b = Bs[(warp * 8 + gid) * kLinStride + k4 + tig];
 #pragma unroll
@@ -211,6 +214,12 @@ __global__ void __launch_bounds__(256) linear_tile_stage(const StageIOT<KT> io, 
             stage_output(io, idx, io.u[idx], Os[n * kLinOutStride + r]);
         }
     }
+}
+
+template <typename KT>
+__global__ void __launch_bounds__(256) linear_tile_stage(const StageIOT<KT> io, const LinearGeom g,
+                                                          const LinearTiles t) {
+    linear_tile_body<KT>(io, g, t, blockIdx.x);
 }
 
 }  // namespace hgg

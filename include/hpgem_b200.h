@@ -164,7 +164,9 @@ int64_t hgg_vector_length(const hgg_handle *h);
 
 /* 1 when the sum-factorised tensor-product kernel drives this handle,
  * 0 when the dense reference-operator kernel does, 2 for the stored-matrix
- * kernel of a handle from hgg_create_linear*. */
+ * kernels: handles from hgg_create_linear*, and matrix-free handles whose
+ * operator the library folded into per-element matrices because the grouped
+ * tensor-core kernel applies them faster (advection on triangles, p >= 4). */
 int hgg_kernel_kind(const hgg_handle *h);
 
 /* When enabled (default), the last stage derivative k_S is stored like the

@@ -41,6 +41,8 @@ PROBLEMS = [
     ([2, 2, 2], True, 2, "wave", [1.0], "RK4_4", 1e-3, 5),              # dense, tets, wave
     ([6, 6], False, 1, "wave", [2.0], "RK4_4", 1e-3, 4),                # dense, squares, wave
     ([8, 8], False, 2, "advection", [1.0, 0.5], "DormandPrince", 1e-3, 3),  # other tableau
+    ([32, 32], True, 4, "advection", [0.8, -0.6], "RK4_4", 2e-4, 4),  # folded operator, tiles
+    ([32, 32], True, 5, "advection", [-0.6, 0.8], "RK4_4", 1e-4, 6),
 ]
 
 
@@ -75,7 +77,8 @@ def test_batch_matches_each_problem_alone(autotune):
         solvers.append(s)
         u0s.append(u0)
         slots.append(batch.add(s, pr[6], pr[7]))
-    assert batch.num_classes == 7
+    assert batch.num_classes == 9
+    assert solvers[-1].handle.kernel_kind == "linear"
     batch.step(max(pr[7] for pr in PROBLEMS) + 2)  # extra steps: finished problems stay put
     batch.synchronize()
     for pr, s, u0, slot in zip(PROBLEMS, solvers, u0s, slots):
@@ -140,4 +143,34 @@ def test_batch_rejects_bad_arguments():
         batch.add(t, 1e-3, 3)  # full
     with pytest.raises(_native.NativeError):
         batch.remove(5)
+    batch.close()
+
+
+def test_batch_steps_stored_matrix_handles():
+    """HpgemAPILinear handles (grouped tile kernel) in a batch beside a matrix-free
+    handle give the same coefficients as stepped alone."""
+    specs = [(hpgem_b200.HpgemAPILinear, [6, 6, 6], 2, 1e-3, 5), (hpgem_b200.HpgemAPILinear, [4, 4, 4], 3, 5e-4, 3),
+             (hpgem_b200.HpgemAPISimplified, [6, 6, 6], 2, 1e-3, 4)]
+    a = [1.0, 0.7, 0.3]
+
+    def build(cls, cells, p):
+        s = cls(3, p, "advection", advection=a, tableau="RK4_4").readMesh(desc(cells))
+        return s
+
+    batch = hpgem_b200.Batch(8)
+    runs = []
+    for cls, cells, p, dt, steps in specs:
+        s = build(cls, cells, p)
+        u0 = np.random.default_rng(p).standard_normal(s.handle.vector_length)
+        s.setTimeIntegrationVector(0, u0)
+        runs.append((s, u0, batch.add(s, dt, steps)))
+    assert runs[0][0].handle.kernel_kind == "linear"
+    batch.step(6)
+    batch.synchronize()
+    for (cls, cells, p, dt, steps), (s, u0, slot) in zip(specs, runs):
+        assert batch.remaining(slot) == 0
+        ref = build(cls, cells, p)
+        ref.setTimeIntegrationVector(0, u0)
+        ref.computeTimeSteps(0.0, dt, steps)
+        assert rel_err(s.getTimeIntegrationVector(0), ref.getTimeIntegrationVector(0)) < RTOL
     batch.close()

@@ -129,8 +129,24 @@ def test_triangles_dense_kernel(p):
     theta = 0.3 + p
     a = [math.cos(theta), math.sin(theta)]
     got, ref, solver = run_pair(desc([6, 6], triangular=True), p, "advection", a, "RK4_4", 1e-3, 4)
+    # too few elements per operator group for the folded form: the dense kernel runs
     assert solver.handle.kernel_kind == "dense"
     assert rel_err(got, ref) < RTOL
+
+
+@pytest.mark.parametrize("p", [4, 5])
+def test_triangles_folded_operator(p):
+    """From p = 4 on a mesh whose elements fill tiles of equal operators, the
+    advection operator is folded into per-element matrices and applied by the
+    stored-matrix tensor-core kernel."""
+    theta = 0.7 + p
+    a = [math.cos(theta), math.sin(theta)]
+    got, ref, solver, gk, rk = run_pair(desc([32, 32], triangular=True), p, "advection", a, "RK4_4", 2e-4, 3,
+                                        stages=True)
+    assert solver.handle.kernel_kind == "linear"
+    assert rel_err(got, ref) < solver.solution_rtol
+    for x, y in zip(gk, rk):
+        assert rel_err(x, y) < solver.stage_rtol
 
 
 @pytest.mark.parametrize("p", [1, 2, 3])
