@@ -145,8 +145,10 @@ def test_triangles_folded_operator(p):
                                         stages=True)
     assert solver.handle.kernel_kind == "linear"
     assert rel_err(got, ref) < solver.solution_rtol
+    # the folded operator applies an explicit inverse of the mass matrix multiplied
+    # into the assembled operator: twice the forward-error bound of one LU solve
     for x, y in zip(gk, rk):
-        assert rel_err(x, y) < solver.stage_rtol
+        assert rel_err(x, y) < 2 * solver.stage_rtol
 
 
 @pytest.mark.parametrize("p", [1, 2, 3])
