@@ -24,7 +24,7 @@ EXPORTED = ["hgg_create", "hgg_destroy", "hgg_last_error", "hgg_set_state", "hgg
             "hgg_create_structured", "hgg_structured_descriptor", "hgg_free_descriptor",
             "hgg_create_mesh_file", "hgg_mesh_file_descriptor",
             "hgg_create_linear", "hgg_linear_descriptor", "hgg_free_linear_descriptor",
-            "hgg_create_linear_structured",
+            "hgg_create_linear_structured", "hgg_create_linear_mesh_file",
             "hgg_quadrature_points", "hgg_num_quadrature_points",
             "hgg_project", "hgg_num_error_points", "hgg_error_points", "hgg_l2_error", "hgg_max_error",
             "hgg_time_derivative_static", "hgg_step_adaptive", "hgg_set_error_estimate",
@@ -156,6 +156,8 @@ def load():
         "hgg_free_linear_descriptor": (None, [H]),
         "hgg_create_linear_structured": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int32, ctypes.c_int32, P,
                                                         ctypes.c_char_p, ctypes.c_int32, ctypes.POINTER(H)]),
+        "hgg_create_linear_mesh_file": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int32, ctypes.c_int32, P,
+                                                       ctypes.c_char_p, ctypes.c_int32, ctypes.POINTER(H)]),
         "hgg_quadrature_points": (ctypes.c_int, [H, P]),
         "hgg_num_quadrature_points": (ctypes.c_int32, [H]),
         "hgg_project": (ctypes.c_int, [H, P, ctypes.c_int32]),

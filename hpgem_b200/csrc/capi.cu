@@ -1375,14 +1375,20 @@ int hgg_create_structured(const char *description, int32_t order, int32_t physic
 }  // extern "C"
 
 namespace {
-// HpgemAPILinear's matrices of a structured mesh (host), with the problem they came from
+// HpgemAPILinear's matrices of a structured mesh or a mesh file (host), with the
+// problem they came from
 int linear_structured_system(const char *description, int32_t order, int32_t physics, const double *params,
-                             const char *tableau, StructuredProblem &P, LinearSystem &sys) {
+                             const char *tableau, StructuredProblem &P, LinearSystem &sys,
+                             const char *mesh_file = nullptr) {
     if (physics != HGG_PHYSICS_ADVECTION && physics != HGG_PHYSICS_WAVE)
         return fail(nullptr, HGG_ERR_UNSUPPORTED,
                     "the stored-matrix form has the reference's linear advection and central-flux wave");
+    if (mesh_file) {
+        int rc = mesh_file_problem(mesh_file, order, physics, params, tableau, P);
+        if (rc) return rc;
+    }
     try {
-        P = build_structured(description, order, physics, params, tableau);
+        if (!mesh_file) P = build_structured(description, order, physics, params, tableau);
         hgg_problem_desc d;
         fill_descriptor(P, HGG_PRECISION_FP64, d);
         sys = assemble_linear(d);
@@ -1480,13 +1486,15 @@ int hgg_linear_descriptor(const char *description, int32_t order, int32_t physic
 
 void hgg_free_linear_descriptor(void *owner) { delete static_cast<LinearDescOwner *>(owner); }
 
-int hgg_create_linear_structured(const char *description, int32_t order, int32_t physics, const double *params,
-                                 const char *tableau, int32_t precision, hgg_handle **out) {
-    if (!description || !out || !tableau) return fail(nullptr, HGG_ERR_INVALID, "null argument");
+}  // extern "C"
+
+namespace {
+int create_linear_from(const char *description, const char *mesh_file, int32_t order, int32_t physics,
+                       const double *params, const char *tableau, int32_t precision, hgg_handle **out) {
     *out = nullptr;
     std::unique_ptr<StructuredProblem> sp(new StructuredProblem());
     LinearSystem sys;
-    int rc = linear_structured_system(description, order, physics, params, tableau, *sp, sys);
+    int rc = linear_structured_system(description, order, physics, params, tableau, *sp, sys, mesh_file);
     if (rc) return rc;
     hgg_problem_desc d;
     fill_descriptor(*sp, precision, d);
@@ -1501,6 +1509,21 @@ int hgg_create_linear_structured(const char *description, int32_t order, int32_t
     butcher_error_estimate(tableau, h->rk_err, h->rk_order);
     *out = h;
     return 0;
+}
+}  // namespace
+
+extern "C" {
+
+int hgg_create_linear_structured(const char *description, int32_t order, int32_t physics, const double *params,
+                                 const char *tableau, int32_t precision, hgg_handle **out) {
+    if (!description || !out || !tableau) return fail(nullptr, HGG_ERR_INVALID, "null argument");
+    return create_linear_from(description, nullptr, order, physics, params, tableau, precision, out);
+}
+
+int hgg_create_linear_mesh_file(const char *path, int32_t order, int32_t physics, const double *params,
+                                const char *tableau, int32_t precision, hgg_handle **out) {
+    if (!path || !out || !tableau) return fail(nullptr, HGG_ERR_INVALID, "null argument");
+    return create_linear_from(nullptr, path, order, physics, params, tableau, precision, out);
 }
 
 int32_t hgg_num_quadrature_points(const hgg_handle *h) { return h && h->sp ? h->sp->rule.size() : -1; }

@@ -66,6 +66,16 @@ class Handle:
         return cls(h)
 
     @classmethod
+    def linear_mesh_file(cls, path, order, physics, params, tableau="RK4_4", precision=_native.PRECISION_FP64):
+        """HpgemAPILinear on a Preprocessor "mesh 2" file (hgg_create_linear_mesh_file)."""
+        lib = _native.load()
+        h = ctypes.c_void_p()
+        p = np.ascontiguousarray(np.asarray(params, dtype=np.float64).reshape(-1))
+        _native.check(lib.hgg_create_linear_mesh_file(str(path).encode(), int(order), int(physics), _ptr(p),
+                                                      tableau.encode(), int(precision), ctypes.byref(h)))
+        return cls(h)
+
+    @classmethod
     def linear(cls, mass, element_stiffness, face_elements, face_stiffness, rk_a, rk_b, rk_c=None,
                precision=_native.PRECISION_FP64):
         """HpgemAPILinear from the matrices hpGEM stored (hgg_create_linear): mass and
@@ -388,6 +398,19 @@ class HpgemAPILinear(HpgemAPISimplified):
         self._mass = None
         self.n_basis = _basis_count(self.dim, description, self.polynomialOrder)
         self.n_elements = self.handle.vector_length // (self.numberOfVariables * self.n_basis)
+        return self
+
+    def readMeshFile(self, path):
+        """readMesh(fileName) + tasksBeforeSolving on a Preprocessor "mesh 2" file."""
+        from .descriptor import mesh_file_descriptor
+        D = mesh_file_descriptor(str(path), self.polynomialOrder, self._physics_code, self.params, self.tableau)
+        self.handle = Handle.linear_mesh_file(path, self.polynomialOrder, self._physics_code, self.params,
+                                              self.tableau, self.precision)
+        self._description = None
+        self._mesh_file = str(path)
+        self._mass = None
+        self.n_basis = D["n_basis"]
+        self.n_elements = D["n_elements"]
         return self
 
 

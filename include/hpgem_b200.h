@@ -348,6 +348,11 @@ int hgg_create_linear_structured(const char *description, int32_t order, int32_t
                                  const double *params, const char *tableau, int32_t precision,
                                  hgg_handle **out);
 
+/* The same from a Preprocessor "mesh 2" file (HpgemAPILinear::readMesh(fileName),
+ * HpgemAPILinear_Impl.h:107-129; the file as for hgg_create_mesh_file). */
+int hgg_create_linear_mesh_file(const char *path, int32_t order, int32_t physics, const double *params,
+                                const char *tableau, int32_t precision, hgg_handle **out);
+
 /* ---- many problems at once ------------------------------------------------
  * No counterpart in the reference (hpGEM advances one mesh per process).  A
  * batch advances many independent problems, each an existing handle with its

@@ -134,3 +134,21 @@ def test_read_mesh_file_solves_like_read_mesh():
         errors.append(s.computeTotalError(exact, 0.2))
     assert abs(errors[0] - errors[1]) <= 1e-12 * errors[1]
     assert errors[0] < 0.2  # p = 2 on 4^3 hexahedra: the solution is resolved
+
+
+@pytest.mark.gpu
+def test_linear_read_mesh_file_steps_like_structured():
+    """HpgemAPILinear from the file steps like HpgemAPILinear from its structured source."""
+    out = []
+    for route in ("file", "structured"):
+        s = hpgem_b200.HpgemAPILinear(3, 2, "wave", c_inv=1.0, tableau="RK4_4")
+        if route == "file":
+            s.readMeshFile(path_of("unitCubeN4Per"))
+        else:
+            s.readMesh(source_description("unitCubeN4Per"))
+        assert s.handle.kernel_kind == "linear"
+        u0 = np.random.default_rng(4).standard_normal(s.handle.vector_length)
+        s.setTimeIntegrationVector(0, u0)
+        s.handle.step(0.0, 1e-3, 5)
+        out.append(s.getTimeIntegrationVector(0))
+    assert np.abs(out[0] - out[1]).max() <= 1e-12 * np.abs(out[1]).max()
