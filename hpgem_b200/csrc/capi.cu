@@ -640,8 +640,8 @@ int create_from_desc(const hgg_problem_desc *desc, hgg_handle *h, bool linear = 
         // matrix slot (the reference's integrands assembled once, the mass inverse
         // folded in: the same operator as the matrix-free kernel to rounding), and
         // the grouped FP64 tensor-core kernel of the stored-matrix path applies it
-        // faster than the per-row dense kernel (256^2 cells, RK4: 0.34 against 0.46
-        // ms per step at p = 4, 0.49 against 0.87 at p = 5; in the mixed form p = 4
+        // faster than the per-row dense kernel (256^2 cells, RK4: 0.39 against 0.46
+        // ms per step at p = 4, 0.48 against 0.87 at p = 5; in the mixed form p = 4
         // measured 0.33 against 0.29 and stays on the dense kernel).  Only when the
         // mesh forms tiles (structured meshes); otherwise the dense kernel runs.
         if (op.physics == HGG_PHYSICS_ADVECTION && op.shape == HGG_SHAPE_TRIANGLE &&
@@ -749,7 +749,8 @@ int attach_linear(hgg_handle *h, const LinearSystem &sys, bool tiles_only) {
     // on structured meshes) and an element has at least kLinTileMinRows rows
     // (below that the padding of the 8-row fragments and the per-chunk
     // synchronisation cost more than the row kernel: measured on quadrilaterals
-    // at p = 2, 9 rows, 0.82 ms per RK4 step against 0.46 ms on 512^2 cells).
+    // at p = 2, 9 rows, 0.82 ms per RK4 step against 0.46 ms on 512^2 cells;
+    // on 256^2 triangles the tiles won from 15 rows: 0.39 against 0.46 ms).
     std::vector<int32_t> tel, tmat;
     int64_t n_tiles = 0;
     {

@@ -115,7 +115,7 @@ constexpr int kLinKC = 32;               // k (column) chunk staged in shared me
 constexpr int kLinRows = 64;             // output rows per pass
 constexpr int kLinStride = kLinKC + 4;   // padded row stride (doubles): fragment loads conflict-free
 constexpr int kLinOutStride = kLinRows + 1;
-constexpr int kLinTileMinRows = 24;      // smaller elements run the row kernel
+constexpr int kLinTileMinRows = 15;      // smaller elements run the row kernel
 
 struct LinearTiles {
     const int32_t *elems;  // [n_tiles][kLinTileN] element ids, -1: padding
@@ -173,18 +173,19 @@ __device__ __forceinline__ void linear_tile_body(const StageIOT<KT> &io, const L
                 // columns up to the next multiple of 4 (zeros beyond R)
                 const int kmax = min(kLinKC, R - kc), kw = (kmax + 3) & ~3, rw = (rows + 7) & ~7;
                 __syncthreads();  // src written; the previous chunk's fragments read
-                for (int i = tid; i < rw * kw; i += blockDim.x) {
-                    const int r = i / kw, k = i % kw;
-                    double v = 0.0;
-                    if (r < rows && k < kmax) v = A[(size_t)(r0 + r) * R + kc + k];
-                    As[r * kLinStride + k] = v;
-                }
-                for (int i = tid; i < kLinTileN * kw; i += blockDim.x) {
-                    const int n = i / kw, k = i % kw;
-                    const int32_t se = src[n];
-                    double v = 0.0;
-                    if (se >= 0 && k < kmax) v = stage_input(io, (int64_t)se * R + kc + k);
-                    Bs[n * kLinStride + k] = v;
+                // lane = column, warp = row (no integer division; a row's columns coalesce)
+                if (lane < kw) {
+                    for (int r = warp; r < rw; r += 8) {
+                        double v = 0.0;
+                        if (r < rows && lane < kmax) v = A[(size_t)(r0 + r) * R + kc + lane];
+                        As[r * kLinStride + lane] = v;
+                    }
+                    for (int n = warp; n < kLinTileN; n += 8) {
+                        const int32_t se = src[n];
+                        double v = 0.0;
+                        if (se >= 0 && lane < kmax) v = stage_input(io, (int64_t)se * R + kc + lane);
+                        Bs[n * kLinStride + lane] = v;
+                    }
                 }
                 __syncthreads();
                 for (int k4 = 0; k4 < kmax; k4 += 4) {
