@@ -121,3 +121,21 @@ def test_linear_create_reports_a_missing_device_or_succeeds():
 def test_python_class_takes_the_linear_applications_only():
     with pytest.raises(ValueError):
         hpgem_b200.HpgemAPILinear(2, 2, "wave_upwind")
+
+
+def test_linear_mesh_file_reports_a_missing_device_or_succeeds():
+    import os
+    lib = _native.load()
+    h = ctypes.c_void_p()
+    a = (ctypes.c_double * 3)(1.0, 0.7, 0.3)
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "mesh_files", "unitCubeN4Per.hpgem")
+    rc = lib.hgg_create_linear_mesh_file(path.encode(), 2, 0, a, b"RK4_4", 0, ctypes.byref(h))
+    if rc == 0:
+        assert lib.hgg_kernel_kind(h) == 2
+        lib.hgg_destroy(h)
+    else:
+        assert rc == -6 and b"device" in lib.hgg_last_error(None)
+    # a missing file and the upwind wave are rejected before any device is touched
+    assert lib.hgg_create_linear_mesh_file(b"/nonexistent.hpgem", 2, 0, a, b"RK4_4", 0, ctypes.byref(h)) == -1
+    assert lib.hgg_create_linear_mesh_file(path.encode(), 2, _native.PHYSICS_WAVE_UPWIND, a, b"RK4_4", 0,
+                                           ctypes.byref(h)) == -2
