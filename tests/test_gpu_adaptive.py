@@ -93,3 +93,27 @@ def test_adaptive_solve_reaches_the_final_time_and_tableaux_without_estimate_ref
     r = hpgem_b200.Advection(2, 2, [1.0, 0.5], tableau="RK4_4").readMesh(desc([4, 4]))
     with pytest.raises(_native.NativeError):
         r.computeOneTimeStepAdaptive(0.0, 1e-6, 0.1)
+
+
+def test_adaptive_steps_on_stored_matrix_handles():
+    """The adaptive control on HpgemAPILinear handles (row kernel and tile kernel)
+    takes the steps of the matrix-free handle of the same physics."""
+    for cells, p in (([8, 8], 2), ([4, 4, 4], 3)):
+        d = len(cells)
+        a = [1.0, 0.5, 0.3][:d]
+        out = []
+        for cls in (hpgem_b200.HpgemAPILinear, hpgem_b200.HpgemAPISimplified):
+            s = cls(d, p, "advection", advection=a, tableau="DormandPrince").readMesh(desc(cells, False))
+            s.setInitialSolution(lambda x: np.sin(2 * np.pi * x).prod(axis=1))
+            s.dtEstimate = 0.05
+            steps = []
+            t = 0.0
+            for _ in range(4):
+                t = s.computeOneTimeStepAdaptive(t, 1e-7, 0.25)
+                steps.append((s.lastDt, s.lastRejections))
+            out.append((steps, s.getTimeIntegrationVector(0)))
+        (lin_steps, u_lin), (free_steps, u_free) = out
+        assert [r for _, r in lin_steps] == [r for _, r in free_steps]
+        for (x, _), (y, _) in zip(lin_steps, free_steps):
+            assert math.isclose(x, y, rel_tol=DT_RTOL)
+        assert rel_err(u_lin, u_free) < 1e-9
