@@ -521,7 +521,8 @@ int check_status(hgg_handle *h) {
     HGG_CUDA(h, cudaStreamSynchronize(h->stream));
     if (st)
         return fail(h, HGG_ERR_DEVICE,
-                    "kernel status word " + std::to_string(st) + " (bit 0: bad neighbour index, bit 1: bad matrix index)");
+                    "kernel status word " + std::to_string(st) +
+                        " (bit 0: bad neighbour index, bit 1: a bounded wait ran out, bit 2: bad matrix index)");
     return 0;
 }
 

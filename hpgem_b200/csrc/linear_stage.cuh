@@ -15,6 +15,8 @@
 
 namespace hgg {
 
+// Status word bits set here: 1 a neighbour index out of range, 4 a matrix
+// index out of range (2 is the bounded-wait bit of the persistent kernels).
 struct LinearGeom {
     const double *table;      // [n_mats][R][R] transposed: table[m][j][i] = (matrix m)_{ij}
     const double *table_rm;   // [n_mats][R][R] row-major (the grouped kernel's copy), or null
@@ -84,13 +86,13 @@ __global__ void __launch_bounds__(256) linear_stage(const StageIOT<KT> io, const
 #pragma unroll 8
         for (int j = 0; j < R; ++j) acc += op[(size_t)j * R] * w[j];
     } else {
-        atomicOr(io.status, 2);
+        atomicOr(io.status, 4);
     }
     for (int s = 0; s < S; ++s) {
         m = g.nbr_mat[e * S + s];
         if (m < 0) continue;
         if (m >= g.n_mats) {
-            atomicOr(io.status, 2);
+            atomicOr(io.status, 4);
             continue;
         }
         const CT *op = T + (size_t)m * RR + r;
@@ -153,7 +155,7 @@ __device__ __forceinline__ void linear_tile_body(const StageIOT<KT> &io, const L
             const int32_t m = t.mats[tile * (S + 1) + s];  // the same for the whole block
             if (m < 0) continue;
             if (m >= g.n_mats) {
-                if (tid == 0) atomicOr(io.status, 2);
+                if (tid == 0) atomicOr(io.status, 4);
                 continue;
             }
             __syncthreads();  // tel written; src, As, Bs free
