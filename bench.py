@@ -25,6 +25,14 @@ the exact translated bump u0(x - a t) (periodic wrap; rule of order 2p+2), and
 for the mixed form its L2 distance and largest relative coefficient difference
 to the FP64 solution.
 
+Secondary legs in the same line (rank 0, one GPU): `tet_wave` (32^3 x 5
+periodic tetrahedra, p = 2, acoustic wave with the upwind flux in both forms
+and the central flux in FP64), `linear` (HpgemAPILinear's stored matrices on
+the benchmark mesh, FP64 tensor-core tiles, roofline against cuBLAS DGEMM
+measured in the same run), `batched` (512 seeded 2D problems in one batch) and
+`served` (a seeded Poisson request stream through the serving loop, p50/p99
+latency).  `--only linear|tet_wave` runs one of them alone for profiling.
+
 --impl reference times the CPU oracle (the restated hpGEM loop: quadrature
 loops, per-element mass matrix rebuilt and LU-solved every stage) on all host
 cores as independent replica processes, each on a 2^3 sample of the same mesh
