@@ -15,14 +15,7 @@
 #include <string>
 #include <vector>
 
-#include "../../include/hpgem_b200.h"
-#include "dg_kernels.cuh"
-#include "linear_stage.cuh"
-#include "tensor_pipe.cuh"
-#include "tensor_slice.cuh"
-#include "host/linear.h"
-#include "host/operators.h"
-#include "host/setup.h"
+#include "handle.cuh"
 
 using namespace hgg;
 
@@ -30,80 +23,9 @@ namespace {
 
 thread_local std::string g_create_error = "no error";
 
-struct DevBuf {
-    void *p = nullptr;
-    size_t bytes = 0;
-};
-
 }  // namespace
 
-struct hgg_handle {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    cudaStream_t own_stream = nullptr;
-    HostOperators op;
-    std::unique_ptr<StructuredProblem> sp;  // set when built from a structured description
-    int S = 0;
-    std::vector<double> rk_a, rk_b, rk_c;
-    std::vector<double> rk_err;   // error coefficients of an embedded tableau (empty: none)
-    int rk_order = 0;
-    int64_t N = 0;                 // doubles per vector
-    int64_t N_alloc = 0;           // doubles allocated per vector (whole tiles)
-    double *sol[2] = {nullptr, nullptr};
-    int cur = 0;                   // which sol[] holds the solution
-    std::vector<void *> k;         // S stage vectors (double, or float in the FP32-mixed form)
-    bool mixed = false;            // FP32-mixed form: float stage vectors and contractions
-    std::vector<DevBuf> bufs;      // every device allocation
-    // device operator / geometry arrays
-    double *d_vol = nullptr, *d_pairs = nullptr, *d_elem_geo = nullptr, *d_face_geo = nullptr;
-    float *d_vol_f = nullptr, *d_pairs_f = nullptr;  // FP32-mixed form: the dense operators in FP32
-    int32_t *d_nbr = nullptr, *d_self = nullptr, *d_nbrp = nullptr;
-    int8_t *d_mode = nullptr;
-    double *d_ahat = nullptr, *d_tsigma = nullptr;
-    int32_t *d_tnbr = nullptr;
-    int8_t *d_tmode = nullptr;
-    unsigned char *d_pgeo = nullptr;  // packed per-element geometry of the pipelined kernel
-    int tile_elems = 1;               // elements per tile (common multiple of the tensor kernels' tiles)
-    int variant = 0;                  // 0: automatic, 1: one-shot, 2: pipelined kernel
-    bool tensor_layout = false;       // device vectors in tensor order (signs folded)
-    bool tiled = false;               // ... and in tiles of 32 elements, coefficient-major (slice kernel)
-    double *d_scratch = nullptr;      // one vector, for layout conversion of set/get_state
-    double *d_reduce = nullptr;       // adaptive steps and error norms: per-element values, partial sums
-    double *d_exact = nullptr;        // error norms: the caller's exact values on the device
-    size_t exact_cap = 0;
-    double *d_maxbuf = nullptr;
-    double *d_err_basis = nullptr, *d_err_w = nullptr, *d_elem_basis = nullptr, *d_absdet = nullptr;
-    int32_t *d_tpos = nullptr;        // hpGEM index -> tensor position
-    double *d_tsign = nullptr;
-    // slice kernel (hexahedra, p = 3): per-element records of SliceShape::GR doubles
-    bool slice_ok = false;
-    double *d_slice_geo = nullptr;
-    // stored-matrix form (HpgemAPILinear): distinct folded matrices, transposed
-    bool linear = false;
-    int lin_R = 0, lin_slots = 0, lin_mats = 0;
-    double *d_lin_table = nullptr;
-    float *d_lin_table_f = nullptr;  // FP32-mixed form with FP32 contractions (R <= kMixedFp32MaxBasis)
-    int32_t *d_lin_self = nullptr, *d_lin_nbr = nullptr, *d_lin_mat = nullptr;
-    // grouped DMMA kernel: tiles of elements with identical matrices (0 tiles: not used)
-    double *d_lin_table_rm = nullptr;
-    int32_t *d_lin_tile_elems = nullptr, *d_lin_tile_mats = nullptr;
-    int64_t lin_tiles = 0;
-    int lin_min_rows = kLinTileMinRows;  // fewer rows per element: the row kernel
-    // grouped dense kernel: tiles of kGroupTile elements with the same operator signature
-    int32_t *d_group_tiles = nullptr;
-    int64_t group_tiles = 0;
-    int num_sms = 148;
-    int *d_status = nullptr;
-    bool store_last = true;
-    int64_t launches = 0;
-    // graph of one full step, per starting buffer, valid for (dt, store_last)
-    cudaGraphExec_t graph[2] = {nullptr, nullptr};
-    double graph_dt = 0.0;
-    bool graph_store_last = true;
-    std::string err = "no error";
-};
-
-namespace {
+namespace hgg {
 
 int fail(hgg_handle *h, int code, const std::string &msg) {
     if (h) h->err = msg;
@@ -111,27 +33,7 @@ int fail(hgg_handle *h, int code, const std::string &msg) {
     return code;
 }
 
-#define HGG_CUDA(h, call)                                                                    \
-    do {                                                                                     \
-        cudaError_t _e = (call);                                                             \
-        if (_e != cudaSuccess)                                                               \
-            return fail(h, HGG_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(_e)); \
-    } while (0)
 
-template <typename T>
-int upload(hgg_handle *h, const std::vector<T> &v, T **dst) {
-    *dst = nullptr;
-    if (v.empty()) return 0;
-    void *p = nullptr;
-    size_t bytes = v.size() * sizeof(T);
-    cudaError_t e = cudaMalloc(&p, bytes);
-    if (e != cudaSuccess) return fail(h, HGG_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
-    h->bufs.push_back({p, bytes});
-    e = cudaMemcpyAsync(p, v.data(), bytes, cudaMemcpyHostToDevice, h->stream);
-    if (e != cudaSuccess) return fail(h, HGG_ERR_CUDA, std::string("cudaMemcpyAsync: ") + cudaGetErrorString(e));
-    *dst = (T *)p;
-    return 0;
-}
 
 int alloc(hgg_handle *h, size_t bytes, void **dst) {
     void *p = nullptr;
@@ -149,39 +51,12 @@ void release_graphs(hgg_handle *h) {
             g = nullptr;
         }
 }
-
 // ---- kernel dispatch ---------------------------------------------------------
 // The device vectors of a sum-factorised handle are already in tensor order
 // with the signs folded in, so the kernels see the identity permutation.
-template <int P, int DIM>
-TensorConsts<P, DIM> tensor_consts(const HostOperators &op) {
-    using TC = TensorConsts<P, DIM>;
-    TC tc;
-    for (int i = 0; i < TC::NP * TC::NP; ++i) tc.D1[i] = op.D1[i];
-    for (int i = 0; i < 2 * TC::NP; ++i) tc.lift[i] = op.lift[i];
-    tc.trace_pos[0] = op.trace_pos[0];
-    tc.trace_pos[1] = op.trace_pos[1];
-    for (int i = 0; i < TC::NB; ++i) {
-        tc.tpos[i] = (short)i;
-        tc.tinv[i] = (short)i;
-        tc.tsign[i] = 1.0;
-    }
-    return tc;
-}
 
 // layout conversion kernels (hpGEM order <-> tensor order, signs folded; tiled:
 // 32-element tiles, coefficient-major inside a tile)
-__device__ __forceinline__ int64_t device_index(int64_t e, int pos, int nb, bool tiled) {
-    return tiled ? (e >> 5) * ((int64_t)nb << 5) + (int64_t)pos * 32 + (e & 31) : e * nb + pos;
-}
-// stage vectors and per-stage coefficients of the error estimate and the rewind
-template <typename KT>
-struct ErrStages {
-    const KT *k[kMaxStages];
-    double err[kMaxStages];
-    double dt;
-    int n;
-};
 
 template <typename TD>
 __global__ void to_tensor_order(const double *src, TD *dst, const int32_t *tpos, const double *tsign,
@@ -210,228 +85,11 @@ __global__ void convert_vector(const float *src, double *dst, int64_t n) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
         dst[i] = (double)src[i];
 }
-
-template <typename KT>
-int launch_slice(hgg_handle *h, const StageIOT<KT> &io) {
-    const HostOperators &op = h->op;
-    SliceOps sops;
-    for (int i = 0; i < 16; ++i) sops.D[i] = op.D1[i];
-    for (int sd = 0; sd < 2; ++sd)
-        for (int a = 0; a < 4; ++a) sops.L[sd][a] = op.lift[sd * 4 + a];
-    const int64_t blocks = (op.nE + SliceShape::TE - 1) / SliceShape::TE;
-    const dim3 grid((unsigned)blocks), block(SliceShape::THREADS);
-    const bool fin = io.unew != nullptr;
-    // each block asks L2 for the inputs of the tile a block of the next resident wave runs
-    // (5 blocks per SM resident): measured 4 % faster per RK4 step for the FP32 form and
-    // 2-3 % for the FP64 form's first three stages; the FP64 final stage (4 resident
-    // blocks, three more input vectors) measured slower with it and goes without
-    const int64_t ahead = (sizeof(KT) == 4 || !io.unew) ? (int64_t)h->num_sms * 5 : 0;
-    if (io.nin == 0 && (!fin || io.nfin == 0))
-        tensor_slice<KT, 0, 0><<<grid, block, 0, h->stream>>>(io, h->d_slice_geo, sops, ahead);
-    else if (io.nin == 1 && (!fin || io.nfin == 0))
-        tensor_slice<KT, 1, 0><<<grid, block, 0, h->stream>>>(io, h->d_slice_geo, sops, ahead);
-    else if (io.nin == 1 && fin && io.nfin == 3)
-        tensor_slice<KT, 1, 3><<<grid, block, 0, h->stream>>>(io, h->d_slice_geo, sops, ahead);
-    else
-        tensor_slice<KT, -1, -1><<<grid, block, 0, h->stream>>>(io, h->d_slice_geo, sops, ahead);
-    return 0;
-}
-
-// shared memory of the pipelined kernel for a ring of `nbuf` slots of `nv` vectors
-template <int P, int DIM>
-size_t pipe_smem(int nbuf, int nv) {
-    using S = PipeShape<P, DIM>;
-    size_t tab_end = (64 + 8 * (S::NP * S::NP + 2 * S::NP + S::NB) + 4 * S::NB + 127) / 128 * 128;
-    size_t slot = (size_t)nv * S::TILE_VEC_BYTES + S::TILE_GEO_BYTES;
-    size_t tail = 8 * ((size_t)S::TE * S::NB * 3 + (size_t)S::TE * S::NS * S::NF);
-    return tab_end + nbuf * slot + tail;
-}
-
-template <int P, int DIM>
-int launch_tensor(hgg_handle *h, const StageIO &io) {
-    using TC = TensorConsts<P, DIM>;
-    const HostOperators &op = h->op;
-    TC tc = tensor_consts<P, DIM>(op);
-    using S = PipeShape<P, DIM>;
-    PipeArgs pa;
-    pa.nv = 1 + io.nin + (io.unew ? io.nfin : 0);
-    pa.slot_bytes = (uint32_t)((size_t)pa.nv * S::TILE_VEC_BYTES + S::TILE_GEO_BYTES);
-    // two blocks per SM when a ring of >= 3 slots fits, else one block with up to 8 slots
-    const size_t budget = 227 * 1024;
-    int per_sm = 2, nbuf = 0;
-    for (int b = 8; b >= 3; --b)
-        if (2 * (pipe_smem<P, DIM>(b, pa.nv) + 1024) <= budget) { nbuf = b; break; }
-    if (!nbuf) {
-        per_sm = 1;
-        for (int b = 8; b >= 2; --b)
-            if (pipe_smem<P, DIM>(b, pa.nv) <= budget) { nbuf = b; break; }
-    }
-    if (!nbuf && h->variant == 2)
-        return fail(h, HGG_ERR_UNSUPPORTED, "pipelined kernel: tile does not fit in shared memory");
-    // the one-shot kernel when asked for, or when a stage reads too many vectors for the ring
-    if (h->variant == 1 || !nbuf) {
-        constexpr int EPB = (256 / TC::NB) > 0 ? (256 / TC::NB) : 1;
-        TensorGeom geo{h->d_ahat, h->d_tnbr, h->d_tmode, h->d_tsigma};
-        int64_t blocks = (op.nE + EPB - 1) / EPB;
-        tensor_stage<double, P, DIM, EPB><<<(unsigned)blocks, EPB * TC::NB, 0, h->stream>>>(io, geo, tc);
-        return 0;
-    }
-    pa.geo = h->d_pgeo;
-    pa.n_tiles = (op.nE + S::TE - 1) / S::TE;
-    pa.nbuf = nbuf;
-    size_t smem = pipe_smem<P, DIM>(nbuf, pa.nv);
-    cudaFuncSetAttribute(tensor_pipe<P, DIM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    int64_t grid = std::min<int64_t>(pa.n_tiles, (int64_t)h->num_sms * per_sm);
-    tensor_pipe<P, DIM><<<(unsigned)grid, S::THREADS, smem, h->stream>>>(io, pa, tc);
-    return 0;
-}
-
-// elements per tile of the pipelined kernel for (order, dim)
-int pipe_tile_elems(int order, int dim) {
-#define HGG_TE(P) \
-    case P: return dim == 2 ? PipeShape<P, 2>::TE : PipeShape<P, 3>::TE;
-    switch (order) { HGG_TE(1) HGG_TE(2) HGG_TE(3) HGG_TE(4) HGG_TE(5) }
-#undef HGG_TE
-    return 1;
-}
-
-int pipe_geo_bytes(int dim) { return dim == 2 ? PipeShape<1, 2>::GEO_BYTES : PipeShape<1, 3>::GEO_BYTES; }
-
-template <int DIM>
-int launch_tensor_dim(hgg_handle *h, const StageIO &io) {
-    switch (h->op.order) {
-        case 1: return launch_tensor<1, DIM>(h, io);
-        case 2: return launch_tensor<2, DIM>(h, io);
-        case 3: return launch_tensor<3, DIM>(h, io);
-        case 4: return launch_tensor<4, DIM>(h, io);
-        case 5: return launch_tensor<5, DIM>(h, io);
-    }
-    return fail(h, HGG_ERR_UNSUPPORTED, "tensor kernel: order out of range");
-}
-
-// wave speed factor of the upwind wave flux, 0 for the central flux
-double upwind_speed(const HostOperators &op) {
-    return op.physics == HGG_PHYSICS_WAVE_UPWIND ? 1.0 / std::sqrt(op.c_inv) : 0.0;
-}
-
-// dense kernel launch for the handle's shape and physics
-template <typename KT>
-int launch_dense_any(hgg_handle *h, const StageIOT<KT> &io);
-
-// FP32-mixed form on squares and cubes other than the slice kernel's: the one-shot kernel
-template <int DIM>
-int launch_tensor_oneshot_f(hgg_handle *h, const StageIOT<float> &io) {
-    auto go = [&](auto pc) {
-        constexpr int P = decltype(pc)::value;
-        using TC = TensorConsts<P, DIM>;
-        constexpr int EPB = (256 / TC::NB) > 0 ? (256 / TC::NB) : 1;
-        const TC tc = tensor_consts<P, DIM>(h->op);
-        TensorGeom geo{h->d_ahat, h->d_tnbr, h->d_tmode, h->d_tsigma};
-        const int64_t blocks = (h->op.nE + EPB - 1) / EPB;
-        tensor_stage<float, P, DIM, EPB><<<(unsigned)blocks, EPB * TC::NB, 0, h->stream>>>(io, geo, tc);
-        return 0;
-    };
-    switch (h->op.order) {
-        case 1: return go(std::integral_constant<int, 1>{});
-        case 2: return go(std::integral_constant<int, 2>{});
-        case 3: return go(std::integral_constant<int, 3>{});
-        case 4: return go(std::integral_constant<int, 4>{});
-        case 5: return go(std::integral_constant<int, 5>{});
-    }
-    return fail(h, HGG_ERR_UNSUPPORTED, "tensor kernel: order out of range");
-}
-
-template <typename KT, int DIM, int NFL, int WAVE>
-int launch_dense(hgg_handle *h, const StageIOT<KT> &io) {
-    const HostOperators &op = h->op;
-    const int V = WAVE ? DIM + 1 : 1;
-    const int R = V * op.nB;
-    if (R > 256) return fail(h, HGG_ERR_UNSUPPORTED, "dense kernel: more than 256 coefficients per element");
-    int epb = std::max(1, 256 / dense_rows(DIM, WAVE, op.nB));
-    DenseGeom g{h->d_vol, h->d_pairs, h->d_vol_f, h->d_pairs_f, h->d_nbr, h->d_self, h->d_nbrp, h->d_mode,
-                h->d_elem_geo, h->d_face_geo, 1.0 / op.c_inv, upwind_speed(op), op.nB, epb};
-    int64_t blocks = (op.nE + epb - 1) / epb;
-    const int threads = dense_threads(DIM, WAVE, op.nB, epb);
-    const bool ok = dense_dispatch<DIM, NFL, WAVE>(op.nB, [&](auto nbc) {
-        constexpr int NB = decltype(nbc)::value;
-        // the grouped kernel where it measured faster: the wave with FP64 contractions
-        // (32^3 x 5 tetrahedra, p = 2, RK4: 1.12 against 2.01 ms per step upwind, 1.00
-        // against 1.71 central); with FP32 contractions, and for advection, the
-        // per-row kernel was as fast or faster (0.97 against 1.09 ms; 0.38 both)
-        if constexpr (DIM >= 2 && NB <= kGroupMaxRows && WAVE) {
-            const bool want = h->variant == 2 || (h->variant == 0 && std::is_same_v<DenseCT<KT, NB>, double>);
-            if (h->group_tiles > 0 && want) {
-                constexpr size_t gsmem = group_smem<DenseCT<KT, NB>, DIM, NFL, NB>();
-                if (gsmem > 48 * 1024)
-                    cudaFuncSetAttribute(dense_group_stage<KT, DIM, NFL, NB>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gsmem);
-                dense_group_stage<KT, DIM, NFL, NB>
-                    <<<(unsigned)h->group_tiles, kGroupTile * NB, gsmem, h->stream>>>(io, g, h->d_group_tiles);
-                return;
-            }
-        }
-        const size_t smem = dense_smem(DIM, NFL, WAVE, NB, epb, sizeof(DenseCT<KT, NB>));
-        if (smem > 48 * 1024)
-            cudaFuncSetAttribute(dense_stage<KT, DIM, NFL, WAVE, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)smem);
-        dense_stage<KT, DIM, NFL, WAVE, NB><<<(unsigned)blocks, threads, smem, h->stream>>>(io, g);
-    });
-    if (!ok) return fail(h, HGG_ERR_UNSUPPORTED, "dense kernel: no kernel for this basis size");
-    return 0;
-}
-
-template <typename KT>
-int launch_dense_any(hgg_handle *h, const StageIOT<KT> &io) {
-    const bool wave = h->op.physics != HGG_PHYSICS_ADVECTION;
-    switch (h->op.shape) {
-        case HGG_SHAPE_LINE: return wave ? launch_dense<KT, 1, 2, 1>(h, io) : launch_dense<KT, 1, 2, 0>(h, io);
-        case HGG_SHAPE_TRIANGLE: return wave ? launch_dense<KT, 2, 3, 1>(h, io) : launch_dense<KT, 2, 3, 0>(h, io);
-        case HGG_SHAPE_SQUARE: return wave ? launch_dense<KT, 2, 4, 1>(h, io) : launch_dense<KT, 2, 4, 0>(h, io);
-        case HGG_SHAPE_TETRAHEDRON: return wave ? launch_dense<KT, 3, 4, 1>(h, io) : launch_dense<KT, 3, 4, 0>(h, io);
-        case HGG_SHAPE_CUBE: return wave ? launch_dense<KT, 3, 6, 1>(h, io) : launch_dense<KT, 3, 6, 0>(h, io);
-    }
-    return fail(h, HGG_ERR_UNSUPPORTED, "shape");
-}
-
-template <typename KT>
-int launch_linear(hgg_handle *h, const StageIOT<KT> &io) {
-    const int R = h->lin_R;
-    const int epb = std::max(1, 256 / R);
-    LinearGeom g{h->d_lin_table, h->d_lin_table_rm, h->d_lin_table_f, h->d_lin_self, h->d_lin_nbr, h->d_lin_mat,
-                 R, h->lin_slots, epb, h->lin_mats};
-    if (h->lin_tiles > 0) {
-        LinearTiles t{h->d_lin_tile_elems, h->d_lin_tile_mats};
-        linear_tile_stage<KT><<<(unsigned)h->lin_tiles, 256, 0, h->stream>>>(io, g, t);
-        return 0;
-    }
-    const unsigned blocks = (unsigned)((h->op.nE + epb - 1) / epb);
-    const int threads = linear_threads(R, epb);
-    auto go = [&](auto ct) {
-        using CT = decltype(ct);
-        const size_t smem = linear_smem(R, h->lin_slots, epb, sizeof(CT));
-        if (smem > 48 * 1024)
-            cudaFuncSetAttribute(linear_stage<KT, CT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        linear_stage<KT, CT><<<blocks, threads, smem, h->stream>>>(io, g);
-    };
-    if (std::is_same_v<KT, float> && h->d_lin_table_f) go(float{});
-    else go(double{});
-    return 0;
-}
-
 int launch_stage(hgg_handle *h, const StageIO &io) {
-    const HostOperators &op = h->op;
     int rc;
-    if (h->linear) {
-        rc = launch_linear<double>(h, io);
-    } else if (h->slice_ok) {
-        rc = launch_slice<double>(h, io);
-    } else if (op.tensor) {
-        rc = op.dim == 2 ? launch_tensor_dim<2>(h, io)
-                         : (op.dim == 3 ? launch_tensor_dim<3>(h, io)
-                                        : fail(h, HGG_ERR_UNSUPPORTED, "tensor kernel needs dim 2 or 3"));
-    } else {
-        rc = launch_dense_any<double>(h, io);
-    }
+    if (h->linear) rc = launch_stage_linear(h, io);
+    else if (h->slice_ok || h->op.tensor) rc = launch_stage_tensor(h, io);
+    else rc = launch_stage_dense(h, io);
     if (rc) return rc;
     h->launches++;
     cudaError_t e = cudaGetLastError();
@@ -442,13 +100,9 @@ int launch_stage(hgg_handle *h, const StageIO &io) {
 // FP32-mixed form: the stage kernels that have it
 int launch_stage(hgg_handle *h, const StageIOT<float> &io) {
     int rc;
-    if (h->linear) rc = launch_linear<float>(h, io);
-    else if (h->slice_ok) rc = launch_slice(h, io);
-    else if (h->op.tensor)
-        rc = h->op.dim == 2 ? launch_tensor_oneshot_f<2>(h, io)
-                            : (h->op.dim == 3 ? launch_tensor_oneshot_f<3>(h, io)
-                                              : fail(h, HGG_ERR_UNSUPPORTED, "tensor kernel needs dim 2 or 3"));
-    else rc = launch_dense_any<float>(h, io);
+    if (h->linear) rc = launch_stage_linear(h, io);
+    else if (h->slice_ok || h->op.tensor) rc = launch_stage_tensor(h, io);
+    else rc = launch_stage_dense(h, io);
     if (rc) return rc;
     h->launches++;
     cudaError_t e = cudaGetLastError();
@@ -466,41 +120,6 @@ void *vector_ptr(hgg_handle *h, int vec) {
 }
 bool vector_is_float(const hgg_handle *h, int vec) { return h->mixed && vec >= 1; }
 
-// Inputs and outputs of stage i of one Runge-Kutta step from sol[from] into
-// sol[1 - from] (stages as in HpgemAPISimplified_Impl.h:788-820; zero tableau
-// entries are skipped).
-template <typename KT>
-StageIOT<KT> make_stage_io(const hgg_handle *h, int from, double dt, int i, int *status) {
-    const int S = h->S;
-    auto kv = [&](int j) { return static_cast<KT *>(h->k[j]); };
-    StageIOT<KT> io{};
-    io.u = h->sol[from];
-    io.n_elements = h->op.nE;
-    io.status = status;
-    for (int j = 0; j < i; ++j) {
-        double c = dt * h->rk_a[i * S + j];
-        if (c != 0.0) {
-            io.kin[io.nin] = kv(j);
-            io.cin[io.nin] = c;
-            io.nin++;
-        }
-    }
-    const bool last = i == S - 1;
-    io.kout = (!last || h->store_last) ? kv(i) : nullptr;
-    if (last) {
-        io.unew = h->sol[1 - from];
-        for (int j = 0; j < S - 1; ++j) {
-            double b = dt * h->rk_b[j];
-            if (b != 0.0) {
-                io.kfin[io.nfin] = kv(j);
-                io.bfin[io.nfin] = b;
-                io.nfin++;
-            }
-        }
-        io.blast = dt * h->rk_b[S - 1];
-    }
-    return io;
-}
 
 template <typename KT>
 int enqueue_step_t(hgg_handle *h, int from, double dt) {
@@ -832,7 +451,7 @@ void destroy_handle(hgg_handle *h) {
     delete h;
 }
 
-}  // namespace
+}  // namespace hgg
 
 extern "C" {
 
@@ -1757,8 +1376,3 @@ int hgg_max_error(hgg_handle *h, int32_t vec, const double *exact, double *max_e
 }
 
 }  // extern "C"
-
-// grouped execution of many problems (hgg_batch_*)
-#include "batch_exec.cuh"
-// serving loop over a batch (hgg_server_*)
-#include "server.cuh"

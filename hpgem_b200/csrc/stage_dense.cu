@@ -1,0 +1,101 @@
+// Stage launches of the dense kernels (simplices, the wave, lines) and of the
+// stored-matrix kernels (HpgemAPILinear and folded operators).
+#include <algorithm>
+#include <type_traits>
+
+#include "handle.cuh"
+
+namespace hgg {
+
+// wave speed factor of the upwind wave flux, 0 for the central flux
+double upwind_speed(const HostOperators &op) {
+    return op.physics == HGG_PHYSICS_WAVE_UPWIND ? 1.0 / std::sqrt(op.c_inv) : 0.0;
+}
+
+namespace {
+
+template <typename KT, int DIM, int NFL, int WAVE>
+int launch_dense(hgg_handle *h, const StageIOT<KT> &io) {
+    const HostOperators &op = h->op;
+    const int V = WAVE ? DIM + 1 : 1;
+    const int R = V * op.nB;
+    if (R > 256) return fail(h, HGG_ERR_UNSUPPORTED, "dense kernel: more than 256 coefficients per element");
+    int epb = std::max(1, 256 / dense_rows(DIM, WAVE, op.nB));
+    DenseGeom g{h->d_vol, h->d_pairs, h->d_vol_f, h->d_pairs_f, h->d_nbr, h->d_self, h->d_nbrp, h->d_mode,
+                h->d_elem_geo, h->d_face_geo, 1.0 / op.c_inv, upwind_speed(op), op.nB, epb};
+    int64_t blocks = (op.nE + epb - 1) / epb;
+    const int threads = dense_threads(DIM, WAVE, op.nB, epb);
+    const bool ok = dense_dispatch<DIM, NFL, WAVE>(op.nB, [&](auto nbc) {
+        constexpr int NB = decltype(nbc)::value;
+        // the grouped kernel where it measured faster: the wave with FP64 contractions
+        // (32^3 x 5 tetrahedra, p = 2, RK4: 1.12 against 2.01 ms per step upwind, 1.00
+        // against 1.71 central); with FP32 contractions, and for advection, the
+        // per-row kernel was as fast or faster (0.97 against 1.09 ms; 0.38 both)
+        if constexpr (DIM >= 2 && NB <= kGroupMaxRows && WAVE) {
+            const bool want = h->variant == 2 || (h->variant == 0 && std::is_same_v<DenseCT<KT, NB>, double>);
+            if (h->group_tiles > 0 && want) {
+                constexpr size_t gsmem = group_smem<DenseCT<KT, NB>, DIM, NFL, NB>();
+                if (gsmem > 48 * 1024)
+                    cudaFuncSetAttribute(dense_group_stage<KT, DIM, NFL, NB>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gsmem);
+                dense_group_stage<KT, DIM, NFL, NB>
+                    <<<(unsigned)h->group_tiles, kGroupTile * NB, gsmem, h->stream>>>(io, g, h->d_group_tiles);
+                return;
+            }
+        }
+        const size_t smem = dense_smem(DIM, NFL, WAVE, NB, epb, sizeof(DenseCT<KT, NB>));
+        if (smem > 48 * 1024)
+            cudaFuncSetAttribute(dense_stage<KT, DIM, NFL, WAVE, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem);
+        dense_stage<KT, DIM, NFL, WAVE, NB><<<(unsigned)blocks, threads, smem, h->stream>>>(io, g);
+    });
+    if (!ok) return fail(h, HGG_ERR_UNSUPPORTED, "dense kernel: no kernel for this basis size");
+    return 0;
+}
+
+template <typename KT>
+int launch_dense_any(hgg_handle *h, const StageIOT<KT> &io) {
+    const bool wave = h->op.physics != HGG_PHYSICS_ADVECTION;
+    switch (h->op.shape) {
+        case HGG_SHAPE_LINE: return wave ? launch_dense<KT, 1, 2, 1>(h, io) : launch_dense<KT, 1, 2, 0>(h, io);
+        case HGG_SHAPE_TRIANGLE: return wave ? launch_dense<KT, 2, 3, 1>(h, io) : launch_dense<KT, 2, 3, 0>(h, io);
+        case HGG_SHAPE_SQUARE: return wave ? launch_dense<KT, 2, 4, 1>(h, io) : launch_dense<KT, 2, 4, 0>(h, io);
+        case HGG_SHAPE_TETRAHEDRON: return wave ? launch_dense<KT, 3, 4, 1>(h, io) : launch_dense<KT, 3, 4, 0>(h, io);
+        case HGG_SHAPE_CUBE: return wave ? launch_dense<KT, 3, 6, 1>(h, io) : launch_dense<KT, 3, 6, 0>(h, io);
+    }
+    return fail(h, HGG_ERR_UNSUPPORTED, "shape");
+}
+
+template <typename KT>
+int launch_linear(hgg_handle *h, const StageIOT<KT> &io) {
+    const int R = h->lin_R;
+    const int epb = std::max(1, 256 / R);
+    LinearGeom g{h->d_lin_table, h->d_lin_table_rm, h->d_lin_table_f, h->d_lin_self, h->d_lin_nbr, h->d_lin_mat,
+                 R, h->lin_slots, epb, h->lin_mats};
+    if (h->lin_tiles > 0) {
+        LinearTiles t{h->d_lin_tile_elems, h->d_lin_tile_mats};
+        linear_tile_stage<KT><<<(unsigned)h->lin_tiles, 256, 0, h->stream>>>(io, g, t);
+        return 0;
+    }
+    const unsigned blocks = (unsigned)((h->op.nE + epb - 1) / epb);
+    const int threads = linear_threads(R, epb);
+    auto go = [&](auto ct) {
+        using CT = decltype(ct);
+        const size_t smem = linear_smem(R, h->lin_slots, epb, sizeof(CT));
+        if (smem > 48 * 1024)
+            cudaFuncSetAttribute(linear_stage<KT, CT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        linear_stage<KT, CT><<<blocks, threads, smem, h->stream>>>(io, g);
+    };
+    if (std::is_same_v<KT, float> && h->d_lin_table_f) go(float{});
+    else go(double{});
+    return 0;
+}
+
+}  // namespace
+
+int launch_stage_dense(hgg_handle *h, const StageIOT<double> &io) { return launch_dense_any<double>(h, io); }
+int launch_stage_dense(hgg_handle *h, const StageIOT<float> &io) { return launch_dense_any<float>(h, io); }
+int launch_stage_linear(hgg_handle *h, const StageIOT<double> &io) { return launch_linear<double>(h, io); }
+int launch_stage_linear(hgg_handle *h, const StageIOT<float> &io) { return launch_linear<float>(h, io); }
+
+}  // namespace hgg
