@@ -775,7 +775,7 @@ int hgg_batch_synchronize(hgg_batch *b) {
     int st = 0;
     HGG_BCUDA(b, cudaMemcpyAsync(&st, b->d_status, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
     HGG_BCUDA(b, cudaStreamSynchronize(b->stream));
-    if (st) return bfail(b, HGG_ERR_DEVICE, "kernel status word " + std::to_string(st) + " (bad neighbour index)");
+    if (st) return bfail(b, HGG_ERR_DEVICE, status_message(st));
     // keep each member handle's notion of its current buffer up to date
     for (int i = 0; i < b->cap; ++i)
         if (b->handles[i]) b->handles[i]->cur = b->parity_host[i] ? 1 - b->base[i] : b->base[i];

@@ -76,6 +76,13 @@ __global__ void from_tensor_order(const TS *src, double *dst, const int32_t *tpo
         dst[i] = tsign[k] * (double)src[device_index(e, tpos[k], nb, tiled)];
     }
 }
+// zeros the coefficients of the padding elements [n_elements, n_pad) of a device vector
+__global__ void zero_padding(double *v, int nb, int64_t n_elements, int64_t n_pad, bool tiled) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= (n_pad - n_elements) * nb) return;
+    const int64_t e = n_elements + i / nb;
+    v[device_index(e, (int)(i % nb), nb, tiled)] = 0.0;
+}
 // plain precision conversion of a vector (FP32-mixed stage vectors without layout change)
 __global__ void convert_vector(const double *src, float *dst, int64_t n) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
@@ -134,14 +141,21 @@ int enqueue_step(hgg_handle *h, int from, double dt) {
     return h->mixed ? enqueue_step_t<float>(h, from, dt) : enqueue_step_t<double>(h, from, dt);
 }
 
+std::string status_message(int st) {
+    std::string m = "kernel status word " + std::to_string(st) + ":";
+    if (st & 1) m += " bad neighbour index (bit 0);";
+    if (st & 2) m += " a bounded wait ran out (bit 1);";
+    if (st & 4) m += " bad matrix index (bit 2);";
+    if (st & ~7) m += " unknown bits;";
+    m.pop_back();
+    return m;
+}
+
 int check_status(hgg_handle *h) {
     int st = 0;
     HGG_CUDA(h, cudaMemcpyAsync(&st, h->d_status, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
     HGG_CUDA(h, cudaStreamSynchronize(h->stream));
-    if (st)
-        return fail(h, HGG_ERR_DEVICE,
-                    "kernel status word " + std::to_string(st) +
-                        " (bit 0: bad neighbour index, bit 1: a bounded wait ran out, bit 2: bad matrix index)");
+    if (st) return fail(h, HGG_ERR_DEVICE, status_message(st));
     return 0;
 }
 
@@ -627,6 +641,14 @@ int hgg_set_kernel_variant(hgg_handle *h, int32_t variant) {
     return 0;
 }
 
+int hgg_test_arm_without_copy(hgg_handle *h, int32_t polls) {
+    if (!h || polls < 1) return fail(h, HGG_ERR_INVALID, "polls must be positive");
+    if (h->linear || h->slice_ok || !h->op.tensor || h->variant != 2)
+        return fail(h, HGG_ERR_UNSUPPORTED, "only the pipelined kernel (kernel variant 2) waits on mbarriers");
+    h->test_arm_polls = (uint32_t)polls;
+    return 0;
+}
+
 // ---- right-hand side without allocation ---------------------------------------
 // The sum-factorised handles keep their vectors in tensor order on the device,
 // so a right-hand side of caller-owned vectors in hpGEM order needs two
@@ -680,9 +702,17 @@ int hgg_time_derivative_static(hgg_handle *h, const double *u, double *k) {
         base = g_static_ptr[dev];
     }
     double *su = base, *sk = base + h->N_alloc;
-    // the padding of the last tile is read (and ignored) by the stage kernel: keep it zero
-    if (h->N_alloc > h->N)
-        HGG_CUDA(h, cudaMemsetAsync(su + h->N, 0, sizeof(double) * (h->N_alloc - h->N), h->stream));
+    // The stage kernels read the padding elements of the last tile (they mask
+    // their results); clear them, wherever the layout puts them (tiled layout:
+    // interleaved with the tile's real elements), so that they read zeros
+    // rather than the previous call's values.
+    const int nbv = h->op.V * h->op.nB;
+    const int64_t n_pad = h->N_alloc / nbv;
+    if (n_pad > h->op.nE) {
+        zero_padding<<<(unsigned)(((n_pad - h->op.nE) * nbv + 255) / 256), 256, 0, h->stream>>>(
+            su, nbv, h->op.nE, n_pad, h->tiled);
+        h->launches++;
+    }
     to_tensor_order<double><<<4 * h->num_sms, 256, 0, h->stream>>>(u, su, h->d_tpos, h->d_tsign, h->op.nB, h->N,
                                                                     h->tiled);
     h->launches++;

@@ -83,6 +83,7 @@ struct hgg_handle {
     int64_t group_tiles = 0;
     int num_sms = 148;
     int *d_status = nullptr;
+    uint32_t test_arm_polls = 0;  // hgg_test_arm_without_copy: poll limit of the next pipelined launch
     bool store_last = true;
     int64_t launches = 0;
     // graph of one full step, per starting buffer, valid for (dt, store_last)
@@ -210,6 +211,9 @@ StageIOT<KT> make_stage_io(const hgg_handle *h, int from, double dt, int i, int 
     return io;
 }
 
+// the failures a device status word records (bit 0: bad neighbour index, bit 1:
+// a bounded wait ran out, bit 2: bad matrix index)
+std::string status_message(int st);
 // reads the device status word (synchronises the handle's stream)
 int check_status(hgg_handle *h);
 

@@ -532,9 +532,16 @@ StructuredProblem build_problem(Mesh mesh, int order, int physics, const double 
     if (!butcher_tableau(tableau, P.rk_a, P.rk_b, P.rk_c, P.n_stages))
         throw std::invalid_argument("unknown Butcher tableau " + tableau);
 
-    // element rule of order 2p+1 (Element.cpp:89-98), face rule of its actual order (Face.cpp:149-168)
+    // Element rule of order 2p+1 (Element::setDefaultBasisFunctionSet, Element.cpp:89-98).
+    // Face rule of order 2p+1 as well: the faces are created while the elements
+    // still hold the rule of their empty basis (Element.h:583, Face.cpp:149-168),
+    // and setQuadratureRulesWithOrder(2p+1) then gives every face of the element
+    // the face shape's rule for the requested order 2p+1, not for the element
+    // rule's actual order (Element.cpp:144-175).  The two differ for triangles at
+    // p = 1 (2 against 3 points) and p = 3 (4 against 5); only integrands that are
+    // not polynomials (source terms) see the difference.
     P.rule = get_rule(m.shape, 2 * order + 1);
-    P.face_rule = get_rule(si.face_shape, P.rule.order);
+    P.face_rule = get_rule(si.face_shape, 2 * order + 1);
     try {  // the reference has no rule of order 2p+2 for every shape (e.g. p = 5)
         P.error_rule = get_rule(m.shape, 2 * order + 2);
     } catch (const std::invalid_argument &) {

@@ -77,6 +77,15 @@ int launch_tensor(hgg_handle *h, const StageIO &io) {
     pa.geo = h->d_pgeo;
     pa.n_tiles = (op.nE + S::TE - 1) / S::TE;
     pa.nbuf = nbuf;
+    pa.polls = kWaitPolls;
+    pa.arm_only = -1;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (h->test_arm_polls && cudaStreamIsCapturing(h->stream, &cap) == cudaSuccess &&
+        cap == cudaStreamCaptureStatusNone) {  // hgg_test_arm_without_copy: this launch only
+        pa.polls = h->test_arm_polls;
+        pa.arm_only = 0;
+        h->test_arm_polls = 0;
+    }
     size_t smem = pipe_smem<P, DIM>(nbuf, pa.nv);
     cudaFuncSetAttribute(tensor_pipe<P, DIM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     int64_t grid = std::min<int64_t>(pa.n_tiles, (int64_t)h->num_sms * per_sm);

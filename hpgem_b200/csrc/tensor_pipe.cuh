@@ -17,7 +17,10 @@
 //   * results are staged in shared memory (hpGEM order) and written back with
 //     bulk asynchronous stores.
 // Every wait on an mbarrier is bounded; a wait that runs out sets bit 1 of the
-// status word and the block stops after draining its own stores.
+// status word and the block stops after draining its own copies: it waits
+// (bounded again) for every tile load it issued and not yet consumed, and for
+// its bulk stores, so that no asynchronous copy targets the block's shared
+// memory after it has exited.
 #pragma once
 
 #include <cstdint>
@@ -112,6 +115,9 @@ struct PipeArgs {
     int nbuf;                   // ring slots
     int nv;                     // vectors loaded per tile: u, kin[0..nin), kfin[0..nfin)
     uint32_t slot_bytes;
+    uint32_t polls;             // try_wait polls of one mbarrier before giving up (kWaitPolls)
+    int32_t arm_only;           // test of the bounded wait: this local tile's mbarrier is armed with
+                                // the slot's byte count but no copy is issued (-1: off)
 };
 
 template <int P, int DIM>
@@ -163,6 +169,7 @@ __global__ void __launch_bounds__(PipeShape<P, DIM>::THREADS)
         const int slot = (int)(j % pa.nbuf);
         unsigned char *dst = ring + (size_t)slot * pa.slot_bytes;
         ptx::mbar_arrive_expect_tx(&mbar[slot], pa.slot_bytes);
+        if (j == pa.arm_only) return;  // nothing in flight: the wait for this tile runs out
         for (int v = 0; v < pa.nv; ++v)
             ptx::bulk_load(dst + (size_t)v * TV, vec_ptr(v) + tile * TE * NB, TV, &mbar[slot]);
         ptx::bulk_load(dst + (size_t)pa.nv * TV, pa.geo + tile * S::TILE_GEO_BYTES, S::TILE_GEO_BYTES,
@@ -171,9 +178,17 @@ __global__ void __launch_bounds__(PipeShape<P, DIM>::THREADS)
     auto wait_slot = [&](int64_t j) -> bool {
         const int slot = (int)(j % pa.nbuf);
         const uint32_t parity = (uint32_t)((j / pa.nbuf) & 1);
-        for (uint32_t it = 0; it < kWaitPolls; ++it)
+        for (uint32_t it = 0; it < pa.polls; ++it)
             if (ptx::mbar_try_wait(&mbar[slot], parity)) return true;
         return false;
+    };
+    // after a wait ran out: thread 0 waits (bounded) for the loads of local tiles
+    // [first, last] that were issued and not consumed, then for its stores
+    auto drain = [&](int64_t first, int64_t last) {
+        if (tid != 0) return;
+        for (int64_t t = first; t <= last && t < my_tiles; ++t) wait_slot(t);
+        ptx::bulk_wait_all();
+        atomicOr(io.status, 2);
     };
     auto geo_of = [&](int64_t j, int e_local) -> const unsigned char * {
         return ring + (size_t)(j % pa.nbuf) * pa.slot_bytes + (size_t)pa.nv * TV + (size_t)e_local * S::GEO_BYTES;
@@ -228,7 +243,7 @@ __global__ void __launch_bounds__(PipeShape<P, DIM>::THREADS)
 
     bool ok = wait_slot(0);
     if (__syncthreads_or(!ok)) {
-        if (tid == 0) atomicOr(io.status, 2);
+        drain(0, (int64_t)pa.nbuf - 1);  // tiles 0 .. nbuf-1 were issued
         return;
     }
     gather(0);
@@ -284,7 +299,10 @@ __global__ void __launch_bounds__(PipeShape<P, DIM>::THREADS)
             if (ok) gather(j + 1);
         }
         if (tid == 0) ptx::bulk_wait_read_all();
-        if (__syncthreads_or(!ok)) break;
+        if (__syncthreads_or(!ok)) {
+            drain(j + 1, j - 1 + pa.nbuf);  // issued so far: tiles up to j - 1 + nbuf
+            return;
+        }
 
         // 3. x-pencil of this thread: volume + face lifts, output in hpGEM order
         {
@@ -349,7 +367,6 @@ __global__ void __launch_bounds__(PipeShape<P, DIM>::THREADS)
         }
     }
     if (tid == 0) ptx::bulk_wait_all();
-    if (!ok && tid == 0) atomicOr(io.status, 2);
 }
 
 }  // namespace hgg

@@ -72,7 +72,8 @@ typedef struct hgg_handle hgg_handle;
 
 /*
  * Everything hpGEM knows about one mesh that the time loop needs, taken
- * from its own objects (see INTEGRATION.md for the code that fills it):
+ * from its own objects (an hpGEM-side subclass fills it from the mesh's
+ * elements and faces, the quadrature rules and the Butcher tableau):
  *   - basis values and reference gradients at the element quadrature points
  *     (PhysicalElement::basisFunction / basisFunctionDeriv before the
  *     J^{-T} transform; GaussQuadratureRule::eval caches),
@@ -198,16 +199,20 @@ int hgg_set_kernel_variant(hgg_handle *h, int32_t variant);
  * allocation's implicit device synchronisation would stall co-scheduled
  * work).  The sum-factorised handles need two vectors of scratch; they come
  * from one file-scope device array of 2^22 doubles (32 MiB) that every GPU
- * using the library holds until the process exits, so the padded vector
- * (hgg_vector_length rounded up to whole 32-element tiles) may hold at most
- * 2^21 doubles, else HGG_ERR_UNSUPPORTED (32^3 hexahedra at p = 3 is the
- * largest cube mesh of that order).  The first call on a device looks the
- * array up (with the handle's device current, which every call requires);
- * make that first call before any stream capture.  All calls on a device
- * share the array and it keeps the last call's contents (the part that must
- * read as zero is cleared each call): calls that overlap on the GPU, from
- * different streams or handles, race.  Runs on the handle's stream and
- * returns after it (like hgg_time_derivative, whose result it reproduces). */
+ * using the library holds until the process exits, so one device vector may
+ * hold at most 2^21 doubles, else HGG_ERR_UNSUPPORTED.  A device vector is
+ * hgg_vector_length padded with the elements that complete the kernel's last
+ * tile (of 7 to 128 elements, by shape and order), which adds fewer than 2048
+ * doubles, so every problem with hgg_vector_length <= 2^21 - 2048 fits (32^3
+ * hexahedra at p = 3 is the largest cube mesh of that order).  The first call
+ * on a device looks the array up (with the handle's device current, which
+ * every call requires); make that first call before any stream capture.  All
+ * calls on a device share the array and it keeps the last call's contents:
+ * each call clears the padding elements of its input (the stage kernels read
+ * them and discard what they compute from them); calls that overlap on the
+ * GPU, from different streams or handles, race.  Runs on the handle's stream
+ * and returns after it (like hgg_time_derivative, whose result it
+ * reproduces). */
 int hgg_time_derivative_static(hgg_handle *h, const double *u, double *k);
 
 /* computeOneTimeStep(time, maximumRelativeError, dtMax)
@@ -235,6 +240,18 @@ int hgg_set_error_estimate(hgg_handle *h, const double *error_coefficients, int3
 
 /* Number of kernel launches the library issued on this handle so far. */
 int64_t hgg_launch_count(const hgg_handle *h);
+
+/* Test of the device-side failure path; no counterpart in the reference.  The
+ * next stage launch of the pipelined kernel (kernel variant 2 on a
+ * sum-factorised handle, outside stream capture) arms the mbarrier of every
+ * block's first tile with the tile's byte count but issues no copy, and gives
+ * up waiting on any mbarrier after `polls` polls: every block then waits
+ * (bounded) for the copies it did issue, sets bit 1 of the handle's status
+ * word and returns, so the call that launched it (hgg_time_derivative,
+ * hgg_synchronize) returns HGG_ERR_DEVICE while the CUDA context stays
+ * usable.  The status word stays set: the handle is then only destroyed.
+ * HGG_ERR_UNSUPPORTED on handles of other kernels. */
+int hgg_test_arm_without_copy(hgg_handle *h, int32_t polls);
 
 /* ---- stand-alone set-up: hpGEM's host side, restated ------------------- */
 

@@ -4,8 +4,8 @@
 quadrature points and hands it to oracle/dg_oracle.c:
 * element rule of order 2p+1 (Element::setDefaultBasisFunctionSet,
   kernel/Base/Element.cpp:89-98, orderCoeff_ = 2 in Element.h:575) and the face
-  rule of the element rule's actual order (Face::createQuadratureRules,
-  kernel/Base/Face.cpp:149-168);
+  rule of the same requested order 2p+1 (Element::setQuadratureRulesWithOrder
+  hands it to the element's faces, kernel/Base/Element.cpp:144-175);
 * basis values and reference gradients at the element points;
 * the element Jacobian of the vertex map (MappingToPhysSimplexLinear,
   MappingToPhysHypercubeLinear), constant on the affine elements of
@@ -135,7 +135,10 @@ class Problem:
         self.cinv = float(cinv)
         self.rule = get_rule(shape, 2 * p + 1)
         fshape = SHAPES[shape]["face_shape"]
-        self.face_rule = get_rule(fshape, self.rule.order)
+        # faces get the rule of the requested order 2p+1 when the element's rule is set
+        # (Element::setQuadratureRulesWithOrder, kernel/Base/Element.cpp:144-175; the
+        # faces were created under the empty basis's rule, Element.h:583, Face.cpp:149-168)
+        self.face_rule = get_rule(fshape, 2 * p + 1)
         self.phi, self.dphi = tabulate(shape, p, self.rule.points)
         self.nB = self.phi.shape[1]
         self.J = element_jacobians(shape, mesh.element_coords)

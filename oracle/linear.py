@@ -19,11 +19,22 @@ Restates kernel/Base/HpgemAPILinear_Impl.h:
   ``time_derivative`` multiplies the element matrix, then adds both sides of
   every face, then solves with the element's mass matrix;
 * the Runge-Kutta loop of HpgemAPISimplified::computeOneTimeStep
-  (HpgemAPISimplified_Impl.h:788-820), which HpgemAPILinear inherits.
+  (HpgemAPISimplified_Impl.h:788-820), which HpgemAPILinear inherits, with the
+  stage time t + c_i dt handed to the right-hand side;
+* the source terms of computeRightHandSide (:471-506): after the multiply,
+  addSourceTerm (:437-450) adds per element the integral of phi_i g_v(x, t)
+  (computeIntegrandSourceTermAtElement, :201-229, ElementIntegral: weights
+  times |J|) and addSourceTermAtBoundary (:452-469) adds, for every boundary
+  face to its left element, the integral of phi_i g_v(x, n, t) (the face
+  integrand of the application, FaceIntegral: weights times |n|), both before
+  the mass solve.  ``source_lifts`` restates the integration weights, and
+  g is the application's function: for 080AdvectionLinear_SelfTest.cpp:72-88
+  g = -u_exact(x, t) (a . n) on inflow faces (a . n < 0), 0 elsewhere.
 """
 import numpy as np
 
-from .dg import ADVECTION, TABLEAUX, WAVE
+from .dg import ADVECTION, TABLEAUX, WAVE, face_map_to_element
+from .refgeom import SHAPES, vertex_shape_functions
 
 
 def assemble(prob):
@@ -86,6 +97,38 @@ def assemble(prob):
     return mass, K, table[:, :2].astype(np.int64), faces
 
 
+def source_lifts(prob):
+    """Integration data of the two source terms of one mesh.
+
+    Returns a dict with, for the element source: ``elem_x`` [E][nQ][dim] (the
+    element rule's points) and ``elem_w`` [E][nQ][nB] (w_q |J_e| phi_i(q)); for
+    the boundary source: ``bface`` (boundary face ids), ``bleft`` (their left
+    elements), ``bface_x`` [Fb][nQf][dim], ``bface_n`` [Fb][dim] (unit normals)
+    and ``bface_w`` [Fb][nQf][nB] (w_q |n_f| phi_i(q) on the left side)."""
+    shape, d = prob.shape, prob.dim
+    coords = prob.mesh.element_coords
+    N = vertex_shape_functions(shape, prob.rule.points)
+    elem_x = np.einsum("qk,ekr->eqr", N, coords)
+    elem_w = np.einsum("q,e,qi->eqi", np.asarray(prob.rule.weights, dtype=float), prob.absdet, prob.phi)
+    table = prob.faces_c
+    bface = np.nonzero(table[:, 1] < 0)[0]
+    fl = SHAPES[shape]["faces"]
+    wf = np.asarray(prob.face_rule.weights, dtype=float)
+    bx, bn, bw = [], [], []
+    for f in bface:
+        L, fL = int(table[f, 0]), int(table[f, 2])
+        xi = face_map_to_element(shape, fl[fL], prob.face_rule.points)
+        bx.append(vertex_shape_functions(shape, xi) @ coords[L])
+        n = prob.normals[f]
+        area = float(np.sqrt(np.dot(n, n)))
+        bn.append(n / area)
+        bw.append(wf[:, None] * area * prob.phiF[fL])
+    z = np.zeros((0, len(wf), d))
+    return {"elem_x": elem_x, "elem_w": elem_w, "bface": bface, "bleft": table[bface, 0].astype(np.int64),
+            "bface_x": np.array(bx) if bx else z, "bface_n": np.array(bn).reshape(-1, d),
+            "bface_w": np.array(bw) if bw else np.zeros((0, len(wf), prob.nB))}
+
+
 class LinearOracle:
     """Stored matrices of one mesh; faces with right element -1 are boundary faces
     (only their (LEFT, LEFT) block is used, HpgemAPILinear_Impl.h:410-430)."""
@@ -96,8 +139,34 @@ class LinearOracle:
         self.fe = np.asarray(face_elements, dtype=np.int64).reshape(-1, 2)
         self.faces = np.asarray(faces, dtype=float)
         self.E, self.R = self.mass.shape[0], self.mass.shape[1]
+        self.lifts = None
+        self.element_source = None   # g(x [n][dim], t) -> [n][V]   (useSourceTerm)
+        self.boundary_source = None  # g(x [n][dim], unit normal [n][dim], t) -> [n][V]  (useSourceTermAtBoundary)
 
-    def time_derivative(self, u):
+    def set_sources(self, prob, element_source=None, boundary_source=None):
+        """HpgemAPILinear's useSourceTerm / useSourceTermAtBoundary with the integrand
+        phi_i g_v; ``prob`` is the oracle Problem the matrices were assembled from."""
+        self.lifts = source_lifts(prob)
+        self.element_source, self.boundary_source = element_source, boundary_source
+        return self
+
+    def _add_sources(self, r, t):
+        lf = self.lifts
+        if self.element_source is not None:  # addSourceTerm: every element
+            x = lf["elem_x"]
+            g = np.asarray(self.element_source(x.reshape(-1, x.shape[2]), t), dtype=float)
+            g = g.reshape(x.shape[0], x.shape[1], -1)
+            r += np.einsum("eqi,eqv->evi", lf["elem_w"], g).reshape(r.shape)
+        if self.boundary_source is not None and len(lf["bface"]):  # addSourceTermAtBoundary
+            x = lf["bface_x"]
+            n = np.repeat(lf["bface_n"][:, None, :], x.shape[1], axis=1)
+            g = np.asarray(self.boundary_source(x.reshape(-1, x.shape[2]), n.reshape(-1, x.shape[2]), t),
+                           dtype=float).reshape(x.shape[0], x.shape[1], -1)
+            add = np.einsum("fqi,fqv->fvi", lf["bface_w"], g).reshape(len(lf["bface"]), -1)
+            for f in range(len(lf["bface"])):  # face by face, as the reference adds them
+                r[lf["bleft"][f]] += add[f]
+
+    def time_derivative(self, u, t=0.0):
         u = np.asarray(u, dtype=float).reshape(self.E, self.R)
         r = np.einsum("eij,ej->ei", self.K, u)
         # both sides of every face (the reference adds them face by face; the sums
@@ -111,14 +180,18 @@ class LinearOracle:
         right = (np.einsum("fij,fj->fi", self.faces[inner, 2], u[L[inner]]) +
                  np.einsum("fij,fj->fi", self.faces[inner, 3], uR[inner]))
         np.add.at(r, Rt[inner], right)
+        if self.lifts is not None:
+            self._add_sources(r, t)
         k = np.linalg.solve(self.mass, r[..., None])[..., 0]   # LU with partial pivoting per element
         return k.reshape(-1)
 
-    def step(self, u, dt, nsteps, tableau="RK4_4"):
+    def step(self, u, dt, nsteps, tableau="RK4_4", t0=0.0):
         tab = TABLEAUX[tableau]
         A, b = np.asarray(tab["A"], dtype=float), np.asarray(tab["b"], dtype=float)
+        c = np.asarray(tab["c"], dtype=float)
         S = len(b)
         u = np.asarray(u, dtype=float).reshape(-1).copy()
+        t = t0
         for _ in range(nsteps):
             ks = []
             for i in range(S):
@@ -126,8 +199,9 @@ class LinearOracle:
                 for j in range(i):
                     if A[i][j] != 0.0:
                         w += dt * A[i][j] * ks[j]
-                ks.append(self.time_derivative(w))
+                ks.append(self.time_derivative(w, t + c[i] * dt))
             for j in range(S):
                 if b[j] != 0.0:
                     u += dt * b[j] * ks[j]
+            t += dt
         return u

@@ -21,6 +21,10 @@ need nothing but this repository.  What it extracts, and from where:
   reference shape, as an if/else chain on the basis-function index.
 * ``advection_goldens.json``: the L2-error tables of
   ``tests/self/Basic/090Advection_SelfTest.cpp:303-337``.
+* ``advection_linear_goldens.json``: the L2-error tables of the stored-matrix
+  self-test ``tests/self/Basic/080AdvectionLinear_SelfTest.cpp:255-297``
+  (non-periodic meshes, inflow boundary through the boundary source term), with
+  the mesh file names of ``tests/self/TestMeshes.h`` behind each table.
 * ``mesh_files/*.hpgem``: three of those Preprocessor outputs as they are
   (the fully periodic 1D line, 2D triangle and 3D cube meshes), for the tests
   of the library's "mesh 2" reader; their structured descriptions are in
@@ -110,6 +114,10 @@ MESHES = [
     ("unitCubeN2Tet", "unitCubeN2Tet.hpgem", "unitCubeN2Tet.hpgem"),
     ("3Dtriangular1", "3Dtriangular1mesh.hpgem", "3Dtriangular1source.hpgem"),
     ("3Dtriangular2", "3Dtriangular2mesh.hpgem", "3Dtriangular2source.hpgem"),
+    # non-periodic meshes of the stored-matrix self-test (080AdvectionLinear_SelfTest)
+    ("unitLineN4", "unitLineN4.hpgem", "unitLineN4.hpgem"),
+    ("unitSquareTrianglesN2", "unitSquareTrianglesN2.hpgem", "unitSquareTrianglesN2.hpgem"),
+    ("unitCubeN4", "unitCubeN4.hpgem", "unitCubeN4.hpgem"),
 ]
 
 
@@ -254,13 +262,38 @@ def extract_advection_goldens(ref):
     return out
 
 
+def extract_linear_advection_goldens(ref):
+    """The L2-error tables of 080AdvectionLinear_SelfTest.cpp:255-297 with their
+    mesh lists (TestMeshes.h) and parameters (p, end time, time steps)."""
+    text = open(os.path.join(ref, "tests", "self", "Basic",
+                             "080AdvectionLinear_SelfTest.cpp")).read()
+    out = {}
+    for key in ("dim1", "dim2P1", "dim2P2", "dim3"):
+        m = re.search(key + r"Meshes\s*=\s*\{(\w+)\(([^)]*)\),\s*\{(.*?)\}\}", text, re.S)
+        vals = [float(v) for v in re.findall(r"([0-9.]+e[-+]\d+)", m.group(3))]
+        levels = [int(t) for t in m.group(2).split(",")] if m.group(2).strip() else []
+        out[key] = {"mesh_list": m.group(1), "levels": levels, "errors": vals}
+        m = re.search(r"AdvectionParameters\s+" + key + r"Params\s*=\s*\{([^}]*)\}", text)
+        p, t_end, steps = [t.strip() for t in m.group(1).split(",")]
+        out[key].update({"p": int(p), "end_time": float(t_end), "time_steps": int(steps)})
+    # the file names behind each mesh list, in level order
+    meshes = open(os.path.join(ref, "tests", "self", "TestMeshes.h")).read()
+    for blob in out.values():
+        m = re.search(r"std::vector<std::string> " + blob["mesh_list"] + r"\(.*?limit\((.*?)minLevel", meshes, re.S)
+        blob["files"] = re.findall(r'"(\w+)\.hpgem"', m.group(1))
+    return out
+
+
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <hpgem source tree>")
+    ref = sys.argv[1]
     blobs = {
         "meshes.json": extract_meshes(ref),
         "simplex_rules.json": extract_rules(ref),
         "quadrature_integrals.json": extract_integrals(ref),
         "advection_goldens.json": extract_advection_goldens(ref),
+        "advection_linear_goldens.json": extract_linear_advection_goldens(ref),
     }
     for name, blob in blobs.items():
         with open(os.path.join(HERE, name), "w") as f:
