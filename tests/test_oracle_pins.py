@@ -7,7 +7,12 @@
   at their 1e-12 tolerance;
 * the whole time-stepping pipeline: the L2-error goldens of
   tests/self/Basic/090Advection_SelfTest.cpp:303-337 (Dormand-Prince, p = 1,
-  periodic 1D lines, 2D triangles, 3D cubes), at that test's 1 % tolerance.
+  periodic 1D lines, 2D triangles, 3D cubes), at that test's 1 % tolerance;
+* the stored-matrix pipeline with its boundary source term: the four L2-error
+  tables of tests/self/Basic/080AdvectionLinear_SelfTest.cpp:255-297
+  (HpgemAPILinear, Dormand-Prince, non-periodic meshes whose inflow boundary
+  enters through addSourceTermAtBoundary; p = 1 lines, triangles and cubes,
+  p = 2 triangles), at that test's 1 % tolerance and to every printed digit.
 """
 import json
 import math
@@ -18,6 +23,7 @@ import pytest
 
 from oracle.basis import tabulate
 from oracle.dg import ADVECTION, Problem
+from oracle.linear import LinearOracle, assemble
 from oracle.mesh import structured_mesh
 from oracle.quadrature import _tensor_rule, rule_by_name
 
@@ -107,3 +113,50 @@ def test_advection_selftest_goldens(dim, level):
     gold = par["errors"][level]
     assert abs(err - gold) < 0.01 * gold  # ConvergenceTest.h:113-122
     assert abs(err - gold) < 1e-7 * gold  # and in fact to every printed digit
+
+
+def _linear_cases():
+    g = _load("advection_linear_goldens.json")
+    for key in ("dim1", "dim2P1", "dim2P2", "dim3"):
+        for level in range(len(g[key]["errors"])):
+            yield key, level
+
+
+def linear_advection_run(key, level, solver):
+    """080AdvectionLinear_SelfTest's set-up (080:58-103, 108-168, 255-297): a_i = 0.1 + 0.1 i,
+    u0 = prod sin(2 pi x_i) projected, inflow boundary value through the boundary source term
+    g = -u_exact(x, t) (a . n) where a . n < 0, Dormand-Prince, nT steps to T; returns
+    (L2 error at T, golden).  ``solver(mesh, prob, a, g, u0, dt, nT)`` runs the steps."""
+    par = _load("advection_linear_goldens.json")[key]
+    D = {"dim1": 1, "dim2P1": 2, "dim2P2": 2, "dim3": 3}[key]
+    name = par["files"][par["levels"][0] + level]   # e.g. unitSquareTrianglesN8
+    N = int(name.rsplit("N", 1)[1])
+    a = np.array([0.1 + 0.1 * i for i in range(D)])
+    mesh = structured_mesh([N] * D, [0.0] * D, [1.0] * D, "Triangles" in name, [False] * D)
+    prob = Problem(mesh, par["p"], ADVECTION, a=a)
+
+    def exact(x, t):
+        return np.prod(np.sin(2 * np.pi * (x - a * t)), axis=1)[:, None]
+
+    def inflow(x, n, t):
+        flow = n @ a
+        return np.where(flow < 0, -exact(x, t)[:, 0] * flow, 0.0)[:, None]
+
+    u0 = prob.project(lambda x: exact(x, 0.0)).reshape(-1)
+    T, nT = par["end_time"], par["time_steps"]
+    u = solver(mesh, prob, a, inflow, u0, T / nT, nT)
+    return prob.l2_error(u, exact, T), par["errors"][level]
+
+
+def _oracle_solver(mesh, prob, a, inflow, u0, dt, nT):
+    lin = LinearOracle(*assemble(prob)).set_sources(prob, boundary_source=inflow)
+    return lin.step(u0, dt, nT, "DormandPrince")
+
+
+@pytest.mark.parametrize("key,level", list(_linear_cases()))
+def test_linear_advection_selftest_goldens(key, level):
+    if key == "dim3" and level == 2:
+        pytest.skip("16^3 level takes a few seconds; the GPU test runs it")
+    err, gold = linear_advection_run(key, level, _oracle_solver)
+    assert abs(err - gold) < 0.01 * gold  # ConvergenceTest.h:113-122
+    assert abs(err - gold) < 1e-8 * gold  # and to every printed digit
