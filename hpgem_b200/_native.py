@@ -21,7 +21,8 @@ ERRORS = {0: "HGG_OK", -1: "HGG_ERR_INVALID", -2: "HGG_ERR_UNSUPPORTED", -3: "HG
 EXPORTED = ["hgg_create", "hgg_destroy", "hgg_last_error", "hgg_set_state", "hgg_get_state",
             "hgg_step", "hgg_time_derivative", "hgg_synchronize", "hgg_vector_length",
             "hgg_kernel_kind", "hgg_set_store_last_stage", "hgg_set_stream", "hgg_set_kernel_variant", "hgg_launch_count",
-            "hgg_test_arm_without_copy",
+            "hgg_test_arm_without_copy", "hgg_set_element_source", "hgg_set_boundary_source",
+            "hgg_time_derivative_at",
             "hgg_create_structured", "hgg_structured_descriptor", "hgg_free_descriptor",
             "hgg_create_mesh_file", "hgg_mesh_file_descriptor",
             "hgg_create_linear", "hgg_linear_descriptor", "hgg_free_linear_descriptor",
@@ -36,6 +37,11 @@ EXPORTED = ["hgg_create", "hgg_destroy", "hgg_last_error", "hgg_set_state", "hgg
             "hgg_server_release", "hgg_server_times", "hgg_server_stats", "hgg_server_timing",
             "hgg_server_last_error",
             "hgg_server_stop"]
+
+# void (*hgg_source_fn)(const double *xyz, const double *normals, int64_t n_points, int32_t dim,
+#                       double time, double *values, void *user)
+SOURCE_FN = ctypes.CFUNCTYPE(None, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double), ctypes.c_int64,
+                             ctypes.c_int32, ctypes.c_double, ctypes.POINTER(ctypes.c_double), ctypes.c_void_p)
 
 # void (*hgg_initial_fn)(const double *xyz, int64_t n_points, int32_t dim, double *values, void *user)
 INITIAL_FN = ctypes.CFUNCTYPE(None, ctypes.POINTER(ctypes.c_double), ctypes.c_int64, ctypes.c_int32,
@@ -104,6 +110,9 @@ def load():
         "hgg_time_derivative": (ctypes.c_int, [H, ctypes.c_int32, ctypes.c_int32]),
         "hgg_time_derivative_static": (ctypes.c_int, [H, ctypes.c_void_p, ctypes.c_void_p]),
         "hgg_test_arm_without_copy": (ctypes.c_int, [H, ctypes.c_int32]),
+        "hgg_set_element_source": (ctypes.c_int, [H, ctypes.c_void_p, ctypes.c_void_p]),
+        "hgg_set_boundary_source": (ctypes.c_int, [H, ctypes.c_void_p, ctypes.c_void_p]),
+        "hgg_time_derivative_at": (ctypes.c_int, [H, ctypes.c_int32, ctypes.c_int32, ctypes.c_double]),
         "hgg_step_adaptive": (ctypes.c_int, [H, ctypes.POINTER(ctypes.c_double), ctypes.c_double, ctypes.c_double,
                                              ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double),
                                              ctypes.POINTER(ctypes.c_int32)]),

@@ -21,7 +21,8 @@ LIB = os.path.join(LIB_DIR, "libhpgem_b200.so")
 SOURCES = sorted(glob.glob(os.path.join(CSRC, "*.cu"))) + [
     os.path.join(CSRC, "host", "setup.cpp"),
     os.path.join(CSRC, "host", "operators.cpp"),
-    os.path.join(CSRC, "host", "linear.cpp")]
+    os.path.join(CSRC, "host", "linear.cpp"),
+    os.path.join(CSRC, "host", "sources.cpp")]
 HEADERS = sorted(glob.glob(os.path.join(CSRC, "*.cuh"))) + sorted(glob.glob(os.path.join(CSRC, "host", "*.h"))) + [
     os.path.join(CSRC, "host", "simplex_rules.inc"),
     os.path.join(os.path.dirname(HERE), "include", "hpgem_b200.h")]

@@ -686,6 +686,7 @@ int hgg_batch_add(hgg_batch *b, hgg_handle *h, double dt, int32_t nsteps, int32_
         if (free_slot < 0 && !b->handles[i]) free_slot = i;
     }
     if (free_slot < 0) return bfail(b, HGG_ERR_INVALID, "batch is full");
+    if (h->src) return bfail(b, HGG_ERR_UNSUPPORTED, "handles with source terms are stepped on their own");
     if (h->linear && h->lin_tiles == 0)
         return bfail(b, HGG_ERR_UNSUPPORTED, "stored-matrix handles without tiles are stepped on their own");
     if (!h->slice_ok && !h->op.tensor && dense_R(h) > 256)

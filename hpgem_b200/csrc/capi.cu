@@ -8,6 +8,7 @@
 #include <cstring>
 #include <fstream>
 #include <limits>
+#include <map>
 #include <sstream>
 #include <memory>
 #include <mutex>
@@ -131,7 +132,9 @@ bool vector_is_float(const hgg_handle *h, int vec) { return h->mixed && vec >= 1
 template <typename KT>
 int enqueue_step_t(hgg_handle *h, int from, double dt) {
     for (int i = 0; i < h->S; ++i) {
-        int rc = launch_stage(h, make_stage_io<KT>(h, from, dt, i, h->d_status));
+        const StageIOT<KT> io = make_stage_io<KT>(h, from, dt, i, h->d_status);
+        int rc = launch_stage(h, io);
+        if (!rc && h->src) rc = enqueue_source(h, from, i, io.kout, io.unew, io.blast);
         if (rc) return rc;
     }
     return 0;
@@ -203,7 +206,7 @@ int attach_linear(hgg_handle *h, const LinearSystem &sys, bool tiles_only = fals
 // vectors stay in hpGEM order and the matrix-free operators are not uploaded
 int create_from_desc(const hgg_problem_desc *desc, hgg_handle *h, bool linear = false) {
     try {
-        h->op = build_operators(*desc);
+        h->op = build_operators(*desc, !linear);
     } catch (const std::exception &ex) {
         return fail(h, HGG_ERR_INVALID, ex.what());
     }
@@ -458,6 +461,7 @@ int attach_linear(hgg_handle *h, const LinearSystem &sys, bool tiles_only) {
 void destroy_handle(hgg_handle *h) {
     if (!h) return;
     release_graphs(h);
+    destroy_sources(h);
     if (h->stream) cudaStreamSynchronize(h->stream);
     if (h->own_stream) cudaStreamSynchronize(h->own_stream);
     for (auto &b : h->bufs) cudaFree(b.p);
@@ -565,7 +569,12 @@ int hgg_step(hgg_handle *h, double *time, double dt, int32_t nsteps) {
         h->graph_dt = dt;
         h->graph_store_last = h->store_last;
     }
+    if (h->src && !time) return fail(h, HGG_ERR_INVALID, "source terms need the time: pass a time");
     for (int s = 0; s < nsteps; ++s) {
+        if (h->src) {  // the source values of this step's stage times
+            int rc = fill_sources(h, h->cur, *time, dt);
+            if (rc) return rc;
+        }
         HGG_CUDA(h, cudaGraphLaunch(h->graph[h->cur], h->stream));
         h->launches += h->S;
         h->cur = 1 - h->cur;
@@ -575,10 +584,19 @@ int hgg_step(hgg_handle *h, double *time, double dt, int32_t nsteps) {
 }
 
 int hgg_time_derivative(hgg_handle *h, int32_t in_vec, int32_t out_vec) {
+    return time_derivative_impl(h, in_vec, out_vec, nullptr);
+}
+
+}  // extern "C"
+
+int hgg::time_derivative_impl(hgg_handle *h, int32_t in_vec, int32_t out_vec, const double *time) {
     if (!h) return fail(h, HGG_ERR_INVALID, "null handle");
     void *in = vector_ptr(h, in_vec), *outp = vector_ptr(h, out_vec);
     if (!in || !outp || in == outp) return fail(h, HGG_ERR_INVALID, "bad vector ids");
+    if (h->src && !time)
+        return fail(h, HGG_ERR_INVALID, "the handle has source terms: use hgg_time_derivative_at with a time");
     int rc;
+    if (h->src && (rc = fill_source_values(h, 2, time, 1))) return rc;
     if (h->mixed) {
         // FP32-mixed form: FP64 input (the solution), FP32 stage vector output
         if (vector_is_float(h, in_vec) || !vector_is_float(h, out_vec))
@@ -589,6 +607,7 @@ int hgg_time_derivative(hgg_handle *h, int32_t in_vec, int32_t out_vec) {
         io.n_elements = h->op.nE;
         io.status = h->d_status;
         rc = launch_stage(h, io);
+        if (!rc && h->src) rc = enqueue_source(h, 2, 0, io.kout, nullptr, 0.0);
     } else {
         StageIO io{};
         io.u = static_cast<const double *>(in);
@@ -596,10 +615,13 @@ int hgg_time_derivative(hgg_handle *h, int32_t in_vec, int32_t out_vec) {
         io.n_elements = h->op.nE;
         io.status = h->d_status;
         rc = launch_stage(h, io);
+        if (!rc && h->src) rc = enqueue_source(h, 2, 0, io.kout, nullptr, 0.0);
     }
     if (rc) return rc;
     return check_status(h);
 }
+
+extern "C" {
 
 int hgg_synchronize(hgg_handle *h) {
     if (!h) return fail(h, HGG_ERR_INVALID, "null handle");
@@ -672,6 +694,7 @@ int hgg_time_derivative_static(hgg_handle *h, const double *u, double *k) {
     HGG_CUDA(h, cudaGetDevice(&dev));
     if (dev != h->device) return fail(h, HGG_ERR_INVALID, "call with the handle's device current");
     if (h->mixed) return fail(h, HGG_ERR_UNSUPPORTED, "the FP32-mixed form has no static-scratch right-hand side");
+    if (h->src) return fail(h, HGG_ERR_UNSUPPORTED, "source terms need a time: use hgg_time_derivative_at");
     StageIO io{};
     io.n_elements = h->op.nE;
     io.status = h->d_status;
@@ -860,7 +883,8 @@ int hgg_step_adaptive(hgg_handle *h, double *time, double max_relative_error, do
     int rc = 0;
     while (max_relative_error * norm < error || std::isinf(error)) {
         const int from = h->cur;
-        rc = enqueue_step(h, from, dt);
+        if (h->src) rc = fill_sources(h, from, *time, dt);
+        if (!rc) rc = enqueue_step(h, from, dt);
         if (rc) break;
         h->cur = 1 - from;
         rc = error_and_norm(h, dt, &error, &norm);
@@ -955,13 +979,13 @@ void hgg_free_descriptor(void *owner) { delete static_cast<StructuredProblem *>(
 namespace {
 // the problem of a mesh file (text read here, parsed by read_mesh2)
 int mesh_file_problem(const char *path, int32_t order, int32_t physics, const double *params, const char *tableau,
-                      StructuredProblem &P) {
+                      StructuredProblem &P, bool boundary_faces = false) {
     std::ifstream in(path, std::ios::binary);
     if (!in) return fail(nullptr, HGG_ERR_INVALID, std::string("cannot open mesh file ") + path);
     std::stringstream text;
     text << in.rdbuf();
     try {
-        P = build_problem(read_mesh2(text.str()), order, physics, params, tableau);
+        P = build_problem(read_mesh2(text.str()), order, physics, params, tableau, boundary_faces);
     } catch (const std::exception &ex) {
         return fail(nullptr, HGG_ERR_INVALID, ex.what());
     }
@@ -1035,11 +1059,12 @@ int linear_structured_system(const char *description, int32_t order, int32_t phy
         return fail(nullptr, HGG_ERR_UNSUPPORTED,
                     "the stored-matrix form has the reference's linear advection and central-flux wave");
     if (mesh_file) {
-        int rc = mesh_file_problem(mesh_file, order, physics, params, tableau, P);
+        int rc = mesh_file_problem(mesh_file, order, physics, params, tableau, P, true);
         if (rc) return rc;
     }
     try {
-        if (!mesh_file) P = build_structured(description, order, physics, params, tableau);
+        // the stored-matrix path takes meshes with boundary faces (non-periodic directions)
+        if (!mesh_file) P = build_structured(description, order, physics, params, tableau, true);
         hgg_problem_desc d;
         fill_descriptor(P, HGG_PRECISION_FP64, d);
         sys = assemble_linear(d);
@@ -1156,6 +1181,22 @@ int create_linear_from(const char *description, const char *mesh_file, int32_t o
         destroy_handle(h);
         return rc;
     }
+    // the distinct mass matrices, for the source terms' lifts
+    {
+        std::map<int32_t, int32_t> compact;
+        const size_t RR = (size_t)sys.R * sys.R;
+        h->lin_mass_of.resize(sys.E);
+        for (int64_t e = 0; e < sys.E; ++e) {
+            auto it = compact.find(sys.mass_id[e]);
+            if (it == compact.end()) {
+                it = compact.emplace(sys.mass_id[e], (int32_t)compact.size()).first;
+                const double *m = sys.pool.get(sys.mass_id[e]);
+                h->lin_mass.insert(h->lin_mass.end(), m, m + RR);
+            }
+            h->lin_mass_of[e] = it->second;
+        }
+    }
+    h->linear_api = true;
     h->sp = std::move(sp);
     butcher_error_estimate(tableau, h->rk_err, h->rk_order);
     *out = h;

@@ -20,6 +20,7 @@
 #include "host/setup.h"
 
 namespace hgg {
+struct SourceState;  // sources.cu
 struct DevBuf {
     void *p = nullptr;
     size_t bytes = 0;
@@ -84,6 +85,11 @@ struct hgg_handle {
     int num_sms = 148;
     int *d_status = nullptr;
     uint32_t test_arm_polls = 0;  // hgg_test_arm_without_copy: poll limit of the next pipelined launch
+    // HpgemAPILinear source terms (sources.cu)
+    bool linear_api = false;            // HpgemAPILinear built from a structured mesh or a mesh file
+    std::vector<double> lin_mass;       // its distinct element mass matrices [n][R][R]
+    std::vector<int32_t> lin_mass_of;   // [E]
+    hgg::SourceState *src = nullptr;    // set: every stage adds the caller's source terms
     bool store_last = true;
     int64_t launches = 0;
     // graph of one full step, per starting buffer, valid for (dt, store_last)
@@ -210,6 +216,18 @@ StageIOT<KT> make_stage_io(const hgg_handle *h, int from, double dt, int i, int 
     }
     return io;
 }
+
+// source terms (sources.cu): the caller's functions evaluated at the stage times
+// t + c_i dt of one step (buf 0 / 1: the step from sol[0] / sol[1]) or at
+// `times` (buf 2) and copied to the device; the lift of stage `stage` added to
+// kout (and blast times it to unew) after the stage kernel
+int fill_sources(hgg_handle *h, int buf, double t, double dt);
+int fill_source_values(hgg_handle *h, int buf, const double *times, int n);
+int enqueue_source(hgg_handle *h, int buf, int stage, double *kout, double *unew, double blast);
+int enqueue_source(hgg_handle *h, int buf, int stage, float *kout, double *unew, double blast);
+void destroy_sources(hgg_handle *h);
+// hgg_time_derivative (time null) and hgg_time_derivative_at
+int time_derivative_impl(hgg_handle *h, int32_t in_vec, int32_t out_vec, const double *time);
 
 // the failures a device status word records (bit 0: bad neighbour index, bit 1:
 // a bounded wait ran out, bit 2: bad matrix index)

@@ -204,12 +204,16 @@ LinearSystem assemble_linear(const hgg_problem_desc &desc) {
     std::map<std::string, int64_t> by_face;
     for (int64_t f = 0; f < s.F; ++f) {
         const int64_t L = desc.face_elements[2 * f], Rt = desc.face_elements[2 * f + 1];
-        if (L < 0 || L >= s.E || Rt < 0 || Rt >= s.E) throw std::invalid_argument("bad face table");
-        const int tab[2] = {desc.face_tab_index[2 * f], desc.face_tab_index[2 * f + 1]};
+        if (L < 0 || L >= s.E || Rt < -1 || Rt >= s.E) throw std::invalid_argument("bad face table");
+        // a boundary face (right element -1) has only its (LEFT, LEFT) block
+        // (FaceMatrix of one side; Face::isInternal() false)
+        const bool boundary = Rt < 0;
+        const int tab[3] = {desc.face_tab_index[2 * f], boundary ? desc.face_tab_index[2 * f] : desc.face_tab_index[2 * f + 1],
+                            boundary ? 1 : 0};
         if (tab[0] < 0 || tab[1] < 0 || tab[0] >= desc.n_face_tabs || tab[1] >= desc.n_face_tabs)
             throw std::invalid_argument("bad face tabulation index");
         const double *n = desc.face_normals + f * d;
-        std::string fkey = geometry_key(n, d, tab, 2);
+        std::string fkey = geometry_key(n, d, tab, 3);
         auto known = by_face.find(fkey);
         if (known != by_face.end()) {
             for (int b = 0; b < 4; ++b) s.face_id[4 * f + b] = s.face_id[4 * known->second + b];
@@ -230,8 +234,8 @@ LinearSystem assemble_linear(const hgg_problem_desc &desc) {
                 double A = 0.0;
                 for (int c = 0; c < d; ++c) A += a[c] * (n[c] / area);
                 const double wq = desc.face_weights[q] * area;
-                for (int ts = 0; ts < 2; ++ts)
-                    for (int tr = 0; tr < 2; ++tr) {
+                for (int ts = 0; ts < (boundary ? 1 : 2); ++ts)
+                    for (int tr = 0; tr < (boundary ? 1 : 2); ++tr) {
                         double factor = 0.0;
                         if (A > 1e-12) factor = tr == 0 ? 1.0 : 0.0;
                         else if (A < -1e-12) factor = tr == 1 ? 1.0 : 0.0;
@@ -247,14 +251,18 @@ LinearSystem assemble_linear(const hgg_problem_desc &desc) {
                 // normal out of the left element, negated for a right-side basis function;
                 // the normal carries the face scale (no |n| factor)
                 const double wq = desc.face_weights[q];
-                for (int ts = 0; ts < 2; ++ts)
-                    for (int tr = 0; tr < 2; ++tr) {
+                for (int ts = 0; ts < (boundary ? 1 : 2); ++ts)
+                    for (int tr = 0; tr < (boundary ? 1 : 2); ++tr) {
                         const double sgn = tr == 1 ? -1.0 : 1.0;
                         double *blk = B.data() + (2 * ts + tr) * RR;
                         for (int j = 0; j < nB; ++j)
                             for (int i = 0; i < nB; ++i) {
                                 const double pp = wq * ph[tr][j] * ph[ts][i];
                                 for (int c = 0; c < d; ++c) {
+                                    if (boundary) {  // :254-258 and :271-272: -n_d in (p, s_d), 0 in (s_d, p)
+                                        blk[(size_t)i * R + (c + 1) * nB + j] += -n[c] * pp;
+                                        continue;
+                                    }
                                     const double t = -0.5 * sgn * n[c] * pp;
                                     blk[(size_t)i * R + (c + 1) * nB + j] += t;
                                     blk[(size_t)((c + 1) * nB + i) * R + j] += t;
@@ -263,7 +271,7 @@ LinearSystem assemble_linear(const hgg_problem_desc &desc) {
                     }
             }
         }
-        for (int b = 0; b < 4; ++b) s.face_id[4 * f + b] = s.pool.add(B.data() + b * RR);
+        for (int b = 0; b < (boundary ? 1 : 4); ++b) s.face_id[4 * f + b] = s.pool.add(B.data() + b * RR);
     }
     return s;
 }

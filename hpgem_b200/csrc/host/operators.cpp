@@ -270,7 +270,7 @@ bool try_tensor(const hgg_problem_desc &desc, HostOperators &op) {
 
 }  // namespace
 
-HostOperators build_operators(const hgg_problem_desc &desc) {
+HostOperators build_operators(const hgg_problem_desc &desc, bool faces) {
     HostOperators op;
     const int d = desc.dim;
     if (d < 1 || d > 3) throw std::invalid_argument("dim must be 1, 2 or 3");
@@ -349,6 +349,11 @@ HostOperators build_operators(const hgg_problem_desc &desc) {
             for (int r = 0; r < d; ++r)
                 for (int c = 0; c < d; ++c) op.elem_geo[(e * d + r) * d + c] = Ji[c * d + r];
         }
+    }
+
+    if (!faces) {
+        op.tensor = false;
+        return op;
     }
 
     // face operators per (test tabulation, trial tabulation) pair

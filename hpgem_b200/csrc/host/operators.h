@@ -61,7 +61,9 @@ struct HostOperators {
 };
 
 // Throws std::invalid_argument / std::runtime_error with a message on bad input.
-HostOperators build_operators(const hgg_problem_desc &desc);
+// faces = false: element data only (the stored-matrix path applies its own face
+// matrices and takes meshes with boundary faces)
+HostOperators build_operators(const hgg_problem_desc &desc, bool faces = true);
 
 // small dense helpers
 void invert_matrix(int n, const double *A, double *Ainv);

@@ -508,11 +508,13 @@ bool butcher_error_estimate(const std::string &name, std::vector<double> &error,
 // descriptor contents for a structured mesh
 // ---------------------------------------------------------------------------
 StructuredProblem build_structured(const std::string &description, int order, int physics,
-                                   const double *params, const std::string &tableau) {
-    return build_problem(structured_mesh(parse_structured(description)), order, physics, params, tableau);
+                                   const double *params, const std::string &tableau, bool boundary_faces) {
+    return build_problem(structured_mesh(parse_structured(description)), order, physics, params, tableau,
+                         boundary_faces);
 }
 
-StructuredProblem build_problem(Mesh mesh, int order, int physics, const double *params, const std::string &tableau) {
+StructuredProblem build_problem(Mesh mesh, int order, int physics, const double *params, const std::string &tableau,
+                                bool boundary_faces) {
     StructuredProblem P;
     P.mesh = std::move(mesh);
     const Mesh &m = P.mesh;
@@ -526,7 +528,7 @@ StructuredProblem build_problem(Mesh mesh, int order, int physics, const double 
     } else {
         P.c_inv = params ? params[0] : 1.0;
     }
-    for (int64_t f = 0; f < m.n_faces(); ++f)
+    for (int64_t f = 0; f < m.n_faces() && !boundary_faces; ++f)
         if (m.face_elements[2 * f + 1] < 0)
             throw std::invalid_argument("boundary faces are not supported: use a fully periodic mesh");
     if (!butcher_tableau(tableau, P.rk_a, P.rk_b, P.rk_c, P.n_stages))
@@ -614,8 +616,12 @@ StructuredProblem build_problem(Mesh mesh, int order, int physics, const double 
         int fL = m.face_local[2 * f], fR = m.face_local[2 * f + 1];
         for (int k = 0; k < fv; ++k) verts[k] = si.faces[fL][k];
         P.face_tab_index[2 * f] = tab_of(verts);
-        for (int k = 0; k < fv; ++k) verts[k] = si.faces[fR][m.face_perm[f * fv + k]];
-        P.face_tab_index[2 * f + 1] = tab_of(verts);
+        if (m.face_elements[2 * f + 1] >= 0) {
+            for (int k = 0; k < fv; ++k) verts[k] = si.faces[fR][m.face_perm[f * fv + k]];
+            P.face_tab_index[2 * f + 1] = tab_of(verts);
+        } else {  // boundary face: no right side; its index repeats the left one
+            P.face_tab_index[2 * f + 1] = P.face_tab_index[2 * f];
+        }
 
         // normal (FaceGeometry::getNormalVector): tangents J * d(face map), wedge, outward
         const double *J = &P.jacobians[L * d * d];

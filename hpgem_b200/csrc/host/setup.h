@@ -83,9 +83,12 @@ struct StructuredProblem {
     int n_stages = 0;
 };
 
+// boundary_faces: the mesh may have faces with one element (right element -1),
+// as the stored-matrix path takes; otherwise every face must have two.
 StructuredProblem build_structured(const std::string &description, int order, int physics,
-                                   const double *params, const std::string &tableau);
-StructuredProblem build_problem(Mesh mesh, int order, int physics, const double *params, const std::string &tableau);
+                                   const double *params, const std::string &tableau, bool boundary_faces = false);
+StructuredProblem build_problem(Mesh mesh, int order, int physics, const double *params, const std::string &tableau,
+                                bool boundary_faces = false);
 
 bool butcher_tableau(const std::string &name, std::vector<double> &a, std::vector<double> &b,
                      std::vector<double> &c, int &stages);

@@ -162,8 +162,35 @@ class Handle:
         e = np.ascontiguousarray(np.asarray(error_coefficients, dtype=np.float64))
         self._check(self._lib.hgg_set_error_estimate(self._raw, _ptr(e), int(order)))
 
-    def time_derivative(self, in_vec, out_vec):
-        self._check(self._lib.hgg_time_derivative(self._raw, int(in_vec), int(out_vec)))
+    def time_derivative(self, in_vec, out_vec, time=None):
+        if time is None:
+            self._check(self._lib.hgg_time_derivative(self._raw, int(in_vec), int(out_vec)))
+        else:
+            self._check(self._lib.hgg_time_derivative_at(self._raw, int(in_vec), int(out_vec), float(time)))
+
+    def set_source(self, boundary, fn, n_vars):
+        """hgg_set_boundary_source / hgg_set_element_source with a Python function:
+        boundary: fn(x [n, dim], unit normals [n, dim], t); element: fn(x [n, dim], t);
+        either returns g [n] or [n, n_vars].  None removes the term."""
+        if fn is None:
+            cb = None
+        else:
+            def cb_py(xyz, normals, n, dim, t, values, user):
+                x = np.ctypeslib.as_array(xyz, shape=(n, dim))
+                out = np.ctypeslib.as_array(values, shape=(n, n_vars))
+                if boundary:
+                    nn = np.ctypeslib.as_array(normals, shape=(n, dim))
+                    g = fn(x, nn, t)
+                else:
+                    g = fn(x, t)
+                out[:] = np.asarray(g, dtype=float).reshape(n, n_vars)
+            cb = _native.SOURCE_FN(cb_py)
+        setter = self._lib.hgg_set_boundary_source if boundary else self._lib.hgg_set_element_source
+        self._check(setter(self._raw, ctypes.cast(cb, ctypes.c_void_p) if cb else None, None))
+        # the library calls the function until it is replaced: keep it alive
+        if not hasattr(self, "_sources"):
+            self._sources = {}
+        self._sources[boundary] = cb
 
     def synchronize(self):
         self._check(self._lib.hgg_synchronize(self._raw))
@@ -317,8 +344,9 @@ class HpgemAPISimplified:
                 outputTime += outputDt
         return time, n
 
-    def computeTimeDerivative(self, in_vec, out_vec):
-        self.handle.time_derivative(in_vec, out_vec)
+    def computeTimeDerivative(self, in_vec, out_vec, time=None):
+        """computeTimeDerivative(in, out, time); the time matters for source terms only."""
+        self.handle.time_derivative(in_vec, out_vec, time)
 
     def solve(self, initialTime, finalTime, dt, numberOfOutputFrames=1, u0=None):
         """Time loop of HpgemAPISimplified::solve (HpgemAPISimplified_Impl.h:976-1045):
@@ -399,6 +427,17 @@ class HpgemAPILinear(HpgemAPISimplified):
         self.n_basis = _basis_count(self.dim, description, self.polynomialOrder)
         self.n_elements = self.handle.vector_length // (self.numberOfVariables * self.n_basis)
         return self
+
+    def setSourceTerm(self, g):
+        """useSourceTerm (HpgemAPILinear_Impl.h:437-450): every stage adds the element
+        integrals of phi_i g_v(x, t); g(x [n, dim], t) -> [n] or [n, V].  None: off."""
+        self.handle.set_source(False, g, self.numberOfVariables)
+
+    def setSourceTermAtBoundary(self, g):
+        """useSourceTermAtBoundary (HpgemAPILinear_Impl.h:452-469): every stage adds, for
+        every boundary face, the face integrals of phi_i g_v(x, n, t) to its element;
+        g(x [n, dim], unit normals [n, dim], t) -> [n] or [n, V].  None: off."""
+        self.handle.set_source(True, g, self.numberOfVariables)
 
     def readMeshFile(self, path):
         """readMesh(fileName) + tasksBeforeSolving on a Preprocessor "mesh 2" file."""

@@ -370,6 +370,44 @@ int hgg_create_linear_structured(const char *description, int32_t order, int32_t
 int hgg_create_linear_mesh_file(const char *path, int32_t order, int32_t physics, const double *params,
                                 const char *tableau, int32_t precision, hgg_handle **out);
 
+/* Both stored-matrix constructors above take meshes with boundary faces
+ * (non-periodic directions): a boundary face contributes its (LEFT, LEFT)
+ * block, with the application's boundary integrand (advection: the upwind
+ * outflow term, nothing on inflow faces; wave: -n_d phi_j phi_i in the
+ * (p, s_d) block, AcousticWaveLinear_Impl.h:254-272). */
+
+/* Source terms of HpgemAPILinear: useSourceTerm / useSourceTermAtBoundary with
+ * addSourceTerm and addSourceTermAtBoundary (HpgemAPILinear_Impl.h:437-469),
+ * which computeRightHandSide (:471-498) calls after the stiffness multiply and
+ * before the mass solve, in every stage at the stage time t + c_i dt.  The
+ * integrand is phi_i(x) g_v(x, t) for basis function i of variable v, as in
+ * computeIntegrandSourceTermAtElement (:201-229) and in the face integrands
+ * of the reference's applications (080AdvectionLinear_SelfTest.cpp:72-88:
+ * g = -u_exact(x, t) (a . n) on inflow faces, 0 elsewhere); the library
+ * integrates it with the element rule times |J| (ElementIntegral) and the
+ * face rule times |n| (FaceIntegral).  The caller's function writes
+ * values[n_points][n_vars] = g(xyz[k], t) for every point: the element
+ * quadrature points of every element for the element source (normals null),
+ * and the face quadrature points of every boundary face, face by face, with
+ * the unit normal out of its element, for the boundary source.  It is called
+ * on the thread that steps the handle, once per stage time of each step
+ * (hgg_step evaluates a step's stage times while the GPU runs the previous
+ * step), never from a CUDA callback.  fn = NULL removes the term.  Only for
+ * handles from hgg_create_linear_structured / hgg_create_linear_mesh_file
+ * (they know the mesh), else HGG_ERR_UNSUPPORTED.  A handle with source terms
+ * needs the time: hgg_step with a non-null time, hgg_time_derivative_at
+ * (hgg_time_derivative and hgg_time_derivative_static return an error), and
+ * is not taken by batches. */
+typedef void (*hgg_source_fn)(const double *xyz, const double *normals, int64_t n_points, int32_t dim, double time,
+                              double *values, void *user);
+int hgg_set_element_source(hgg_handle *h, hgg_source_fn fn, void *user);
+int hgg_set_boundary_source(hgg_handle *h, hgg_source_fn fn, void *user);
+
+/* computeTimeDerivative(in, out, time) (HpgemAPISimplified_Impl.h:764-770)
+ * with the time the source terms are evaluated at; the same as
+ * hgg_time_derivative for handles without source terms. */
+int hgg_time_derivative_at(hgg_handle *h, int32_t in_vec, int32_t out_vec, double time);
+
 /* ---- many problems at once ------------------------------------------------
  * No counterpart in the reference (hpGEM advances one mesh per process).  A
  * batch advances many independent problems, each an existing handle with its

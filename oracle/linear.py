@@ -88,6 +88,11 @@ def assemble(prob):
                         factor = 0.5
                     an = A if ts == 0 else -A
                     blk[:] = -an * area * factor * pp
+                elif Rt < 0:
+                    # boundary face (AcousticWaveLinear_Impl.h:254-258, 271-272): -n_d in
+                    # the (p, s_d) block, nothing in (s_d, p); only (LEFT, LEFT) is used
+                    for c in range(d):
+                        blk[0:nB, (c + 1) * nB:(c + 2) * nB] = -n[c] * pp
                 else:
                     sgn = -1.0 if tr == 1 else 1.0
                     for c in range(d):

@@ -37,6 +37,18 @@ IDS = ["%dD-%s-p%d-%s" % (int(c[0].split()[2]), "tri" if "triangular" in c[0] el
                           "adv" if c[2] == 0 else "wave") for c in CASES]
 
 
+# meshes with boundary faces (non-periodic directions): the stored-matrix path takes them
+BOUNDARY_CASES = [
+    ("structured 1 1\n4\n0\n1\nrectangular\nfalse\n", 1, 0, [0.1]),
+    ("structured 1 2\n4 4\n0 0\n1 1\ntriangular\nfalse false\n", 2, 0, [0.1, 0.2]),
+    ("structured 1 2\n3 4\n0 0\n1 1\nrectangular\ntrue false\n", 2, 0, [1.0, -0.5]),
+    ("structured 1 3\n3 2 2\n0 0 0\n1 1 1\nrectangular\nfalse false false\n", 1, 0, [0.1, 0.2, 0.3]),
+    ("structured 1 3\n2 2 2\n0 0 0\n1 1 1\ntriangular\nfalse false false\n", 2, 0, [0.4, -0.3, 0.8]),
+    ("structured 1 2\n4 4\n0 0\n1 1\ntriangular\nfalse false\n", 2, 1, [1.0]),
+    ("structured 1 3\n2 3 2\n0 0 0\n1 1 1\nrectangular\nfalse true false\n", 2, 1, [0.7]),
+]
+
+
 def oracle_problem(description, p, physics, params):
     mesh = mesh_from_description(description)
     if physics == 0:
@@ -48,6 +60,23 @@ def oracle_problem(description, p, physics, params):
 def test_library_matrices_match_oracle_assembly(description, p, physics, params):
     prob = oracle_problem(description, p, physics, params)
     mass, K, fe, faces = assemble(prob)
+    D = linear_descriptor(description, p, physics, params)
+    scale = max(np.abs(K).max(), np.abs(faces).max())
+    assert np.array_equal(D["face_elements"], fe)
+    assert np.allclose(D["mass"], mass, rtol=0, atol=1e-15 * np.abs(mass).max() * 10)
+    assert np.allclose(D["element_stiffness"], K, rtol=0, atol=1e-14 * scale)
+    assert np.allclose(D["face_stiffness"], faces, rtol=0, atol=1e-14 * scale)
+
+
+@pytest.mark.parametrize("description,p,physics,params", BOUNDARY_CASES)
+def test_boundary_face_matrices_match_oracle_assembly(description, p, physics, params):
+    """Boundary faces carry only their (LEFT, LEFT) block, with the application's
+    boundary integrand (080:125-168 outflow term; AcousticWaveLinear_Impl.h:254-272)."""
+    prob = oracle_problem(description, p, physics, params)
+    mass, K, fe, faces = assemble(prob)
+    boundary = fe[:, 1] < 0
+    assert boundary.any()
+    faces[boundary, 1:] = 0.0  # only (LEFT, LEFT) exists on a boundary face
     D = linear_descriptor(description, p, physics, params)
     scale = max(np.abs(K).max(), np.abs(faces).max())
     assert np.array_equal(D["face_elements"], fe)

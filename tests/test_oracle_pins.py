@@ -126,13 +126,16 @@ def linear_advection_run(key, level, solver):
     """080AdvectionLinear_SelfTest's set-up (080:58-103, 108-168, 255-297): a_i = 0.1 + 0.1 i,
     u0 = prod sin(2 pi x_i) projected, inflow boundary value through the boundary source term
     g = -u_exact(x, t) (a . n) where a . n < 0, Dormand-Prince, nT steps to T; returns
-    (L2 error at T, golden).  ``solver(mesh, prob, a, g, u0, dt, nT)`` runs the steps."""
+    (L2 error at T, golden).  ``solver(cells, triangular, prob, a, g, exact, u0, dt, nT)``
+    runs the steps on the structured mesh of ``cells`` per direction, not periodic, from
+    the projection of exact(x, 0) (``u0``: the oracle's projection)."""
     par = _load("advection_linear_goldens.json")[key]
     D = {"dim1": 1, "dim2P1": 2, "dim2P2": 2, "dim3": 3}[key]
     name = par["files"][par["levels"][0] + level]   # e.g. unitSquareTrianglesN8
     N = int(name.rsplit("N", 1)[1])
     a = np.array([0.1 + 0.1 * i for i in range(D)])
-    mesh = structured_mesh([N] * D, [0.0] * D, [1.0] * D, "Triangles" in name, [False] * D)
+    triangular = "Triangles" in name
+    mesh = structured_mesh([N] * D, [0.0] * D, [1.0] * D, triangular, [False] * D)
     prob = Problem(mesh, par["p"], ADVECTION, a=a)
 
     def exact(x, t):
@@ -144,11 +147,11 @@ def linear_advection_run(key, level, solver):
 
     u0 = prob.project(lambda x: exact(x, 0.0)).reshape(-1)
     T, nT = par["end_time"], par["time_steps"]
-    u = solver(mesh, prob, a, inflow, u0, T / nT, nT)
+    u = solver([N] * D, triangular, prob, a, inflow, exact, u0, T / nT, nT)
     return prob.l2_error(u, exact, T), par["errors"][level]
 
 
-def _oracle_solver(mesh, prob, a, inflow, u0, dt, nT):
+def _oracle_solver(cells, triangular, prob, a, inflow, exact, u0, dt, nT):
     lin = LinearOracle(*assemble(prob)).set_sources(prob, boundary_source=inflow)
     return lin.step(u0, dt, nT, "DormandPrince")
 
