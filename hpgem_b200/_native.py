@@ -13,7 +13,7 @@ LIB_PATH = os.path.join(HERE, "_lib", "libhpgem_b200.so")
 # enum values of include/hpgem_b200.h
 SHAPE_LINE, SHAPE_SQUARE, SHAPE_TRIANGLE, SHAPE_CUBE, SHAPE_TETRAHEDRON = 1, 2, 3, 4, 5
 PHYSICS_ADVECTION, PHYSICS_WAVE, PHYSICS_WAVE_UPWIND = 0, 1, 2
-PRECISION_FP64, PRECISION_FP32 = 0, 1
+PRECISION_FP64, PRECISION_FP32, PRECISION_BF16X3 = 0, 1, 2
 ERRORS = {0: "HGG_OK", -1: "HGG_ERR_INVALID", -2: "HGG_ERR_UNSUPPORTED", -3: "HGG_ERR_CUDA",
           -4: "HGG_ERR_NOMEM", -5: "HGG_ERR_DEVICE", -6: "HGG_ERR_NOT_LOADED"}
 

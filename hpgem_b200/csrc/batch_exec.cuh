@@ -49,6 +49,14 @@ struct SliceItem {
     int slot;
 };
 
+// stored-matrix tiles on the tensor cores (tcgen05), the mixed forms
+struct UmmaItem {
+    StageIOT<float> io[2];
+    UmmaArgs a;
+    int64_t block0;  // first virtual tile
+    int slot;
+};
+
 template <typename KT>
 struct LinearItem {
     StageIOT<KT> io[2];
@@ -130,6 +138,31 @@ __global__ void __launch_bounds__(256)
     }
 }
 
+// the tiles of all members of a class, for the persistent tensor-core kernel
+struct UmmaGroupedTiles {
+    const UmmaItem *items;
+    int n;
+    int64_t nb;
+    const int *parity, *remaining;
+    __device__ int64_t total() const { return nb; }
+    __device__ bool get(int64_t vt, StageIOT<float> &io, UmmaArgs &a, int64_t &tile) const {
+        const int i = find_item(items, n, vt);
+        const int slot = items[i].slot;
+        if (remaining[slot] <= 0) return false;
+        io = items[i].io[parity[slot]];
+        a = items[i].a;
+        tile = vt - items[i].block0;
+        return true;
+    }
+};
+
+template <int KIND, int NIN>
+__global__ void __launch_bounds__(kUmmaThreads, 1)
+    grouped_umma(const UmmaItem *items, const int *n_items, const int64_t *total, const int *parity,
+                 const int *remaining, const UmmaShape sh, int *status) {
+    umma_persistent<KIND, NIN>(sh, UmmaGroupedTiles{items, *n_items, *total, parity, remaining}, status);
+}
+
 // end of one step of every member: flip the current buffer, count the step
 __global__ void batch_advance(int *parity, int *remaining, int cap) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -143,12 +176,13 @@ __global__ void batch_advance(int *parity, int *remaining, int cap) {
 
 namespace {
 
-enum BatchKind { KIND_DENSE = 0, KIND_TENSOR = 1, KIND_SLICE = 2, KIND_LINEAR = 3 };
+enum BatchKind { KIND_DENSE = 0, KIND_TENSOR = 1, KIND_SLICE = 2, KIND_LINEAR = 3, KIND_UMMA = 4 };
 
 struct BatchClass {
     // key
     int kind = 0, shape = 0, order = 0, dim = 0, physics = 0, S = 0;
     bool mixed = false;
+    int precision = 0, rows = 0, lslots = 0;  // tensor-core tiles: precision, rows and slots per element
     std::vector<double> rk_a, rk_b;
     // members and launch shape
     std::vector<int> slots;
@@ -224,6 +258,7 @@ int bfail(hgg_batch *b, int code, const std::string &msg) {
     } while (0)
 
 int batch_kind(const hgg_handle *h) {
+    if (h->umma_tiles > 0) return KIND_UMMA;
     if (h->linear) return KIND_LINEAR;
     if (h->slice_ok) return KIND_SLICE;
     if (h->op.tensor) return KIND_TENSOR;
@@ -233,7 +268,8 @@ int batch_kind(const hgg_handle *h) {
 bool same_class(const BatchClass &c, const hgg_handle *h) {
     return c.kind == batch_kind(h) && c.shape == h->op.shape && c.order == h->op.order && c.dim == h->op.dim &&
            c.physics == h->op.physics && c.mixed == h->mixed && c.S == h->S && c.rk_a == h->rk_a &&
-           c.rk_b == h->rk_b;
+           c.rk_b == h->rk_b &&
+           (c.kind != KIND_UMMA || (c.precision == h->precision && c.rows == h->lin_R && c.lslots == h->lin_slots));
 }
 
 int dense_R(const hgg_handle *h) { return h->op.V * h->op.nB; }
@@ -246,6 +282,7 @@ int tensor_epb(int order, int dim) {
 int64_t item_blocks(const BatchClass &c, const hgg_handle *h) {
     const int64_t nE = h->op.nE;
     if (c.kind == KIND_LINEAR) return h->lin_tiles;
+    if (c.kind == KIND_UMMA) return h->umma_tiles;
     if (c.kind == KIND_SLICE) return (nE + SliceShape::TE - 1) / SliceShape::TE;
     if (c.kind == KIND_TENSOR) {
         const int epb = tensor_epb(c.order, c.dim);
@@ -258,6 +295,7 @@ size_t class_item_bytes(const BatchClass &c) {
     if (c.kind == KIND_DENSE) return c.mixed ? sizeof(DenseItem<float>) : sizeof(DenseItem<double>);
     if (c.kind == KIND_TENSOR) return c.mixed ? sizeof(TensorItem<float>) : sizeof(TensorItem<double>);
     if (c.kind == KIND_LINEAR) return c.mixed ? sizeof(LinearItem<float>) : sizeof(LinearItem<double>);
+    if (c.kind == KIND_UMMA) return sizeof(UmmaItem);
     return c.mixed ? sizeof(SliceItem<float>) : sizeof(SliceItem<double>);
 }
 
@@ -282,6 +320,15 @@ void fill_items(const hgg_batch *b, const BatchClass &c, int stage, std::vector<
             for (int par = 0; par < 2; ++par)
                 it.io[par] = make_stage_io<KT>(h, par ? 1 - base : base, b->dt[slot], stage, b->d_status);
             it.g = dense_geom(h, c.epb);
+            it.block0 = block0;
+            it.slot = slot;
+            std::memcpy(dst, &it, sizeof(it));
+        } else if (c.kind == KIND_UMMA) {
+            UmmaItem it{};
+            for (int par = 0; par < 2; ++par)
+                it.io[par] = make_stage_io<float>(h, par ? 1 - base : base, b->dt[slot], stage, b->d_status);
+            it.a = UmmaArgs{h->d_umma_img, h->d_umma_tile_elems, h->d_umma_tile_mats, h->d_lin_nbr, h->umma_tiles,
+                            h->lin_mats, kUmmaPolls};
             it.block0 = block0;
             it.slot = slot;
             std::memcpy(dst, &it, sizeof(it));
@@ -398,7 +445,35 @@ void launch_grouped_slice(const hgg_batch *b, const BatchClass &c, int st, unsig
 void launch_class_stage(hgg_batch *b, const BatchClass &c, int st, cudaStream_t s) {
     // a fixed persistent grid: membership changes leave the launch (and the graph) as it is
     const unsigned grid = (unsigned)(c.ctas_per_sm * b->num_sms);
-    if (c.kind == KIND_LINEAR) {
+    if (c.kind == KIND_UMMA) {
+        const int kind = c.precision == HGG_PRECISION_BF16X3 ? kUmmaBF16 : kUmmaTF32;
+        const UmmaShape sh = umma_shape(c.rows, c.lslots, kind);
+        int nin = 0;  // stage-input vectors of this stage (the tableau's nonzero a_ij)
+        for (int j = 0; j < st; ++j) nin += c.rk_a[st * c.S + j] != 0.0;
+        if (!(c.rows % 4 == 0 && nin <= 1)) nin = -1;
+        const size_t smem = umma_smem(sh);
+        const UmmaItem *it = static_cast<const UmmaItem *>(c.d_items[st]);
+        auto go = [&](auto kc, auto nc) {
+            constexpr int K = decltype(kc)::value, NIN = decltype(nc)::value;
+            cudaFuncSetAttribute(grouped_umma<K, NIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            grouped_umma<K, NIN><<<grid, kUmmaThreads, smem, s>>>(it, c.d_n, c.d_total, b->d_parity,
+                                                                   b->d_remaining, sh, b->d_status);
+        };
+        using I0 = std::integral_constant<int, 0>;
+        using I1 = std::integral_constant<int, 1>;
+        using IM = std::integral_constant<int, -1>;
+        using KT32 = std::integral_constant<int, kUmmaTF32>;
+        using KB16 = std::integral_constant<int, kUmmaBF16>;
+        if (kind == kUmmaTF32) {
+            if (nin == 0) go(KT32{}, I0{});
+            else if (nin == 1) go(KT32{}, I1{});
+            else go(KT32{}, IM{});
+        } else {
+            if (nin == 0) go(KB16{}, I0{});
+            else if (nin == 1) go(KB16{}, I1{});
+            else go(KB16{}, IM{});
+        }
+    } else if (c.kind == KIND_LINEAR) {
         if (c.mixed)
             grouped_linear<float><<<grid, 256, 0, s>>>(static_cast<const LinearItem<float> *>(c.d_items[st]), c.d_n,
                                                        c.d_total, b->d_parity, b->d_remaining);
@@ -454,6 +529,15 @@ int tune_class(hgg_batch *b, BatchClass &c) {
             if (!same_epb) return upload_class(b, c);  // dense block counts depend on epb
             return 0;
         }
+    }
+    if (c.kind == KIND_UMMA) {
+        // one resident CTA per SM (its shared memory and tensor memory), or as many as fit
+        const int kind = c.precision == HGG_PRECISION_BF16X3 ? kUmmaBF16 : kUmmaTF32;
+        const size_t smem = umma_smem(umma_shape(c.rows, c.lslots, kind));
+        c.ctas_per_sm = std::max(1, std::min(4, (int)((227 * 1024) / (smem + 1024))));
+        c.tuned = true;
+        c.tuned_bucket = key.bucket;
+        return 0;
     }
     std::vector<std::pair<int, int>> cands;  // (epb, ctas_per_sm)
     const int ctas[] = {2, 4, 8};
@@ -707,6 +791,9 @@ int hgg_batch_add(hgg_batch *b, hgg_handle *h, double dt, int32_t nsteps, int32_
         c.S = h->S;
         c.rk_a = h->rk_a;
         c.rk_b = h->rk_b;
+        c.precision = h->precision;
+        c.rows = h->lin_R;
+        c.lslots = h->lin_slots;
         c.epb = c.kind == KIND_DENSE ? std::max(1, 256 / dense_rows(h->op.dim, h->op.physics != HGG_PHYSICS_ADVECTION, h->op.nB)) : 1;
         c.item_bytes = class_item_bytes(c);
         c.d_items.assign(c.S, nullptr);

@@ -144,6 +144,22 @@ int enqueue_step(hgg_handle *h, int from, double dt) {
     return h->mixed ? enqueue_step_t<float>(h, from, dt) : enqueue_step_t<double>(h, from, dt);
 }
 
+uint32_t float_bits(float f) {
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    return u;
+}
+float bits_float(uint32_t u) {
+    float f;
+    std::memcpy(&f, &u, 4);
+    return f;
+}
+// BF16 bits of f, rounded to nearest even (f finite)
+uint16_t bf16_rn(float f) {
+    const uint32_t u = float_bits(f);
+    return (uint16_t)((u + 0x7FFFu + ((u >> 16) & 1u)) >> 16);
+}
+
 std::string status_message(int st) {
     std::string m = "kernel status word " + std::to_string(st) + ":";
     if (st & 1) m += " bad neighbour index (bit 0);";
@@ -171,9 +187,11 @@ int set_tableau(hgg_handle *h, int32_t n_stages, const double *a, const double *
     h->rk_a.assign(a, a + h->S * h->S);
     h->rk_b.assign(b, b + h->S);
     h->rk_c = c ? std::vector<double>(c, c + h->S) : std::vector<double>(h->S, 0.0);
-    if (precision != HGG_PRECISION_FP64 && precision != HGG_PRECISION_FP32)
-        return fail(h, HGG_ERR_INVALID, "precision must be HGG_PRECISION_FP64 or HGG_PRECISION_FP32");
-    h->mixed = precision == HGG_PRECISION_FP32;
+    if (precision != HGG_PRECISION_FP64 && precision != HGG_PRECISION_FP32 && precision != HGG_PRECISION_BF16X3)
+        return fail(h, HGG_ERR_INVALID,
+                    "precision must be HGG_PRECISION_FP64, HGG_PRECISION_FP32 or HGG_PRECISION_BF16X3");
+    h->mixed = precision != HGG_PRECISION_FP64;
+    h->precision = precision;
     return 0;
 }
 
@@ -200,7 +218,10 @@ int init_device_vectors(hgg_handle *h) {
     return 0;
 }
 
-int attach_linear(hgg_handle *h, const LinearSystem &sys, bool tiles_only = false);
+// tiles_only: 0 attach in any case; 1 only when a tile kernel (FP64 tensor-core
+// DMMA tiles or the tcgen05 tiles of the mixed forms) will run; 2 only for the
+// tcgen05 tiles
+int attach_linear(hgg_handle *h, const LinearSystem &sys, int tiles_only = 0);
 
 // linear: the handle will run the stored-matrix kernel (attach_linear), so the
 // vectors stay in hpGEM order and the matrix-free operators are not uploaded
@@ -210,7 +231,8 @@ int create_from_desc(const hgg_problem_desc *desc, hgg_handle *h, bool linear = 
     } catch (const std::exception &ex) {
         return fail(h, HGG_ERR_INVALID, ex.what());
     }
-    if (linear) h->op.tensor = false;
+    // split-BF16 runs only as folded tiles on the tensor cores: not the sum-factorised kernels
+    if (linear || desc->precision == HGG_PRECISION_BF16X3) h->op.tensor = false;
     int rc = set_tableau(h, desc->n_stages, desc->rk_a, desc->rk_b, desc->rk_c, desc->precision);
     if (rc) return rc;
     const HostOperators &op = h->op;
@@ -281,8 +303,14 @@ int create_from_desc(const hgg_problem_desc *desc, hgg_handle *h, bool linear = 
         // ms per step at p = 4, 0.48 against 0.87 at p = 5; in the mixed form p = 4
         // measured 0.33 against 0.29 and stays on the dense kernel).  Only when the
         // mesh forms tiles (structured meshes); otherwise the dense kernel runs.
-        if (op.physics == HGG_PHYSICS_ADVECTION && op.shape == HGG_SHAPE_TRIANGLE &&
-            (op.nB >= 21 || (op.nB >= 15 && !h->mixed))) {
+        // The mixed forms run folded tiles on the tensor cores (tcgen05) where the mesh
+        // forms them: split-BF16 always (it has no other kernel), the FP32 form for the
+        // wave and for advection on triangles at p = 5.
+        const bool fold_tri = op.physics == HGG_PHYSICS_ADVECTION && op.shape == HGG_SHAPE_TRIANGLE &&
+                              (op.nB >= 21 || (op.nB >= 15 && !h->mixed));
+        const bool fold_tc = h->precision == HGG_PRECISION_BF16X3 ||
+                             (h->precision == HGG_PRECISION_FP32 && op.physics != HGG_PHYSICS_ADVECTION);
+        if (fold_tri || fold_tc) {
             LinearSystem sys;
             bool assembled = true;
             try {
@@ -292,9 +320,12 @@ int create_from_desc(const hgg_problem_desc *desc, hgg_handle *h, bool linear = 
             }
             if (assembled) {
                 h->lin_min_rows = 1;
-                if ((rc = attach_linear(h, sys, true))) return rc;
+                if ((rc = attach_linear(h, sys, fold_tri ? 1 : 2))) return rc;
                 if (h->linear) return 0;
             }
+            if (h->precision == HGG_PRECISION_BF16X3)
+                return fail(h, HGG_ERR_UNSUPPORTED,
+                            "split-BF16 runs on tiles of elements with identical matrices: this mesh forms none");
         }
         // the dense kernel reads its operators transposed ([..][j][i]): coalesced across rows i
         auto transposed = [&](const std::vector<double> &m) {
@@ -370,7 +401,7 @@ int create_from_desc(const hgg_problem_desc *desc, hgg_handle *h, bool linear = 
 // Folds the stored matrices (fold_linear) and uploads them: the handle's
 // stages then run the stored-matrix kernel.  With tiles_only, nothing is
 // attached (and 0 returned) unless the grouped tensor-core kernel will run.
-int attach_linear(hgg_handle *h, const LinearSystem &sys, bool tiles_only) {
+int attach_linear(hgg_handle *h, const LinearSystem &sys, int tiles_only) {
     LinearOperators lo;
     try {
         lo = fold_linear(sys);
@@ -388,9 +419,8 @@ int attach_linear(hgg_handle *h, const LinearSystem &sys, bool tiles_only) {
     // synchronisation cost more than the row kernel: measured on quadrilaterals
     // at p = 2, 9 rows, 0.82 ms per RK4 step against 0.46 ms on 512^2 cells;
     // on 256^2 triangles the tiles won from 15 rows: 0.39 against 0.46 ms).
-    std::vector<int32_t> tel, tmat;
-    int64_t n_tiles = 0;
-    {
+    // tiles of `tile_n` elements with identical matrices, in the order of their first element
+    auto make_tiles = [&](int tile_n, std::vector<int32_t> &tel, std::vector<int32_t> &tmat) -> int64_t {
         const int S = lo.slots, W = S + 1;
         auto tuple = [&](int64_t e, int k) { return k == 0 ? lo.self_mat[e] : lo.nbr_mat[(size_t)e * S + k - 1]; };
         std::vector<int64_t> order(lo.E);
@@ -400,7 +430,7 @@ int attach_linear(hgg_handle *h, const LinearSystem &sys, bool tiles_only) {
                 if (tuple(x, k) != tuple(y, k)) return tuple(x, k) < tuple(y, k);
             return false;
         });
-        int fill = kLinTileN;
+        int fill = tile_n;
         for (size_t i = 0; i < order.size(); ++i) {
             const int64_t e = order[i];
             const bool same = i > 0 && [&] {
@@ -408,30 +438,49 @@ int attach_linear(hgg_handle *h, const LinearSystem &sys, bool tiles_only) {
                     if (tuple(e, k) != tuple(order[i - 1], k)) return false;
                 return true;
             }();
-            if (!same || fill == kLinTileN) {
-                tel.insert(tel.end(), kLinTileN, -1);
+            if (!same || fill == tile_n) {
+                tel.insert(tel.end(), tile_n, -1);
                 for (int k = 0; k < W; ++k) tmat.push_back(tuple(e, k));
                 fill = 0;
             }
-            tel[tel.size() - kLinTileN + fill++] = (int32_t)e;
+            tel[tel.size() - tile_n + fill++] = (int32_t)e;
         }
-        n_tiles = (int64_t)(tel.size() / kLinTileN);
+        const int64_t n_tiles = (int64_t)(tel.size() / tile_n);
         // tiles in the order of their first element (see the grouped dense kernel)
         std::vector<int64_t> torder(n_tiles);
         for (int64_t t2 = 0; t2 < n_tiles; ++t2) torder[t2] = t2;
         std::stable_sort(torder.begin(), torder.end(),
-                         [&](int64_t x, int64_t y) { return tel[x * kLinTileN] < tel[y * kLinTileN]; });
+                         [&](int64_t x, int64_t y) { return tel[x * tile_n] < tel[y * tile_n]; });
         std::vector<int32_t> el2(tel.size()), mat2(tmat.size());
         for (int64_t t2 = 0; t2 < n_tiles; ++t2) {
-            std::copy(tel.begin() + torder[t2] * kLinTileN, tel.begin() + (torder[t2] + 1) * kLinTileN,
-                      el2.begin() + t2 * kLinTileN);
+            std::copy(tel.begin() + torder[t2] * tile_n, tel.begin() + (torder[t2] + 1) * tile_n,
+                      el2.begin() + t2 * tile_n);
             std::copy(tmat.begin() + torder[t2] * W, tmat.begin() + (torder[t2] + 1) * W, mat2.begin() + t2 * W);
         }
         tel.swap(el2);
         tmat.swap(mat2);
-    }
+        return n_tiles;
+    };
+    std::vector<int32_t> tel, tmat;
+    const int64_t n_tiles = make_tiles(kLinTileN, tel, tmat);
     const bool use_tiles = n_tiles * kLinTileN <= 2 * lo.E && R >= h->lin_min_rows;
-    if (tiles_only && !use_tiles) return 0;
+    // the mixed forms run the tiles on the tensor cores (tcgen05), 128 elements per tile,
+    // where the operands fit the shared memory of one CTA
+    std::vector<int32_t> utel, utmat;
+    int64_t u_tiles = 0;
+    const int ukind = h->precision == HGG_PRECISION_BF16X3 ? kUmmaBF16 : kUmmaTF32;
+    const UmmaShape ush = umma_shape(R, lo.slots, ukind);
+    if (h->mixed && umma_smem(ush) <= 227 * 1024 && ush.NP <= 256) {
+        u_tiles = make_tiles(kUmmaTileN, utel, utmat);
+        if (!(u_tiles * kUmmaTileN <= 2 * lo.E)) u_tiles = 0;
+    }
+    if (h->precision == HGG_PRECISION_BF16X3 && u_tiles == 0) {
+        if (tiles_only) return 0;
+        return fail(h, HGG_ERR_UNSUPPORTED,
+                    "split-BF16 runs on tiles of elements with identical matrices: this mesh forms none");
+    }
+    if (tiles_only == 1 && !use_tiles && u_tiles == 0) return 0;
+    if (tiles_only == 2 && u_tiles == 0) return 0;
     std::vector<double> t(lo.table.size());
     for (int m = 0; m < lo.n_mats(); ++m)
         for (int i = 0; i < R; ++i)
@@ -449,6 +498,34 @@ int attach_linear(hgg_handle *h, const LinearSystem &sys, bool tiles_only) {
             (rc = upload(h, tmat, &h->d_lin_tile_mats)))
             return rc;
         h->lin_tiles = n_tiles;
+    }
+    if (u_tiles > 0) {
+        // operand images of every distinct matrix: hi part then lo part, each NP x KP in the
+        // core-matrix layout the kernel's shared memory holds (umma_offset)
+        const size_t part = ush.b_bytes, mats = (size_t)lo.n_mats();
+        std::vector<unsigned char> img(mats * 2 * part, 0);
+        for (size_t m = 0; m < mats; ++m)
+            for (int n = 0; n < R; ++n)
+                for (int k = 0; k < R; ++k) {
+                    const double x = lo.table[m * RR + (size_t)n * R + k];
+                    unsigned char *dst = img.data() + m * 2 * part + umma_offset(n, k, ush.KP, ush.es);
+                    if (ukind == kUmmaTF32) {
+                        const uint32_t hb = float_bits((float)x) & 0xFFFFE000u;
+                        const uint32_t lb = float_bits((float)(x - (double)bits_float(hb)));
+                        std::memcpy(dst, &hb, 4);
+                        std::memcpy(dst + part, &lb, 4);
+                    } else {
+                        const uint16_t hb = bf16_rn((float)x);
+                        const uint16_t lb = bf16_rn((float)(x - (double)bits_float((uint32_t)hb << 16)));
+                        std::memcpy(dst, &hb, 2);
+                        std::memcpy(dst + part, &lb, 2);
+                    }
+                }
+        if ((rc = upload(h, img, &h->d_umma_img)) || (rc = upload(h, utel, &h->d_umma_tile_elems)) ||
+            (rc = upload(h, utmat, &h->d_umma_tile_mats)))
+            return rc;
+        if (!h->d_lin_nbr && lo.slots > 0 && (rc = upload(h, lo.nbr, &h->d_lin_nbr))) return rc;
+        h->umma_tiles = u_tiles;
     }
     h->lin_R = R;
     h->lin_slots = lo.slots;
@@ -631,7 +708,9 @@ int hgg_synchronize(hgg_handle *h) {
 
 int64_t hgg_vector_length(const hgg_handle *h) { return h ? h->N : -1; }
 
-int hgg_kernel_kind(const hgg_handle *h) { return h ? (h->linear ? 2 : (h->op.tensor ? 1 : 0)) : -1; }
+int hgg_kernel_kind(const hgg_handle *h) {
+    return h ? (h->umma_tiles > 0 ? 3 : (h->linear ? 2 : (h->op.tensor ? 1 : 0))) : -1;
+}
 
 int hgg_set_store_last_stage(hgg_handle *h, int32_t enable) {
     if (!h) return fail(h, HGG_ERR_INVALID, "null handle");
@@ -1055,9 +1134,9 @@ namespace {
 int linear_structured_system(const char *description, int32_t order, int32_t physics, const double *params,
                              const char *tableau, StructuredProblem &P, LinearSystem &sys,
                              const char *mesh_file = nullptr) {
-    if (physics != HGG_PHYSICS_ADVECTION && physics != HGG_PHYSICS_WAVE)
+    if (physics != HGG_PHYSICS_ADVECTION && physics != HGG_PHYSICS_WAVE && physics != HGG_PHYSICS_WAVE_UPWIND)
         return fail(nullptr, HGG_ERR_UNSUPPORTED,
-                    "the stored-matrix form has the reference's linear advection and central-flux wave");
+                    "the stored-matrix form has the reference's linear advection and wave (central or upwind flux)");
     if (mesh_file) {
         int rc = mesh_file_problem(mesh_file, order, physics, params, tableau, P, true);
         if (rc) return rc;

@@ -13,6 +13,7 @@
 #include "../../include/hpgem_b200.h"
 #include "dg_kernels.cuh"
 #include "linear_stage.cuh"
+#include "linear_umma.cuh"
 #include "tensor_pipe.cuh"
 #include "tensor_slice.cuh"
 #include "host/linear.h"
@@ -79,6 +80,12 @@ struct hgg_handle {
     int32_t *d_lin_tile_elems = nullptr, *d_lin_tile_mats = nullptr;
     int64_t lin_tiles = 0;
     int lin_min_rows = hgg::kLinTileMinRows;  // fewer rows per element: the row kernel
+    // mixed forms on the tensor cores (tcgen05): tiles of 128 elements with identical
+    // matrices, matrix operand images split into hi / lo parts
+    int precision = 0;                     // enum hgg_precision
+    int64_t umma_tiles = 0;                // 0: not used
+    int32_t *d_umma_tile_elems = nullptr, *d_umma_tile_mats = nullptr;
+    unsigned char *d_umma_img = nullptr;
     // grouped dense kernel: tiles of kGroupTile elements with the same operator signature
     int32_t *d_group_tiles = nullptr;
     int64_t group_tiles = 0;

@@ -125,9 +125,13 @@ LinearSystem linear_from_desc(const hgg_linear_desc &d) {
 }
 
 LinearSystem assemble_linear(const hgg_problem_desc &desc) {
-    const bool wave = desc.physics == HGG_PHYSICS_WAVE;
+    const bool upwind = desc.physics == HGG_PHYSICS_WAVE_UPWIND;
+    const bool wave = desc.physics == HGG_PHYSICS_WAVE || upwind;
     if (desc.physics != HGG_PHYSICS_ADVECTION && !wave)
-        throw std::invalid_argument("the stored-matrix form has advection and the central-flux wave");
+        throw std::invalid_argument("the stored-matrix form has advection and the wave");
+    // the upwind wave's extra face terms (1/2) |A_n| [[U]]: c |n| [[v]] / 2 and
+    // c c_inv n (n . [[s]]) / (2 |n|), c = 1 / sqrt(c_inv) (the matrix-free kernels' flux)
+    const double c_wave = upwind ? 1.0 / std::sqrt(desc.c_inv) : 0.0;
     const int d = desc.dim, nB = desc.n_basis, nQ = desc.n_quad, nQf = desc.n_face_quad;
     const int V = wave ? d + 1 : 1, R = V * nB;
     if (R > 256) throw std::invalid_argument("the stored-matrix form takes at most 256 rows per element");
@@ -208,6 +212,7 @@ LinearSystem assemble_linear(const hgg_problem_desc &desc) {
         // a boundary face (right element -1) has only its (LEFT, LEFT) block
         // (FaceMatrix of one side; Face::isInternal() false)
         const bool boundary = Rt < 0;
+        if (boundary && upwind) throw std::invalid_argument("the upwind wave has no boundary faces here");
         const int tab[3] = {desc.face_tab_index[2 * f], boundary ? desc.face_tab_index[2 * f] : desc.face_tab_index[2 * f + 1],
                             boundary ? 1 : 0};
         if (tab[0] < 0 || tab[1] < 0 || tab[0] >= desc.n_face_tabs || tab[1] >= desc.n_face_tabs)
@@ -266,6 +271,14 @@ LinearSystem assemble_linear(const hgg_problem_desc &desc) {
                                     const double t = -0.5 * sgn * n[c] * pp;
                                     blk[(size_t)i * R + (c + 1) * nB + j] += t;
                                     blk[(size_t)((c + 1) * nB + i) * R + j] += t;
+                                }
+                                if (upwind) {  // own side: -(1/2) |A_n|; other side: +(1/2) |A_n|
+                                    const double side = ts == tr ? -0.5 : 0.5;
+                                    blk[(size_t)i * R + j] += side * c_wave * area * pp;
+                                    for (int c = 0; c < d; ++c)
+                                        for (int m = 0; m < d; ++m)
+                                            blk[(size_t)((c + 1) * nB + i) * R + (m + 1) * nB + j] +=
+                                                side * c_wave * desc.c_inv * n[c] * n[m] / area * pp;
                                 }
                             }
                     }

@@ -66,8 +66,43 @@ int launch_dense_any(hgg_handle *h, const StageIOT<KT> &io) {
     return fail(h, HGG_ERR_UNSUPPORTED, "shape");
 }
 
+// the mixed forms on the tensor cores: persistent CTAs over the 128-element tiles
+int launch_umma(hgg_handle *h, const StageIOT<float> &io) {
+    const int kind = h->precision == HGG_PRECISION_BF16X3 ? kUmmaBF16 : kUmmaTF32;
+    const UmmaShape sh = umma_shape(h->lin_R, h->lin_slots, kind);
+    UmmaArgs a{h->d_umma_img, h->d_umma_tile_elems, h->d_umma_tile_mats, h->d_lin_nbr, h->umma_tiles, h->lin_mats,
+               kUmmaPolls};
+    const size_t smem = umma_smem(sh);
+    const unsigned grid = (unsigned)std::min<int64_t>(h->umma_tiles, h->num_sms);
+    auto go = [&](auto kc, auto nc) {
+        constexpr int K = decltype(kc)::value, NIN = decltype(nc)::value;
+        cudaFuncSetAttribute(linear_umma_stage<K, NIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        linear_umma_stage<K, NIN><<<grid, kUmmaThreads, smem, h->stream>>>(io, a, sh);
+    };
+    // vector loads need 16-byte aligned rows (R a multiple of 4) and at most one stage-input vector
+    const int nin = (h->lin_R % 4 == 0 && io.nin <= 1) ? io.nin : -1;
+    using I0 = std::integral_constant<int, 0>;
+    using I1 = std::integral_constant<int, 1>;
+    using IM = std::integral_constant<int, -1>;
+    using KT32 = std::integral_constant<int, kUmmaTF32>;
+    using KB16 = std::integral_constant<int, kUmmaBF16>;
+    if (kind == kUmmaTF32) {
+        if (nin == 0) go(KT32{}, I0{});
+        else if (nin == 1) go(KT32{}, I1{});
+        else go(KT32{}, IM{});
+    } else {
+        if (nin == 0) go(KB16{}, I0{});
+        else if (nin == 1) go(KB16{}, I1{});
+        else go(KB16{}, IM{});
+    }
+    return 0;
+}
+
 template <typename KT>
 int launch_linear(hgg_handle *h, const StageIOT<KT> &io) {
+    if constexpr (std::is_same_v<KT, float>) {
+        if (h->umma_tiles > 0) return launch_umma(h, io);
+    }
     const int R = h->lin_R;
     const int epb = std::max(1, 256 / R);
     LinearGeom g{h->d_lin_table, h->d_lin_table_rm, h->d_lin_table_f, h->d_lin_self, h->d_lin_nbr, h->d_lin_mat,

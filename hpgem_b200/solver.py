@@ -118,7 +118,7 @@ class Handle:
 
     @property
     def kernel_kind(self):
-        return {1: "tensor", 2: "linear"}.get(self._lib.hgg_kernel_kind(self._raw), "dense")
+        return {1: "tensor", 2: "linear", 3: "linear_tc"}.get(self._lib.hgg_kernel_kind(self._raw), "dense")
 
     @property
     def launch_count(self):

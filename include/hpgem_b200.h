@@ -55,7 +55,16 @@ enum hgg_physics { HGG_PHYSICS_ADVECTION = 0, HGG_PHYSICS_WAVE = 1, HGG_PHYSICS_
 
 enum hgg_precision {
     HGG_PRECISION_FP64 = 0,  /* everything in FP64 (parity form) */
-    HGG_PRECISION_FP32 = 1   /* contractions in FP32, geometry / mass inverse / RK sums in FP64 */
+    HGG_PRECISION_FP32 = 1,  /* FP32-mixed: FP32 stage vectors and contractions; geometry, mass
+                                inverse, stage input and RK sums in FP64.  Where the stage is
+                                a dense product (stored-matrix tiles, folded operators) the
+                                contractions run on the tensor cores as three TF32 products
+                                (hi*hi + hi*lo + lo*hi of split operands), FP32-accurate */
+    HGG_PRECISION_BF16X3 = 2 /* split-BF16: as FP32 but every contraction on the tensor cores as
+                                three BF16 products of split operands with FP32 accumulation
+                                (about 2^-17 of each product); only handles whose stage runs as
+                                tiles of dense products (stored matrices, folded operators on
+                                structured meshes), else HGG_ERR_UNSUPPORTED */
 };
 
 enum hgg_error {
@@ -167,7 +176,10 @@ int64_t hgg_vector_length(const hgg_handle *h);
  * 0 when the dense reference-operator kernel does, 2 for the stored-matrix
  * kernels: handles from hgg_create_linear*, and matrix-free handles whose
  * operator the library folded into per-element matrices because the grouped
- * tensor-core kernel applies them faster (advection on triangles, p >= 4). */
+ * tensor-core kernel applies them faster (advection on triangles, p >= 4);
+ * 3 for the same stored-matrix tiles on the fifth-generation tensor cores
+ * (tcgen05: the FP32-mixed form as three TF32 products, the split-BF16 form as
+ * three BF16 products, 128-element tiles). */
 int hgg_kernel_kind(const hgg_handle *h);
 
 /* When enabled (default), the last stage derivative k_S is stored like the

@@ -85,6 +85,22 @@ def test_boundary_face_matrices_match_oracle_assembly(description, p, physics, p
     assert np.allclose(D["face_stiffness"], faces, rtol=0, atol=1e-14 * scale)
 
 
+@pytest.mark.parametrize("description,p", [(CASES[7][0], 2), (CASES[8][0], 2), (CASES[6][0], 3)])
+def test_upwind_wave_matrices_give_the_matrix_free_upwind_operator(description, p):
+    """The folded form of the upwind wave (the mixed forms fold the wave onto the
+    tensor-core tiles): its stored matrices, applied as HpgemAPILinear applies them,
+    give the matrix-free oracle's upwind right-hand side."""
+    from oracle.dg import WAVE_UPWIND
+    prob = Problem(mesh_from_description(description), p, WAVE_UPWIND, cinv=0.7)
+    D = linear_descriptor(description, p, 2, [0.7])
+    lin = LinearOracle(D["mass"], D["element_stiffness"], D["face_elements"], D["face_stiffness"])
+    u = np.random.default_rng(12).standard_normal(prob.n_dof)
+    k_lin, k_free = lin.time_derivative(u), prob.time_derivative(u)
+    M = np.einsum("q,qi,qj->ij", prob.rule.weights, prob.phi, prob.phi)
+    tol = max(1e-12, 8 * np.linalg.cond(M) * np.finfo(float).eps)
+    assert np.abs(k_lin - k_free).max() <= tol * np.abs(k_free).max()
+
+
 @pytest.mark.parametrize("description,p,physics,params", CASES, ids=IDS)
 def test_stored_matrices_give_the_matrix_free_operator(description, p, physics, params):
     prob = oracle_problem(description, p, physics, params)
@@ -112,9 +128,8 @@ def test_invalid_linear_inputs_are_rejected():
     owner = ctypes.c_void_p()
     quads = b"structured 1 2\n4 4\n0 0\n1 1\nrectangular\ntrue true\n"
     a = (ctypes.c_double * 3)(1.0, 0.5, 0.0)
-    # the upwind wave has no stored-matrix application in the reference
-    rc = lib.hgg_linear_descriptor(quads, 2, _native.PHYSICS_WAVE_UPWIND, a, b"RK4_4", 0,
-                                   ctypes.byref(desc), ctypes.byref(owner))
+    # physics the stored-matrix form does not assemble
+    rc = lib.hgg_linear_descriptor(quads, 2, 7, a, b"RK4_4", 0, ctypes.byref(desc), ctypes.byref(owner))
     assert rc == -2
     assert lib.hgg_linear_descriptor(quads, 2, 0, a, b"NoSuchTableau", 0, ctypes.byref(desc),
                                      ctypes.byref(owner)) == -1
@@ -164,7 +179,6 @@ def test_linear_mesh_file_reports_a_missing_device_or_succeeds():
         lib.hgg_destroy(h)
     else:
         assert rc == -6 and b"device" in lib.hgg_last_error(None)
-    # a missing file and the upwind wave are rejected before any device is touched
+    # a missing file and an unknown physics are rejected before any device is touched
     assert lib.hgg_create_linear_mesh_file(b"/nonexistent.hpgem", 2, 0, a, b"RK4_4", 0, ctypes.byref(h)) == -1
-    assert lib.hgg_create_linear_mesh_file(path.encode(), 2, _native.PHYSICS_WAVE_UPWIND, a, b"RK4_4", 0,
-                                           ctypes.byref(h)) == -2
+    assert lib.hgg_create_linear_mesh_file(path.encode(), 2, 7, a, b"RK4_4", 0, ctypes.byref(h)) == -2
