@@ -156,11 +156,26 @@ struct UmmaGroupedTiles {
     }
 };
 
-template <int KIND, int NIN>
+template <int KIND>
 __global__ void __launch_bounds__(kUmmaThreads, 1)
     grouped_umma(const UmmaItem *items, const int *n_items, const int64_t *total, const int *parity,
                  const int *remaining, const UmmaShape sh, int *status) {
-    umma_persistent<KIND, NIN>(sh, UmmaGroupedTiles{items, *n_items, *total, parity, remaining}, status);
+    umma_persistent<KIND>(sh, UmmaGroupedTiles{items, *n_items, *total, parity, remaining}, status);
+}
+
+// the split stage input of every member (blockIdx.y: member)
+template <int KIND, int NIN>
+__global__ void __launch_bounds__(256)
+    grouped_umma_planes(const UmmaItem *items, const int *n_items, const int *parity, const int *remaining,
+                        const UmmaShape sh) {
+    constexpr int per16 = KIND == kUmmaTF32 ? 4 : 8;
+    if ((int)blockIdx.y >= *n_items) return;
+    const UmmaItem &it = items[blockIdx.y];
+    if (remaining[it.slot] <= 0) return;
+    const StageIOT<float> &io = it.io[parity[it.slot]];
+    const int64_t n = io.n_elements * (sh.KP / per16);
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        umma_planes_body<KIND, NIN>(io, const_cast<unsigned char *>(it.a.planes), sh.R, sh.KP, i);
 }
 
 // end of one step of every member: flip the current buffer, count the step
@@ -327,8 +342,8 @@ void fill_items(const hgg_batch *b, const BatchClass &c, int stage, std::vector<
             UmmaItem it{};
             for (int par = 0; par < 2; ++par)
                 it.io[par] = make_stage_io<float>(h, par ? 1 - base : base, b->dt[slot], stage, b->d_status);
-            it.a = UmmaArgs{h->d_umma_img, h->d_umma_tile_elems, h->d_umma_tile_mats, h->d_lin_nbr, h->umma_tiles,
-                            h->lin_mats, kUmmaPolls};
+            it.a = UmmaArgs{h->d_umma_img, h->d_umma_planes, h->d_umma_tile_elems, h->d_umma_tile_mats, h->d_lin_nbr,
+                            h->umma_tiles, h->lin_mats, kUmmaPolls};
             it.block0 = block0;
             it.slot = slot;
             std::memcpy(dst, &it, sizeof(it));
@@ -453,11 +468,16 @@ void launch_class_stage(hgg_batch *b, const BatchClass &c, int st, cudaStream_t 
         if (!(c.rows % 4 == 0 && nin <= 1)) nin = -1;
         const size_t smem = umma_smem(sh);
         const UmmaItem *it = static_cast<const UmmaItem *>(c.d_items[st]);
-        auto go = [&](auto kc, auto nc) {
+        const dim3 pgrid((unsigned)(2 * b->num_sms), (unsigned)b->cap);
+        auto planes = [&](auto kc, auto nc) {
             constexpr int K = decltype(kc)::value, NIN = decltype(nc)::value;
-            cudaFuncSetAttribute(grouped_umma<K, NIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            grouped_umma<K, NIN><<<grid, kUmmaThreads, smem, s>>>(it, c.d_n, c.d_total, b->d_parity,
-                                                                   b->d_remaining, sh, b->d_status);
+            grouped_umma_planes<K, NIN><<<pgrid, 256, 0, s>>>(it, c.d_n, b->d_parity, b->d_remaining, sh);
+        };
+        auto tiles = [&](auto kc) {
+            constexpr int K = decltype(kc)::value;
+            cudaFuncSetAttribute(grouped_umma<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            grouped_umma<K><<<grid, kUmmaThreads, smem, s>>>(it, c.d_n, c.d_total, b->d_parity, b->d_remaining, sh,
+                                                             b->d_status);
         };
         using I0 = std::integral_constant<int, 0>;
         using I1 = std::integral_constant<int, 1>;
@@ -465,14 +485,17 @@ void launch_class_stage(hgg_batch *b, const BatchClass &c, int st, cudaStream_t 
         using KT32 = std::integral_constant<int, kUmmaTF32>;
         using KB16 = std::integral_constant<int, kUmmaBF16>;
         if (kind == kUmmaTF32) {
-            if (nin == 0) go(KT32{}, I0{});
-            else if (nin == 1) go(KT32{}, I1{});
-            else go(KT32{}, IM{});
+            if (nin == 0) planes(KT32{}, I0{});
+            else if (nin == 1) planes(KT32{}, I1{});
+            else planes(KT32{}, IM{});
+            tiles(KT32{});
         } else {
-            if (nin == 0) go(KB16{}, I0{});
-            else if (nin == 1) go(KB16{}, I1{});
-            else go(KB16{}, IM{});
+            if (nin == 0) planes(KB16{}, I0{});
+            else if (nin == 1) planes(KB16{}, I1{});
+            else planes(KB16{}, IM{});
+            tiles(KB16{});
         }
+        b->launches++;  // the planes launch
     } else if (c.kind == KIND_LINEAR) {
         if (c.mixed)
             grouped_linear<float><<<grid, 256, 0, s>>>(static_cast<const LinearItem<float> *>(c.d_items[st]), c.d_n,

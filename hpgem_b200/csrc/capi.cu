@@ -470,7 +470,8 @@ int attach_linear(hgg_handle *h, const LinearSystem &sys, int tiles_only) {
     int64_t u_tiles = 0;
     const int ukind = h->precision == HGG_PRECISION_BF16X3 ? kUmmaBF16 : kUmmaTF32;
     const UmmaShape ush = umma_shape(R, lo.slots, ukind);
-    if (h->mixed && umma_smem(ush) <= 227 * 1024 && ush.NP <= 256) {
+    // (plane rows of at most 512 bytes: a thread's copies of one item stay in registers)
+    if (h->mixed && umma_smem(ush) <= 227 * 1024 && ush.NP <= 256 && ush.KP * ush.es <= 512) {
         u_tiles = make_tiles(kUmmaTileN, utel, utmat);
         if (!(u_tiles * kUmmaTileN <= 2 * lo.E)) u_tiles = 0;
     }
@@ -501,14 +502,14 @@ int attach_linear(hgg_handle *h, const LinearSystem &sys, int tiles_only) {
     }
     if (u_tiles > 0) {
         // operand images of every distinct matrix: hi part then lo part, each NP x KP in the
-        // core-matrix layout the kernel's shared memory holds (umma_offset)
+        // swizzled layout the kernel's shared memory holds (umma_offset)
         const size_t part = ush.b_bytes, mats = (size_t)lo.n_mats();
         std::vector<unsigned char> img(mats * 2 * part, 0);
         for (size_t m = 0; m < mats; ++m)
             for (int n = 0; n < R; ++n)
                 for (int k = 0; k < R; ++k) {
                     const double x = lo.table[m * RR + (size_t)n * R + k];
-                    unsigned char *dst = img.data() + m * 2 * part + umma_offset(n, k, ush.KP, ush.es);
+                    unsigned char *dst = img.data() + m * 2 * part + umma_offset(n, k, ush.NP, ush.es);
                     if (ukind == kUmmaTF32) {
                         const uint32_t hb = float_bits((float)x) & 0xFFFFE000u;
                         const uint32_t lb = float_bits((float)(x - (double)bits_float(hb)));
@@ -525,6 +526,8 @@ int attach_linear(hgg_handle *h, const LinearSystem &sys, int tiles_only) {
             (rc = upload(h, utmat, &h->d_umma_tile_mats)))
             return rc;
         if (!h->d_lin_nbr && lo.slots > 0 && (rc = upload(h, lo.nbr, &h->d_lin_nbr))) return rc;
+        if ((rc = alloc(h, 2 * (size_t)lo.E * ush.KP * ush.es, (void **)&h->d_umma_planes))) return rc;
+        HGG_CUDA(h, cudaMemsetAsync(h->d_umma_planes, 0, 2 * (size_t)lo.E * ush.KP * ush.es, h->stream));
         h->umma_tiles = u_tiles;
     }
     h->lin_R = R;

@@ -86,6 +86,7 @@ struct hgg_handle {
     int64_t umma_tiles = 0;                // 0: not used
     int32_t *d_umma_tile_elems = nullptr, *d_umma_tile_mats = nullptr;
     unsigned char *d_umma_img = nullptr;
+    unsigned char *d_umma_planes = nullptr;  // split stage input, two planes [E][KP]
     // grouped dense kernel: tiles of kGroupTile elements with the same operator signature
     int32_t *d_group_tiles = nullptr;
     int64_t group_tiles = 0;

@@ -66,35 +66,45 @@ int launch_dense_any(hgg_handle *h, const StageIOT<KT> &io) {
     return fail(h, HGG_ERR_UNSUPPORTED, "shape");
 }
 
-// the mixed forms on the tensor cores: persistent CTAs over the 128-element tiles
+// the mixed forms on the tensor cores: the split stage input (planes), then
+// persistent CTAs over the 128-element tiles
 int launch_umma(hgg_handle *h, const StageIOT<float> &io) {
     const int kind = h->precision == HGG_PRECISION_BF16X3 ? kUmmaBF16 : kUmmaTF32;
     const UmmaShape sh = umma_shape(h->lin_R, h->lin_slots, kind);
-    UmmaArgs a{h->d_umma_img, h->d_umma_tile_elems, h->d_umma_tile_mats, h->d_lin_nbr, h->umma_tiles, h->lin_mats,
-               kUmmaPolls};
+    UmmaArgs a{h->d_umma_img, h->d_umma_planes, h->d_umma_tile_elems, h->d_umma_tile_mats, h->d_lin_nbr,
+               h->umma_tiles, h->lin_mats, kUmmaPolls};
     const size_t smem = umma_smem(sh);
     const unsigned grid = (unsigned)std::min<int64_t>(h->umma_tiles, h->num_sms);
-    auto go = [&](auto kc, auto nc) {
-        constexpr int K = decltype(kc)::value, NIN = decltype(nc)::value;
-        cudaFuncSetAttribute(linear_umma_stage<K, NIN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        linear_umma_stage<K, NIN><<<grid, kUmmaThreads, smem, h->stream>>>(io, a, sh);
-    };
+    const int64_t chunks = h->op.nE * (sh.KP * sh.es / 16);
+    const unsigned pgrid = (unsigned)std::min<int64_t>((chunks + 255) / 256, (int64_t)h->num_sms * 8);
     // vector loads need 16-byte aligned rows (R a multiple of 4) and at most one stage-input vector
     const int nin = (h->lin_R % 4 == 0 && io.nin <= 1) ? io.nin : -1;
+    auto planes = [&](auto kc, auto nc) {
+        constexpr int K = decltype(kc)::value, NIN = decltype(nc)::value;
+        umma_planes<K, NIN><<<pgrid, 256, 0, h->stream>>>(io, h->d_umma_planes, sh.R, sh.KP);
+    };
+    auto tiles = [&](auto kc) {
+        constexpr int K = decltype(kc)::value;
+        cudaFuncSetAttribute(linear_umma_stage<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        linear_umma_stage<K><<<grid, kUmmaThreads, smem, h->stream>>>(io, a, sh);
+    };
     using I0 = std::integral_constant<int, 0>;
     using I1 = std::integral_constant<int, 1>;
     using IM = std::integral_constant<int, -1>;
     using KT32 = std::integral_constant<int, kUmmaTF32>;
     using KB16 = std::integral_constant<int, kUmmaBF16>;
     if (kind == kUmmaTF32) {
-        if (nin == 0) go(KT32{}, I0{});
-        else if (nin == 1) go(KT32{}, I1{});
-        else go(KT32{}, IM{});
+        if (nin == 0) planes(KT32{}, I0{});
+        else if (nin == 1) planes(KT32{}, I1{});
+        else planes(KT32{}, IM{});
+        tiles(KT32{});
     } else {
-        if (nin == 0) go(KB16{}, I0{});
-        else if (nin == 1) go(KB16{}, I1{});
-        else go(KB16{}, IM{});
+        if (nin == 0) planes(KB16{}, I0{});
+        else if (nin == 1) planes(KB16{}, I1{});
+        else planes(KB16{}, IM{});
+        tiles(KB16{});
     }
+    h->launches++;  // the planes launch (the tile launch is counted by the caller)
     return 0;
 }
 
