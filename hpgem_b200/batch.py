@@ -63,3 +63,30 @@ class Batch:
     @property
     def num_classes(self):
         return int(self._lib.hgg_batch_num_classes(self._raw))
+
+    KINDS = {0: "dense", 1: "sum-factorised", 2: "sum-factorised slices", 3: "stored-matrix tiles",
+             4: "tensor-core tiles"}
+
+    def class_info(self):
+        """One dict per kernel class with members: kernel kind, shape, dim, order, physics,
+        precision, stages, members, elements, coefficients."""
+        import numpy as np
+        out = []
+        for i in range(self.num_classes):
+            v = np.zeros(10, dtype=np.int64)
+            _native.check_batch(self._lib.hgg_batch_class_info(self._raw, i, ctypes.c_void_p(v.ctypes.data)),
+                                self._raw)
+            out.append(dict(kind=self.KINDS.get(int(v[0]), int(v[0])), shape=int(v[1]), dim=int(v[2]),
+                            order=int(v[3]), physics=int(v[4]), precision=int(v[5]), stages=int(v[6]),
+                            members=int(v[7]), elements=int(v[8]), coefficients=int(v[9])))
+        return out
+
+    def profile_step(self):
+        """One step, class after class, each timed with CUDA events: ms per class (the order
+        of class_info)."""
+        import numpy as np
+        n = self.num_classes
+        ms = np.zeros(max(n, 1))
+        _native.check_batch(self._lib.hgg_batch_profile_step(self._raw, ctypes.c_void_p(ms.ctypes.data), n),
+                            self._raw)
+        return ms[:n]

@@ -21,6 +21,7 @@
 // fastest is cached per (class, size bucket) for the life of the process.
 #pragma once
 
+#include <cstring>
 #include <map>
 #include <mutex>
 #include <tuple>
@@ -187,6 +188,13 @@ __global__ void batch_advance(int *parity, int *remaining, int cap) {
     }
 }
 
+// a member's counters when it joins (kernel arguments are copied at launch, so the
+// host issues the change without waiting for the stream)
+__global__ void batch_set_slot(int *parity, int *remaining, int slot, int nsteps) {
+    parity[slot] = 0;
+    remaining[slot] = nsteps;
+}
+
 }  // namespace hgg
 
 namespace {
@@ -213,6 +221,12 @@ struct BatchClass {
     int64_t *d_total = nullptr;
     int64_t total_blocks = 0;
     int64_t total_elements = 0;
+    // pinned staging of the table uploads, two buffers used in turn: an upload only waits
+    // for the copy issued from the same buffer two uploads earlier, never for the stream
+    unsigned char *h_up[2] = {nullptr, nullptr};
+    cudaEvent_t up_done[2] = {nullptr, nullptr};
+    int up_next = 0;
+    size_t up_bytes = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t done = nullptr;
 };
@@ -385,18 +399,41 @@ int upload_class(hgg_batch *b, BatchClass &c) {
         c.total_blocks += item_blocks(c, b->handles[slot]);
         c.total_elements += b->handles[slot]->op.nE;
     }
+    // layout of a staging buffer: the S item arrays, then n and the block total
+    const size_t items = c.item_bytes * (size_t)b->cap;
+    const size_t need = items * c.S + 16;
+    const int u = c.up_next;
+    c.up_next ^= 1;
+    if (!c.h_up[u] || c.up_bytes < need) {
+        HGG_BCUDA(b, cudaStreamSynchronize(b->stream));  // both staging buffers idle before a resize
+        for (int i = 0; i < 2; ++i) {
+            if (c.h_up[i]) cudaFreeHost(c.h_up[i]);
+            c.h_up[i] = nullptr;
+            HGG_BCUDA(b, cudaHostAlloc((void **)&c.h_up[i], need, cudaHostAllocDefault));
+        }
+        c.up_bytes = need;
+    } else if (c.up_done[u]) {
+        HGG_BCUDA(b, cudaEventSynchronize(c.up_done[u]));  // the copy from this buffer two uploads ago
+    }
+    if (!c.up_done[u]) HGG_BCUDA(b, cudaEventCreateWithFlags(&c.up_done[u], cudaEventDisableTiming));
+    unsigned char *stage = c.h_up[u];
     std::vector<unsigned char> buf;
     for (int st = 0; st < c.S; ++st) {
         if (c.mixed) fill_items<float>(b, c, st, buf);
         else fill_items<double>(b, c, st, buf);
-        if (!buf.empty())
-            HGG_BCUDA(b, cudaMemcpyAsync(c.d_items[st], buf.data(), buf.size(), cudaMemcpyHostToDevice, b->stream));
+        if (!buf.empty()) {
+            std::memcpy(stage + items * st, buf.data(), buf.size());
+            HGG_BCUDA(b, cudaMemcpyAsync(c.d_items[st], stage + items * st, buf.size(), cudaMemcpyHostToDevice,
+                                         b->stream));
+        }
     }
+    unsigned char *tail = stage + items * c.S;
     const int n = (int)c.slots.size();
-    HGG_BCUDA(b, cudaMemcpyAsync(c.d_n, &n, sizeof(int), cudaMemcpyHostToDevice, b->stream));
-    HGG_BCUDA(b, cudaMemcpyAsync(c.d_total, &c.total_blocks, sizeof(int64_t), cudaMemcpyHostToDevice, b->stream));
-    // the host buffers above are reused: wait for the copies
-    HGG_BCUDA(b, cudaStreamSynchronize(b->stream));
+    std::memcpy(tail, &c.total_blocks, sizeof(int64_t));
+    std::memcpy(tail + 8, &n, sizeof(int));
+    HGG_BCUDA(b, cudaMemcpyAsync(c.d_total, tail, sizeof(int64_t), cudaMemcpyHostToDevice, b->stream));
+    HGG_BCUDA(b, cudaMemcpyAsync(c.d_n, tail + 8, sizeof(int), cudaMemcpyHostToDevice, b->stream));
+    HGG_BCUDA(b, cudaEventRecord(c.up_done[u], b->stream));
     return 0;
 }
 
@@ -638,19 +675,20 @@ void release_batch_graph(hgg_batch *b) {
     }
 }
 
-// tables of the classes whose members changed, autotuning of classes with
-// enough work and no tuned shape for their size, and a new capture of one step
-// only when the launch shapes changed
+// tables of the classes whose members changed (an emptied class gets n = 0, so a graph
+// that still launches it finds no work), autotuning of classes with enough work and no
+// tuned shape for their size, and a new capture of one step only when a class with
+// members is missing from the captured step or its launch shape changed
 int prepare_batch(hgg_batch *b) {
     if (!b->dirty && b->graph) return 0;
     bool counters_read = false;
     for (auto &c : b->classes) {
-        if (c.slots.empty()) continue;
         if (c.table_dirty) {
             int rc = upload_class(b, c);
             if (rc) return rc;
             c.table_dirty = false;
         }
+        if (c.slots.empty()) continue;
         // tuning launches stage 1 of the members (every member must have steps left for it
         // to run); a one-stage tableau's first stage is its final update, so it is not tuned;
         // classes with less than two blocks per SM keep the default shape
@@ -672,14 +710,20 @@ int prepare_batch(hgg_batch *b) {
         }
     }
     std::vector<int> sig;
+    bool covered = b->graph != nullptr;
     for (size_t i = 0; i < b->classes.size(); ++i) {
         const auto &c = b->classes[i];
         if (c.slots.empty()) continue;
         sig.push_back((int)i);
         sig.push_back(c.epb);
         sig.push_back(c.ctas_per_sm);
+        bool found = false;
+        for (size_t j = 0; j + 2 < b->graph_sig.size(); j += 3)
+            found = found || (b->graph_sig[j] == (int)i && b->graph_sig[j + 1] == c.epb &&
+                              b->graph_sig[j + 2] == c.ctas_per_sm);
+        covered = covered && found;
     }
-    if (b->graph && sig == b->graph_sig) {
+    if (covered) {
         b->dirty = false;
         return 0;
     }
@@ -707,10 +751,14 @@ int prepare_batch(hgg_batch *b) {
     return 0;
 }
 
+// kernels of one captured step: each class in it launches its S stages (tensor-core
+// classes also form the split stage input before each stage), then the counters advance
 int launches_per_step(const hgg_batch *b) {
     int n = 1;
-    for (auto &c : b->classes)
-        if (!c.slots.empty()) n += c.S;
+    for (size_t j = 0; j < b->graph_sig.size(); j += 3) {
+        const BatchClass &c = b->classes[b->graph_sig[j]];
+        n += c.kind == KIND_UMMA ? 2 * c.S : c.S;
+    }
     return n;
 }
 
@@ -721,6 +769,10 @@ void destroy_batch(hgg_batch *b) {
     for (auto &c : b->classes) {
         if (c.stream) cudaStreamSynchronize(c.stream);
         for (void *p : c.d_items) cudaFree(p);
+        for (int i = 0; i < 2; ++i) {
+            if (c.h_up[i]) cudaFreeHost(c.h_up[i]);
+            if (c.up_done[i]) cudaEventDestroy(c.up_done[i]);
+        }
         cudaFree(c.d_n);
         cudaFree(c.d_total);
         if (c.done) cudaEventDestroy(c.done);
@@ -732,6 +784,24 @@ void destroy_batch(hgg_batch *b) {
     if (b->fork) cudaEventDestroy(b->fork);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
+}
+
+// takes the member of `slot` out of the batch, given the parity of its buffers after its
+// last step: host bookkeeping, and a reset of its counters ordered after the steps already
+// issued (no wait for the stream); the tables are rewritten before the next step
+int remove_member(hgg_batch *b, int slot, int parity) {
+    hgg_handle *h = b->handles[slot];
+    h->cur = parity ? 1 - b->base[slot] : b->base[slot];
+    BatchClass &c = b->classes[b->cls[slot]];
+    c.slots.erase(std::find(c.slots.begin(), c.slots.end(), slot));
+    c.table_dirty = true;
+    b->handles[slot] = nullptr;
+    b->cls[slot] = -1;
+    b->remaining_host[slot] = 0;
+    batch_set_slot<<<1, 1, 0, b->stream>>>(b->d_parity, b->d_remaining, slot, 0);
+    HGG_BCUDA(b, cudaGetLastError());
+    b->dirty = true;
+    return 0;
 }
 
 }  // namespace
@@ -837,11 +907,10 @@ int hgg_batch_add(hgg_batch *b, hgg_handle *h, double dt, int32_t nsteps, int32_
     b->cls[free_slot] = ci;
     b->remaining_host[free_slot] = nsteps;
     b->parity_host[free_slot] = 0;
-    const int zero = 0;
-    HGG_BCUDA(b, cudaMemcpyAsync(b->d_parity + free_slot, &zero, sizeof(int), cudaMemcpyHostToDevice, b->stream));
-    HGG_BCUDA(b, cudaMemcpyAsync(b->d_remaining + free_slot, &b->remaining_host[free_slot], sizeof(int),
-                                 cudaMemcpyHostToDevice, b->stream));
-    HGG_BCUDA(b, cudaStreamSynchronize(b->stream));
+    // ordered after every step already issued, in which the slot is free or its
+    // previous member has no steps left
+    batch_set_slot<<<1, 1, 0, b->stream>>>(b->d_parity, b->d_remaining, free_slot, nsteps);
+    HGG_BCUDA(b, cudaGetLastError());
     b->dirty = true;
     *slot = free_slot;
     return 0;
@@ -851,19 +920,7 @@ int hgg_batch_remove(hgg_batch *b, int32_t slot) {
     if (!b || slot < 0 || slot >= b->cap || !b->handles[slot]) return bfail(b, HGG_ERR_INVALID, "bad slot");
     int rc = read_counters(b);
     if (rc) return rc;
-    hgg_handle *h = b->handles[slot];
-    h->cur = b->parity_host[slot] ? 1 - b->base[slot] : b->base[slot];
-    BatchClass &c = b->classes[b->cls[slot]];
-    c.slots.erase(std::find(c.slots.begin(), c.slots.end(), slot));
-    c.table_dirty = true;
-    b->handles[slot] = nullptr;
-    b->cls[slot] = -1;
-    b->remaining_host[slot] = 0;
-    const int zero = 0;
-    HGG_BCUDA(b, cudaMemcpyAsync(b->d_remaining + slot, &zero, sizeof(int), cudaMemcpyHostToDevice, b->stream));
-    HGG_BCUDA(b, cudaStreamSynchronize(b->stream));
-    b->dirty = true;
-    return 0;
+    return remove_member(b, slot, b->parity_host[slot]);
 }
 
 int hgg_batch_step(hgg_batch *b, int32_t nsteps) {
@@ -911,6 +968,58 @@ int32_t hgg_batch_num_classes(const hgg_batch *b) {
     int n = 0;
     for (auto &c : b->classes) n += !c.slots.empty();
     return n;
+}
+
+int hgg_batch_class_info(const hgg_batch *b, int32_t i, int64_t *info10) {
+    if (!b || !info10) return HGG_ERR_INVALID;
+    int k = -1;
+    for (size_t j = 0; j < b->classes.size(); ++j) {
+        if (b->classes[j].slots.empty()) continue;
+        if (++k != i) continue;
+        const BatchClass &c = b->classes[j];
+        int64_t dofs = 0, elements = 0;
+        for (int slot : c.slots) {
+            const hgg_handle *h = b->handles[slot];
+            dofs += h->N;
+            elements += h->op.nE;
+        }
+        const int64_t v[10] = {c.kind, c.shape, c.dim, c.order, c.physics, c.precision,
+                               c.S, (int64_t)c.slots.size(), elements, dofs};
+        std::copy(v, v + 10, info10);
+        return 0;
+    }
+    return HGG_ERR_INVALID;
+}
+
+int hgg_batch_profile_step(hgg_batch *b, double *ms, int32_t n) {
+    if (!b || !ms || n < hgg_batch_num_classes(b)) return bfail(b, HGG_ERR_INVALID, "bad argument");
+    int rc = prepare_batch(b);
+    if (rc) return rc;
+    cudaEvent_t e0, e1;
+    HGG_BCUDA(b, cudaEventCreate(&e0));
+    HGG_BCUDA(b, cudaEventCreate(&e1));
+    int k = 0;
+    for (auto &c : b->classes) {
+        if (c.slots.empty()) continue;
+        cudaEventRecord(e0, b->stream);
+        for (int st = 0; st < c.S; ++st) launch_class_stage(b, c, st, b->stream);
+        cudaEventRecord(e1, b->stream);
+        cudaError_t e = cudaEventSynchronize(e1);
+        if (e != cudaSuccess) {
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            return bfail(b, HGG_ERR_CUDA, std::string("profiled step: ") + cudaGetErrorString(e));
+        }
+        float t = 0.f;
+        cudaEventElapsedTime(&t, e0, e1);
+        ms[k++] = t;
+    }
+    batch_advance<<<(b->cap + 255) / 256, 256, 0, b->stream>>>(b->d_parity, b->d_remaining, b->cap);
+    b->launches++;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    HGG_BCUDA(b, cudaStreamSynchronize(b->stream));
+    return 0;
 }
 
 }  // extern "C"

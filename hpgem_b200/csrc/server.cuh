@@ -5,13 +5,15 @@
 // arrival order by device-memory footprint: a set-up thread reserves the
 // request's footprint against the budget (waiting while it does not fit),
 // builds its handle and projects its initial condition.  The GPU thread owns
-// one hgg_batch: between chunks of steps it adds the requests that are ready
-// and takes out the ones that are done (their solution is copied to the host
-// and their device memory freed, which admits the next ones).  So requests that
-// arrive while others run join the running mix at the next chunk boundary, and
-// every RK stage of all running requests of a kernel class is one launch.  A
-// chunk is the smallest number of steps any running request still needs,
-// capped, so no request idles on the device after its last step.
+// one hgg_batch and keeps two chunks of steps in flight: it issues chunk k+1,
+// then waits for chunk k and reads, from a pinned copy of the batch counters
+// taken at the end of chunk k, which members have no steps left.  Those leave
+// the batch (host bookkeeping and stream-ordered table updates, no wait for the
+// device) and go to a retire thread, which copies their solution back on the
+// handle's own stream into a pinned buffer and frees their device memory, which
+// admits the next requests.  Requests that are ready join before the next chunk
+// is issued.  A chunk is max_chunk steps (fewer when no member needs more);
+// members that finish inside a chunk stay in it without work.
 #pragma once
 
 #include <chrono>
@@ -43,6 +45,8 @@ struct ServerRequest {
     std::string message;
     hgg_handle *h = nullptr;
     int slot = -1;
+    int issued = 0;         // steps issued to the device
+    int64_t join_seq = 0;   // sequence number of the first chunk issued after joining
     int64_t footprint = 0;
     int64_t dofs = 0;
     std::vector<double> result;
@@ -56,20 +60,24 @@ struct hgg_server {
     int64_t budget = 0;
     int max_chunk = 25;
     std::mutex mu;
-    std::condition_variable cv_setup, cv_gpu, cv_done, cv_mem;
-    std::deque<ServerRequest *> queued, ready;
+    std::condition_variable cv_setup, cv_gpu, cv_done, cv_mem, cv_retire;
+    std::deque<ServerRequest *> queued, ready, retiring;
     std::unordered_map<int64_t, std::unique_ptr<ServerRequest>> requests;
     int64_t next_id = 1;
     int64_t reserved = 0;
     bool stopping = false;
+    bool gpu_done = false;  // the GPU thread has ended: the retire thread empties its queue and ends
     std::vector<std::thread> setup_threads;
-    std::thread gpu_thread;
+    std::thread gpu_thread, retire_thread;
     hgg_batch *batch = nullptr;
     std::string err = "no error";
     int gpu_error = 0;
     // counters
     int64_t completed = 0, dof_updates = 0, chunks = 0;
-    double t_step = 0, t_members = 0, t_idle = 0;  // GPU thread: stepping, joining/retiring, waiting
+    // GPU thread: waiting for chunks, membership work (joins, removals, tables,
+    // graph, issuing launches), waiting for work; retire thread busy; device time
+    // of the chunks (CUDA events around each chunk on the batch stream)
+    double t_step = 0, t_members = 0, t_idle = 0, t_retire = 0, t_device = 0;
 };
 
 namespace {
@@ -152,6 +160,11 @@ void setup_loop(hgg_server *s) {
             }
             if (rc) r->message = hgg_last_error(r->h);
             else hgg_set_store_last_stage(r->h, 0);
+            // the batch reads the handle's buffers on its own stream
+            if (rc == 0 && cudaStreamSynchronize(r->h->stream) != cudaSuccess) {
+                rc = HGG_ERR_CUDA;
+                r->message = "set-up copies failed";
+            }
         }
         std::vector<double>().swap(r->u0);
         std::lock_guard<std::mutex> lk(s->mu);
@@ -175,116 +188,225 @@ void setup_loop(hgg_server *s) {
     }
 }
 
-void gpu_loop(hgg_server *s) {
-    cudaSetDevice(s->device);
-    std::vector<ServerRequest *> running;
+// the batch counters after one chunk, copied into pinned memory on the batch stream
+struct ChunkSnapshot {
+    int *host = nullptr;  // parity[cap], remaining[cap], status
+    cudaEvent_t start = nullptr, end = nullptr;
+    int64_t seq = 0;
+};
+
+// a request finished or failed: bookkeeping under the lock
+void finish_request(hgg_server *s, ServerRequest *r, int rc, const std::string &msg) {
+    r->error = rc;
+    if (rc) r->message = msg;
+    r->state = rc ? 5 : 4;
+    r->t_done = now_s();
+    s->reserved -= r->footprint;
+    if (rc == 0) {
+        s->completed++;
+        s->dof_updates += r->dofs * (int64_t)r->nsteps;
+    }
+    s->cv_mem.notify_all();
+    s->cv_done.notify_all();
+}
+
+// every request not finished fails with the device error; the server stops
+void fail_unfinished(hgg_server *s, int rc, const std::string &msg) {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->gpu_error = rc;
+    s->err = msg;
+    for (auto &kv : s->requests) {
+        ServerRequest *r = kv.second.get();
+        if (r->state >= 4) continue;
+        r->error = rc;
+        r->message = msg;
+        r->state = 5;
+        r->t_done = now_s();
+    }
+    s->queued.clear();
+    s->ready.clear();
+    s->stopping = true;
+    s->cv_done.notify_all();
+    s->cv_setup.notify_all();
+    s->cv_mem.notify_all();
+}
+
+void gpu_loop_body(hgg_server *s, ChunkSnapshot *snap) {
+    hgg_batch *b = s->batch;
+    const int cap = b->cap;
+    std::vector<ServerRequest *> member(cap, nullptr);  // by batch slot
+    int n_members = 0;
+    std::deque<int> inflight;  // snapshots of the chunks issued and not yet waited for, oldest first
+    int next_snap = 0;
+    int64_t seq = 0;  // chunks issued
     for (;;) {
+        // 1. the requests that are ready; block only with nothing in the batch
         std::vector<ServerRequest *> joining;
-        const double t_wait0 = now_s();
+        const double t0 = now_s();
         {
             std::unique_lock<std::mutex> lk(s->mu);
-            if (running.empty())
+            if (n_members == 0 && inflight.empty()) {
                 s->cv_gpu.wait(lk, [&] {
                     return !s->ready.empty() || (s->stopping && s->queued.empty() && s->ready.empty());
                 });
-            if (running.empty() && s->ready.empty() && s->stopping) return;
-            while (!s->ready.empty()) {
+                if (s->ready.empty()) return;  // stopping
+            }
+            while (!s->ready.empty() && n_members + (int)joining.size() < cap) {
                 joining.push_back(s->ready.front());
                 s->ready.pop_front();
             }
+            s->t_idle += now_s() - t0;
         }
-        const double t_join0 = now_s();
-        {
-            std::lock_guard<std::mutex> lk(s->mu);
-            s->t_idle += t_join0 - t_wait0;
-        }
+        const double t1 = now_s();
+        // 2. joins: stream-ordered after the chunks in flight
         for (ServerRequest *r : joining) {
             int32_t slot = -1;
-            int rc = hgg_batch_add(s->batch, r->h, r->dt, r->nsteps, &slot);
-            std::lock_guard<std::mutex> lk(s->mu);
+            int rc = hgg_batch_add(b, r->h, r->dt, r->nsteps, &slot);
             if (rc) {
-                r->error = rc;
-                r->message = hgg_batch_last_error(s->batch);
-                r->state = 5;
-                r->t_done = now_s();
+                const std::string msg = hgg_batch_last_error(b);
                 hgg_destroy(r->h);
                 r->h = nullptr;
-                s->reserved -= r->footprint;
-                s->cv_mem.notify_all();
-                s->cv_done.notify_all();
+                std::lock_guard<std::mutex> lk(s->mu);
+                finish_request(s, r, rc, msg);
                 continue;
             }
             r->slot = slot;
+            r->issued = 0;
+            r->join_seq = seq;
+            member[slot] = r;
+            n_members++;
+            std::lock_guard<std::mutex> lk(s->mu);
             r->state = 3;
             r->t_start = now_s();
-            running.push_back(r);
         }
-        if (running.empty()) continue;
-        int chunk = s->max_chunk;
-        for (ServerRequest *r : running) {
-            const int left = hgg_batch_remaining(s->batch, r->slot);
-            if (left > 0) chunk = std::min(chunk, left);
+        // 3. issue the next chunk: the most steps any member still needs, capped
+        int chunk = 0;
+        for (int i = 0; i < cap; ++i)
+            if (member[i]) chunk = std::max(chunk, member[i]->nsteps - member[i]->issued);
+        chunk = std::min(chunk, s->max_chunk);
+        if (chunk > 0) {
+            ChunkSnapshot &sn = snap[next_snap];
+            cudaEventRecord(sn.start, b->stream);
+            int rc = hgg_batch_step(b, chunk);
+            if (rc) return fail_unfinished(s, rc, hgg_batch_last_error(b));
+            cudaMemcpyAsync(sn.host, b->d_parity, sizeof(int) * cap, cudaMemcpyDeviceToHost, b->stream);
+            cudaMemcpyAsync(sn.host + cap, b->d_remaining, sizeof(int) * cap, cudaMemcpyDeviceToHost, b->stream);
+            cudaMemcpyAsync(sn.host + 2 * cap, b->d_status, sizeof(int), cudaMemcpyDeviceToHost, b->stream);
+            cudaEventRecord(sn.end, b->stream);
+            sn.seq = seq++;
+            inflight.push_back(next_snap);
+            next_snap = (next_snap + 1) % 3;
+            for (int i = 0; i < cap; ++i)
+                if (member[i]) member[i]->issued = std::min(member[i]->nsteps, member[i]->issued + chunk);
+        } else if (inflight.empty()) {
+            // every member's steps are issued and waited for, yet a member remains
+            return fail_unfinished(s, HGG_ERR_INVALID, "serving loop: a member has no steps left to issue");
         }
-        chunk = std::max(chunk, 1);
-        const double t_step0 = now_s();
-        int rc = hgg_batch_step(s->batch, chunk);
-        if (rc == 0) rc = hgg_batch_synchronize(s->batch);
-        const double t_step1 = now_s();
+        const double t2 = now_s();
         {
             std::lock_guard<std::mutex> lk(s->mu);
-            s->t_members += t_step0 - t_join0;
-            s->t_step += t_step1 - t_step0;
+            s->t_members += t2 - t1;
+            if (chunk > 0) s->chunks++;
         }
-        if (rc) {
-            std::lock_guard<std::mutex> lk(s->mu);
-            s->gpu_error = rc;
-            s->err = hgg_batch_last_error(s->batch);
-            // every request not finished fails with the device error
-            for (auto &kv : s->requests) {
-                ServerRequest *r = kv.second.get();
-                if (r->state >= 4) continue;
-                r->error = rc;
-                r->message = s->err;
-                r->state = 5;
-                r->t_done = now_s();
-            }
-            s->queued.clear();
-            s->ready.clear();
-            s->stopping = true;
-            s->cv_done.notify_all();
-            s->cv_setup.notify_all();
-            s->cv_mem.notify_all();
-            return;
+        // 4. wait for the oldest chunk once two are in flight (or nothing more can be issued)
+        if (inflight.size() < 2 && chunk > 0) continue;
+        ChunkSnapshot &sn = snap[inflight.front()];
+        inflight.pop_front();
+        cudaError_t e = cudaEventSynchronize(sn.end);
+        const double t3 = now_s();
+        if (e != cudaSuccess) return fail_unfinished(s, HGG_ERR_CUDA, std::string("chunk: ") + cudaGetErrorString(e));
+        const int status = sn.host[2 * cap];
+        if (status) return fail_unfinished(s, HGG_ERR_DEVICE, hgg::status_message(status));
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, sn.start, sn.end);
+        // 5. members with no steps left after that chunk leave the batch for the retire thread
+        std::vector<ServerRequest *> done;
+        for (int i = 0; i < cap; ++i) {
+            ServerRequest *r = member[i];
+            if (!r || r->join_seq > sn.seq || sn.host[cap + i] != 0) continue;
+            int rc = remove_member(b, i, sn.host[i]);
+            if (rc) return fail_unfinished(s, rc, hgg_batch_last_error(b));
+            member[i] = nullptr;
+            n_members--;
+            done.push_back(r);
         }
-        s->chunks++;
-        std::vector<ServerRequest *> still;
-        for (ServerRequest *r : running) {
-            if (hgg_batch_remaining(s->batch, r->slot) > 0) {
-                still.push_back(r);
-                continue;
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->t_step += t3 - t2;
+        s->t_members += now_s() - t3;
+        s->t_device += 1e-3 * ms;
+        for (ServerRequest *r : done) s->retiring.push_back(r);
+        if (!done.empty()) s->cv_retire.notify_one();
+    }
+}
+
+void gpu_loop(hgg_server *s) {
+    cudaSetDevice(s->device);
+    ChunkSnapshot snap[3];
+    bool ok = true;
+    for (auto &sn : snap) {
+        ok = ok && cudaHostAlloc((void **)&sn.host, sizeof(int) * (2 * s->batch->cap + 1), cudaHostAllocDefault) ==
+                       cudaSuccess;
+        ok = ok && cudaEventCreate(&sn.start) == cudaSuccess && cudaEventCreate(&sn.end) == cudaSuccess;
+    }
+    if (ok) gpu_loop_body(s, snap);
+    else fail_unfinished(s, HGG_ERR_CUDA, "serving loop: pinned counters or events could not be created");
+    cudaStreamSynchronize(s->batch->stream);
+    for (auto &sn : snap) {
+        if (sn.host) cudaFreeHost(sn.host);
+        if (sn.start) cudaEventDestroy(sn.start);
+        if (sn.end) cudaEventDestroy(sn.end);
+    }
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->gpu_done = true;
+    s->cv_retire.notify_all();
+}
+
+// copies finished solutions back (the handle's own stream, a pinned buffer) and frees
+// their device memory, off the GPU thread
+void retire_loop(hgg_server *s) {
+    cudaSetDevice(s->device);
+    double *pinned = nullptr;
+    size_t pinned_n = 0;
+    for (;;) {
+        std::vector<ServerRequest *> work;
+        {
+            std::unique_lock<std::mutex> lk(s->mu);
+            s->cv_retire.wait(lk, [&] { return !s->retiring.empty() || s->gpu_done; });
+            if (s->retiring.empty()) break;
+            work.assign(s->retiring.begin(), s->retiring.end());
+            s->retiring.clear();
+        }
+        for (ServerRequest *r : work) {
+            const double t0 = now_s();
+            bool failed_already;
+            {
+                std::lock_guard<std::mutex> lk(s->mu);
+                failed_already = r->state >= 4;
             }
-            int rr = hgg_batch_remove(s->batch, r->slot);
-            if (rr == 0) {
-                r->result.resize((size_t)hgg_vector_length(r->h));
-                rr = hgg_get_state(r->h, 0, r->result.data());
+            int rc = 0;
+            std::string msg;
+            if (!failed_already) {
+                const size_t n = (size_t)hgg_vector_length(r->h);
+                if (n > pinned_n) {
+                    if (pinned) cudaFreeHost(pinned);
+                    pinned = nullptr;
+                    pinned_n = 0;
+                    if (cudaHostAlloc((void **)&pinned, sizeof(double) * n, cudaHostAllocDefault) == cudaSuccess)
+                        pinned_n = n;
+                }
+                r->result.resize(n);
+                rc = hgg_get_state(r->h, 0, pinned ? pinned : r->result.data());
+                if (rc == 0 && pinned) std::memcpy(r->result.data(), pinned, sizeof(double) * n);
+                if (rc) msg = hgg_last_error(r->h);
             }
             hgg_destroy(r->h);
             r->h = nullptr;
             std::lock_guard<std::mutex> lk(s->mu);
-            r->error = rr;
-            if (rr) r->message = hgg_batch_last_error(s->batch);
-            r->state = rr ? 5 : 4;
-            r->t_done = now_s();
-            s->reserved -= r->footprint;
-            s->completed++;
-            s->dof_updates += r->dofs * (int64_t)r->nsteps;
-            s->cv_mem.notify_all();
-            s->cv_done.notify_all();
+            if (!failed_already) finish_request(s, r, rc, msg);
+            s->t_retire += now_s() - t0;
         }
-        running.swap(still);
-        std::lock_guard<std::mutex> lk(s->mu);
-        s->t_members += now_s() - t_step1;
     }
+    if (pinned) cudaFreeHost(pinned);
 }
 
 int sfail(hgg_server *s, int code, const std::string &msg) {
@@ -319,8 +441,11 @@ int hgg_server_start(int64_t budget_bytes, int32_t max_chunk, int32_t setup_thre
         delete s;
         return rc;
     }
+    // fixed launch shapes: timing candidates would wait for the chunks in flight
+    hgg_batch_set_autotune(s->batch, 0);
     for (int i = 0; i < setup_threads; ++i) s->setup_threads.emplace_back(setup_loop, s);
     s->gpu_thread = std::thread(gpu_loop, s);
+    s->retire_thread = std::thread(retire_loop, s);
     *out = s;
     return 0;
 }
@@ -436,14 +561,17 @@ int hgg_server_stats(hgg_server *s, int64_t *stats4) {
     return 0;
 }
 
-// GPU-thread seconds: stepping (launches and the wait for them), joining and
-// retiring solves (tables, graph, copies back, frees), waiting for work
-int hgg_server_timing(hgg_server *s, double *t3) {
-    if (!s || !t3) return sfail(s, HGG_ERR_INVALID, "null argument");
+// seconds: GPU thread waiting for chunks, GPU thread membership work (joins,
+// removals, tables, graph, issuing launches), GPU thread waiting for work, retire
+// thread (copies back, frees), device time of the chunks
+int hgg_server_timing(hgg_server *s, double *t5) {
+    if (!s || !t5) return sfail(s, HGG_ERR_INVALID, "null argument");
     std::lock_guard<std::mutex> lk(s->mu);
-    t3[0] = s->t_step;
-    t3[1] = s->t_members;
-    t3[2] = s->t_idle;
+    t5[0] = s->t_step;
+    t5[1] = s->t_members;
+    t5[2] = s->t_idle;
+    t5[3] = s->t_retire;
+    t5[4] = s->t_device;
     return 0;
 }
 
@@ -472,6 +600,7 @@ int hgg_server_stop(hgg_server *s) {
     s->cv_mem.notify_all();
     for (auto &t : s->setup_threads) t.join();
     s->gpu_thread.join();
+    s->retire_thread.join();
     const int rc = s->gpu_error;
     hgg_batch_destroy(s->batch);
     for (auto &kv : s->requests)

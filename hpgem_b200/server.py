@@ -3,7 +3,9 @@
 Requests are admitted in arrival order while their device footprint fits the
 budget, keep their state on the device, and advance together with every other
 running request (one launch per RK stage and kernel class); requests that
-arrive while others run join at the next chunk boundary.
+arrive while others run join at the next chunk boundary.  The GPU thread keeps
+two chunks of steps in flight; finished solutions are copied back and freed on
+a retire thread.
 """
 import ctypes
 import threading
@@ -86,11 +88,11 @@ class Server:
     def stats(self):
         st = np.zeros(4, dtype=np.int64)
         self._check(self._lib.hgg_server_stats(self._raw, ctypes.c_void_p(st.ctypes.data)))
-        t = np.zeros(3)
+        t = np.zeros(5)
         self._check(self._lib.hgg_server_timing(self._raw, ctypes.c_void_p(t.ctypes.data)))
         return dict(completed=int(st[0]), dof_updates=int(st[1]), chunks=int(st[2]), reserved_bytes=int(st[3]),
                     gpu_thread_step_s=float(t[0]), gpu_thread_members_s=float(t[1]),
-                    gpu_thread_idle_s=float(t[2]))
+                    gpu_thread_idle_s=float(t[2]), retire_thread_s=float(t[3]), device_chunk_s=float(t[4]))
 
     def stop(self):
         if self._raw:

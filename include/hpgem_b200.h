@@ -465,6 +465,18 @@ int hgg_batch_set_autotune(hgg_batch *b, int32_t enable);
 int64_t hgg_batch_launch_count(const hgg_batch *b);
 int32_t hgg_batch_num_classes(const hgg_batch *b);
 
+/* Kernel class i (0 .. hgg_batch_num_classes - 1, classes with members):
+ * info10 = kind (0 matrix-free dense, 1 sum-factorised, 2 sum-factorised slices,
+ * 3 stored-matrix tiles, 4 tensor-core tiles), shape, dim, order, physics,
+ * precision (0 FP64, 1 FP32-mixed, 2 split-BF16), stages, members, elements,
+ * coefficients. */
+int hgg_batch_class_info(const hgg_batch *b, int32_t i, int64_t *info10);
+
+/* One step of every member with steps left, class after class on the batch
+ * stream, each class's stages timed with CUDA events: ms[i] for class i (the
+ * order of hgg_batch_class_info).  Synchronous; for profiling the mix. */
+int hgg_batch_profile_step(hgg_batch *b, double *ms, int32_t n);
+
 /* ---- serving loop ------------------------------------------------------------
  * No counterpart in the reference.  A server admits solves (a Preprocessor
  * structured description, order, physics, parameters, tableau, precision,
@@ -474,8 +486,9 @@ int32_t hgg_batch_num_classes(const hgg_batch *b);
  * running solves of a kernel class is one launch); solves that arrive while
  * others run join at the next chunk boundary, and a finished solve's memory
  * admits the next.  Set-up (host descriptor, handle, projection) runs on
- * `setup_threads` threads beside the GPU thread.  submit/poll/release/times/
- * stats are thread-safe. */
+ * `setup_threads` threads beside the GPU thread; the GPU thread keeps two chunks
+ * of steps in flight, and a retire thread copies finished solutions back and
+ * frees their memory.  submit/poll/release/times/stats are thread-safe. */
 typedef struct hgg_server hgg_server;
 
 /* Initial condition callback: values[n_points][n_vars] at points xyz[n_points][dim]
@@ -511,9 +524,12 @@ int hgg_server_times(hgg_server *s, int64_t id, double *t4);
 /* Completed solves, their DoF-updates, chunks stepped, device bytes reserved now. */
 int hgg_server_stats(hgg_server *s, int64_t *stats4);
 
-/* GPU-thread seconds so far: stepping (launches and the wait for them),
- * joining and retiring solves (tables, graph, copies back, frees), idle. */
-int hgg_server_timing(hgg_server *s, double *t3);
+/* Seconds so far: [0] the GPU thread waiting for chunks of steps, [1] the GPU
+ * thread's membership work (joins, removals, table uploads, graph captures,
+ * issuing launches), [2] the GPU thread waiting for work, [3] the retire thread
+ * (solutions copied back, device memory freed), [4] device time of the chunks
+ * (CUDA events on the batch stream). */
+int hgg_server_timing(hgg_server *s, double *t5);
 
 const char *hgg_server_last_error(hgg_server *s);
 

@@ -95,3 +95,25 @@ def test_request_larger_than_the_budget_fails_cleanly():
         server.poll(rid, wait=True)
     assert ex.value.code == -4  # HGG_ERR_NOMEM
     server.stop()
+
+
+def test_more_requests_than_slots_wait_for_a_slot_and_mixed_form():
+    """A server with 3 slots and 10 requests: the requests beyond the slots wait until
+    members leave (none fails); FP32-mixed solves equal the same solves alone in the
+    mixed form to the FP32 accumulation error."""
+    specs = small_stream(10, seed=14)
+    server = hpgem_b200.Server(budget_bytes=2 << 30, max_chunk=4, setup_threads=2, capacity=3)
+    ids = []
+    for spec in specs:
+        fn, nv = initial(spec)
+        ids.append(server.submit(description(spec), spec["order"], spec["physics"], spec["params"], spec["dt"],
+                                 spec["steps"], initial=fn, n_vars=nv, precision=_native.PRECISION_FP32))
+    results = [server.poll(rid, wait=True) for rid in ids]
+    stats = server.stats()
+    server.stop()
+    assert stats["completed"] == len(specs)
+    assert stats["device_chunk_s"] > 0 and stats["retire_thread_s"] > 0
+    for spec, (done, u, _) in zip(specs, results):
+        s = workloads.make_solver(spec, precision=_native.PRECISION_FP32)
+        s.computeTimeSteps(0.0, spec["dt"], spec["steps"])
+        assert done and rel_err(u, s.getTimeIntegrationVector(0).reshape(-1)) < 1e-5, spec["id"]
