@@ -363,9 +363,21 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_batched:
         line["tet_wave"] = run_tet_wave(args, stream)
         line["linear"] = run_linear(args, stream)
+        # split-BF16 of this mesh: the matrix-free handle with HGG_PRECISION_BF16X3 folds its
+        # operator into the per-element matrices the stored-matrix leg runs on tcgen05
+        bf = dict(line["linear"]["forms"]["split_bf16"])
+        bf["measured_as"] = ("the linear leg's split-BF16 form (the same operator, folded; same mesh, "
+                             "bump and dt)")
+        line["forms"]["split_bf16"] = bf
         line["batched"] = run_batched_forms(args, stream)
+        line["batched"]["forms"]["split_bf16"] = {
+            "unavailable": "split-BF16 runs only on tiles of 128 elements with equal matrices; most of the "
+                           "512 meshes (8^2..128^2 cells) do not form them"}
     if rank == 0 and world == 1 and not args.no_served:
         line["served"] = run_served_legs(args)
+        line["served"]["forms"]["split_bf16"] = {
+            "unavailable": "split-BF16 needs tiles of 128 elements with equal matrices; the stream's "
+                           "small meshes (from 1e3 DoF) do not form them"}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, sample = cpu_sample_rate()
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
@@ -465,7 +477,8 @@ def run_tet_wave(args, stream):
     d = hpgem_b200.structured_description([32, 32, 32], [0, 0, 0], [1, 1, 1], True, True)
     out = {}
     sols = {}
-    for name, prec, flux in (("fp64", 0, "upwind"), ("fp32_mixed", 1, "upwind"), ("fp64_central", 0, "central")):
+    for name, prec, flux in (("fp64", 0, "upwind"), ("fp32_mixed", 1, "upwind"), ("split_bf16", 2, "upwind"),
+                             ("fp64_central", 0, "central")):
         s = hpgem_b200.AcousticWave(3, 2, c_inv=1.0, tableau="RK4_4", precision=prec, flux=flux).readMesh(d)
         h = s.handle
         h.set_stream(stream.cuda_stream)
@@ -484,18 +497,28 @@ def run_tet_wave(args, stream):
         n = h.vector_length
         sols[name] = (s, s.getTimeIntegrationVector(0))
         out[name] = {"value": n / (ms / 1e3), "unit": UNIT, "dof": n, "ms_per_step": ms, "steps": steps,
-                     "gpu_launches": int(h.launch_count - launches0),
+                     "gpu_launches": int(h.launch_count - launches0), "kernel": h.kernel_kind,
                      "finite": bool(np.isfinite(sols[name][1]).all())}
     s64, u64 = sols["fp64"]
-    u32 = sols["fp32_mixed"][1]
-    out["fp32_mixed"]["l2_distance_to_fp64"] = s64.l2Distance(u32, u64)
-    out["fp32_mixed"]["max_rel_coef_diff_vs_fp64"] = float(np.abs(u32 - u64).max() / np.abs(u64).max())
+    for name in ("fp32_mixed", "split_bf16"):
+        u = sols[name][1]
+        out[name]["l2_distance_to_fp64"] = s64.l2Distance(u, u64)
+        out[name]["max_rel_coef_diff_vs_fp64"] = float(np.abs(u - u64).max() / np.abs(u64).max())
     res = {"workload": "3D acoustic wave, 32^3 x 5 periodic tetrahedra, p = 2, upwind flux, RK4, "
                        "dt = 5e-4, seeded 3-mode pressure, 23 steps", "dtype": "f64",
            "kernel": "dense_group_stage<double,3,4,10> (FP64: 32-element tiles of equal operators, "
-                     "lane = element); dense_stage<float,3,4,1,10> (FP32-mixed: one thread per element row)"}
+                     "lane = element); dense_stage<float,3,4,1,10> (FP32-mixed: one thread per element row); "
+                     "linear_umma_stage (split-BF16: the operator folded into per-element matrices, "
+                     "128-element tiles on tcgen05, FP32 accumulation in tensor memory)"}
     res.update(out["fp64"])
-    res["forms"] = {"fp32_mixed": out["fp32_mixed"]}
+    # roofline of the FP64 kernel: the state an RK4 step must move (stage inputs u and the
+    # previous stage vector, neighbour traces from L2, the stage output; the final update
+    # reads k1..k3 and writes u): 130 bytes per DoF-update, against the measured HBM copy
+    peak, peak_kind = measured_peak_hbm()
+    achieved = 130.0 * res["value"] / 1e9
+    res["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                       "peak_kind": peak_kind, "algorithmic_bytes_per_dof_update": 130}
+    res["forms"] = {"fp32_mixed": out["fp32_mixed"], "split_bf16": out["split_bf16"]}
     res["central_flux_fp64"] = out["fp64_central"]
     return res
 
@@ -536,7 +559,7 @@ def run_linear(args, stream):
     a = [1.0, 0.7, 0.3]
     warm, steps = (args.warmup, args.steps) if args.only else (3, 20)
     out, sols = {}, {}
-    for name, prec in (("fp64", 0), ("fp32_mixed", 1)):
+    for name, prec in (("fp64", 0), ("fp32_mixed", 1), ("split_bf16", 2)):
         t0 = time.time()
         s = hpgem_b200.HpgemAPILinear(3, 3, "advection", advection=a, tableau="RK4_4", precision=prec).readMesh(d)
         setup = time.time() - t0
@@ -578,9 +601,11 @@ def run_linear(args, stream):
     res["roofline"] = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                        "frac": achieved / peak, "peak_kind": "cuBLAS DGEMM 8192^3 measured in this run",
                        "algorithmic_flop_per_dof_update": flop}
-    u32 = sols["fp32_mixed"][1]
-    out["fp32_mixed"]["l2_distance_to_fp64"] = s64.l2Distance(u32, u64)
-    res["forms"] = {"fp32_mixed": out["fp32_mixed"]}
+    for name in ("fp32_mixed", "split_bf16"):
+        u = sols[name][1]
+        out[name]["l2_distance_to_fp64"] = s64.l2Distance(u, u64)
+        out[name]["max_rel_coef_diff_vs_fp64"] = float(np.abs(u - u64).max() / np.abs(u64).max())
+    res["forms"] = {"fp32_mixed": out["fp32_mixed"], "split_bf16": out["split_bf16"]}
     return res
 
 
@@ -593,7 +618,7 @@ def run_served(args, precision=0, n=None, rate=200.0):
 
     specs = workloads.served_requests(n=n or args.served_requests, rate=rate)
     setup_threads = max(2, min(16, (os.cpu_count() or 4) // 2))
-    server = hpgem_b200.Server(budget_bytes=48 << 30, max_chunk=25, setup_threads=setup_threads)
+    server = hpgem_b200.Server(budget_bytes=48 << 30, max_chunk=args.served_chunk, setup_threads=setup_threads)
 
     def desc(sp):
         d = len(sp["cells"])
@@ -633,9 +658,12 @@ def run_served(args, precision=0, n=None, rate=200.0):
             "span_s": span, "dof_updates": stats["dof_updates"], "chunks": stats["chunks"],
             "gpu_thread_s": {"stepping": stats["gpu_thread_step_s"], "joining_retiring": stats["gpu_thread_members_s"],
                              "idle": stats["gpu_thread_idle_s"]},
-            "retire_thread_s": stats["retire_thread_s"], "device_chunk_s": stats["device_chunk_s"],
+            "joining_retiring_parts_s": {"joins": stats["gpu_thread_join_s"],
+                                         "tables_and_captures": stats["gpu_thread_tables_s"]},
+            "retire_thread_s": stats["retire_thread_s"], "retire_copyback_s": stats["retire_copyback_s"],
+            "device_chunk_s": stats["device_chunk_s"],
             "device_busy_frac": stats["device_chunk_s"] / span,
-            "setup_threads": setup_threads, "budget_bytes": 48 << 30,
+            "setup_threads": setup_threads, "budget_bytes": 48 << 30, "steps_per_chunk": args.served_chunk,
             "offered_dof_updates_per_s": sum(workloads.dof(sp) * sp["steps"] for sp in specs)
             / max(specs[-1]["arrival"], 1e-9),
             "timing": "host steady clock, latency = done - submit (set-up, queueing, steps, copy back)"}
@@ -670,6 +698,7 @@ def main():
     ap.add_argument("--no-served", action="store_true", help="skip the served request-stream leg")
     ap.add_argument("--served-requests", type=int, default=2000,
                     help="requests of the seeded stream to serve at 200 requests/s (the stream has 2000)")
+    ap.add_argument("--served-chunk", type=int, default=6, help="the server's steps per chunk")
     ap.add_argument("--sustained-requests", type=int, default=500,
                     help="requests of the same stream served at a sustainable load (0: skip)")
     ap.add_argument("--only", choices=["linear", "tet_wave", "served"],

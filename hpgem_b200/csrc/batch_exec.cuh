@@ -21,6 +21,7 @@
 // fastest is cached per (class, size bucket) for the life of the process.
 #pragma once
 
+#include <cstddef>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -32,6 +33,7 @@ template <typename KT>
 struct DenseItem {
     StageIOT<KT> io[2];  // [parity]: from sol[base] / from sol[1 - base]
     DenseGeom g;
+    const int32_t *tiles;  // the wave on tiles of equal operators: the member's tiles (else null)
     int64_t block0;  // first virtual block
     int slot;
 };
@@ -91,6 +93,23 @@ __global__ void __launch_bounds__(256)
         __syncthreads();  // shared memory of the previous virtual block is free
         if (remaining[slot] <= 0) continue;
         dense_any_body<KT, DIM, NFL, WAVE, NB>(items[i].io[parity[slot]], items[i].g, vb - items[i].block0);
+    }
+}
+
+// the wave on tiles of elements with equal operators (one virtual block per tile)
+template <typename KT, int DIM, int NFL, int NB>
+__global__ void __launch_bounds__(kGroupTile *NB, 1024 / (kGroupTile * NB) > 0 ? 1024 / (kGroupTile * NB) : 1)
+    grouped_wave_tiles(const DenseItem<KT> *items, const int *n_items, const int64_t *total, const int *parity,
+                       const int *remaining) {
+    const int n = *n_items;
+    const int64_t nb = *total;
+    for (int64_t vb = blockIdx.x; vb < nb; vb += gridDim.x) {
+        const int i = find_item(items, n, vb);
+        const int slot = items[i].slot;
+        __syncthreads();
+        if (remaining[slot] <= 0) continue;
+        wave_group_body<KT, DIM, NFL, NB>(items[i].io[parity[slot]], items[i].g, items[i].tiles,
+                                          vb - items[i].block0);
     }
 }
 
@@ -164,19 +183,21 @@ __global__ void __launch_bounds__(kUmmaThreads, 1)
     umma_persistent<KIND>(sh, UmmaGroupedTiles{items, *n_items, *total, parity, remaining}, status);
 }
 
-// the split stage input of every member (blockIdx.y: member)
+// the split stage input of every member (blockIdx.y, then in steps of gridDim.y: member)
 template <int KIND, int NIN>
 __global__ void __launch_bounds__(256)
     grouped_umma_planes(const UmmaItem *items, const int *n_items, const int *parity, const int *remaining,
                         const UmmaShape sh) {
     constexpr int per16 = KIND == kUmmaTF32 ? 4 : 8;
-    if ((int)blockIdx.y >= *n_items) return;
-    const UmmaItem &it = items[blockIdx.y];
-    if (remaining[it.slot] <= 0) return;
-    const StageIOT<float> &io = it.io[parity[it.slot]];
-    const int64_t n = io.n_elements * (sh.KP / per16);
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        umma_planes_body<KIND, NIN>(io, const_cast<unsigned char *>(it.a.planes), sh.R, sh.KP, i);
+    const int members = *n_items;
+    for (int m = blockIdx.y; m < members; m += gridDim.y) {
+        const UmmaItem &it = items[m];
+        if (remaining[it.slot] <= 0) continue;
+        const StageIOT<float> &io = it.io[parity[it.slot]];
+        const int64_t n = io.n_elements * (sh.KP / per16);
+        for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+            umma_planes_body<KIND, NIN>(io, const_cast<unsigned char *>(it.a.planes), sh.R, sh.KP, i);
+    }
 }
 
 // end of one step of every member: flip the current buffer, count the step
@@ -199,13 +220,17 @@ __global__ void batch_set_slot(int *parity, int *remaining, int slot, int nsteps
 
 namespace {
 
-enum BatchKind { KIND_DENSE = 0, KIND_TENSOR = 1, KIND_SLICE = 2, KIND_LINEAR = 3, KIND_UMMA = 4 };
+enum BatchKind { KIND_DENSE = 0, KIND_TENSOR = 1, KIND_SLICE = 2, KIND_LINEAR = 3, KIND_UMMA = 4, KIND_WAVE_TILES = 5 };
 
 struct BatchClass {
     // key
     int kind = 0, shape = 0, order = 0, dim = 0, physics = 0, S = 0;
     bool mixed = false;
     int precision = 0, rows = 0, lslots = 0;  // tensor-core tiles: precision, rows and slots per element
+    // the reference-element data the launches take (basis size, 1D operators), from the
+    // first member: the class launches the same way when it has no members
+    HostOperators rep;
+    unsigned grid_floor = 0;  // grid of the last capture: a class's grid never shrinks
     std::vector<double> rk_a, rk_b;
     // members and launch shape
     std::vector<int> slots;
@@ -260,11 +285,14 @@ struct hgg_batch {
     std::vector<int> base;               // the handle's current buffer when it was added
     std::vector<int> cls;                // class index of each slot
     std::vector<int> remaining_host;     // as last read back
+    std::vector<std::vector<unsigned char>> item_cache;  // per slot: its items of every stage
+    std::vector<int> cache_epb;          // elements per block the cached items were formed with
+    std::vector<int64_t> slot_blocks;    // virtual blocks of each slot's member
     std::vector<int> parity_host;
     int *d_parity = nullptr, *d_remaining = nullptr, *d_status = nullptr;
     std::vector<BatchClass> classes;
     cudaGraphExec_t graph = nullptr;
-    std::vector<int> graph_sig;  // (class, epb, ctas per SM) of the captured step
+    std::vector<int> graph_sig;  // (class, epb, ctas per SM, grid) of the captured step
     bool dirty = true;
     bool autotune = true;
     int64_t launches = 0;
@@ -291,6 +319,9 @@ int batch_kind(const hgg_handle *h) {
     if (h->linear) return KIND_LINEAR;
     if (h->slice_ok) return KIND_SLICE;
     if (h->op.tensor) return KIND_TENSOR;
+    // the same choice as the handle's own dense launch: tiles where the contraction is FP64
+    const bool fp64_contraction = !h->mixed || h->op.nB > kMixedFp32MaxBasis;
+    if (h->group_tiles > 0 && (h->variant == 2 || (h->variant == 0 && fp64_contraction))) return KIND_WAVE_TILES;
     return KIND_DENSE;
 }
 
@@ -312,6 +343,7 @@ int64_t item_blocks(const BatchClass &c, const hgg_handle *h) {
     const int64_t nE = h->op.nE;
     if (c.kind == KIND_LINEAR) return h->lin_tiles;
     if (c.kind == KIND_UMMA) return h->umma_tiles;
+    if (c.kind == KIND_WAVE_TILES) return h->group_tiles;
     if (c.kind == KIND_SLICE) return (nE + SliceShape::TE - 1) / SliceShape::TE;
     if (c.kind == KIND_TENSOR) {
         const int epb = tensor_epb(c.order, c.dim);
@@ -321,7 +353,8 @@ int64_t item_blocks(const BatchClass &c, const hgg_handle *h) {
 }
 
 size_t class_item_bytes(const BatchClass &c) {
-    if (c.kind == KIND_DENSE) return c.mixed ? sizeof(DenseItem<float>) : sizeof(DenseItem<double>);
+    if (c.kind == KIND_DENSE || c.kind == KIND_WAVE_TILES)
+        return c.mixed ? sizeof(DenseItem<float>) : sizeof(DenseItem<double>);
     if (c.kind == KIND_TENSOR) return c.mixed ? sizeof(TensorItem<float>) : sizeof(TensorItem<double>);
     if (c.kind == KIND_LINEAR) return c.mixed ? sizeof(LinearItem<float>) : sizeof(LinearItem<double>);
     if (c.kind == KIND_UMMA) return sizeof(UmmaItem);
@@ -334,61 +367,92 @@ DenseGeom dense_geom(const hgg_handle *h, int epb) {
                      h->d_elem_geo, h->d_face_geo, 1.0 / op.c_inv, upwind_speed(op), op.nB, epb};
 }
 
-// host copy of the items of one stage of a class
+// the item of one member for one stage (block0: its first virtual block in the class)
 template <typename KT>
-void fill_items(const hgg_batch *b, const BatchClass &c, int stage, std::vector<unsigned char> &buf) {
-    buf.assign(c.item_bytes * c.slots.size(), 0);
+void fill_member(const hgg_batch *b, const BatchClass &c, int slot, int stage, int64_t block0, unsigned char *dst) {
+    const hgg_handle *h = b->handles[slot];
+    const int base = b->base[slot];
+    if (c.kind == KIND_DENSE || c.kind == KIND_WAVE_TILES) {
+        DenseItem<KT> it{};
+        for (int par = 0; par < 2; ++par)
+            it.io[par] = make_stage_io<KT>(h, par ? 1 - base : base, b->dt[slot], stage, b->d_status);
+        it.g = dense_geom(h, c.epb);
+        it.tiles = c.kind == KIND_WAVE_TILES ? h->d_group_tiles : nullptr;
+        it.block0 = block0;
+        it.slot = slot;
+        std::memcpy(dst, &it, sizeof(it));
+    } else if (c.kind == KIND_UMMA) {
+        UmmaItem it{};
+        for (int par = 0; par < 2; ++par)
+            it.io[par] = make_stage_io<float>(h, par ? 1 - base : base, b->dt[slot], stage, b->d_status);
+        it.a = UmmaArgs{h->d_umma_img, h->d_umma_planes, h->d_umma_tile_elems, h->d_umma_tile_mats, h->d_lin_nbr,
+                        h->umma_tiles, h->lin_mats, kUmmaPolls};
+        it.block0 = block0;
+        it.slot = slot;
+        std::memcpy(dst, &it, sizeof(it));
+    } else if (c.kind == KIND_LINEAR) {
+        LinearItem<KT> it{};
+        for (int par = 0; par < 2; ++par)
+            it.io[par] = make_stage_io<KT>(h, par ? 1 - base : base, b->dt[slot], stage, b->d_status);
+        it.g = LinearGeom{h->d_lin_table, h->d_lin_table_rm, h->d_lin_table_f, h->d_lin_self, h->d_lin_nbr,
+                          h->d_lin_mat, h->lin_R, h->lin_slots, std::max(1, 256 / h->lin_R), h->lin_mats};
+        it.t = LinearTiles{h->d_lin_tile_elems, h->d_lin_tile_mats};
+        it.block0 = block0;
+        it.slot = slot;
+        std::memcpy(dst, &it, sizeof(it));
+    } else if (c.kind == KIND_TENSOR) {
+        TensorItem<KT> it{};
+        for (int par = 0; par < 2; ++par)
+            it.io[par] = make_stage_io<KT>(h, par ? 1 - base : base, b->dt[slot], stage, b->d_status);
+        it.geo = TensorGeom{h->d_ahat, h->d_tnbr, h->d_tmode, h->d_tsigma};
+        it.block0 = block0;
+        it.slot = slot;
+        std::memcpy(dst, &it, sizeof(it));
+    } else {
+        SliceItem<KT> it{};
+        for (int par = 0; par < 2; ++par)
+            it.io[par] = make_stage_io<KT>(h, par ? 1 - base : base, b->dt[slot], stage, b->d_status);
+        it.geo = h->d_slice_geo;
+        it.block0 = block0;
+        it.slot = slot;
+        std::memcpy(dst, &it, sizeof(it));
+    }
+}
+
+// sets the first virtual block of a stored item (every item type ends with block0, slot)
+template <typename KT>
+void set_block0(const BatchClass &c, unsigned char *dst, int64_t block0) {
+    auto put = [&](auto *it) {
+        using T = std::remove_pointer_t<decltype(it)>;
+        std::memcpy(dst + offsetof(T, block0), &block0, sizeof(block0));
+    };
+    if (c.kind == KIND_DENSE || c.kind == KIND_WAVE_TILES) put((DenseItem<KT> *)nullptr);
+    else if (c.kind == KIND_UMMA) put((UmmaItem *)nullptr);
+    else if (c.kind == KIND_LINEAR) put((LinearItem<KT> *)nullptr);
+    else if (c.kind == KIND_TENSOR) put((TensorItem<KT> *)nullptr);
+    else put((SliceItem<KT> *)nullptr);
+}
+
+// host copy of the items of one stage of a class: each member's items are formed once
+// when it joins (or when the class's elements per block change) and kept per slot, so
+// a table rewrite after a join or a removal copies them and sets their first blocks
+template <typename KT>
+void fill_items(hgg_batch *b, const BatchClass &c, int stage, std::vector<unsigned char> &buf) {
+    buf.resize(c.item_bytes * c.slots.size());
     int64_t block0 = 0;
     for (size_t m = 0; m < c.slots.size(); ++m) {
         const int slot = c.slots[m];
-        const hgg_handle *h = b->handles[slot];
-        const int base = b->base[slot];
-        unsigned char *dst = buf.data() + m * c.item_bytes;
-        if (c.kind == KIND_DENSE) {
-            DenseItem<KT> it{};
-            for (int par = 0; par < 2; ++par)
-                it.io[par] = make_stage_io<KT>(h, par ? 1 - base : base, b->dt[slot], stage, b->d_status);
-            it.g = dense_geom(h, c.epb);
-            it.block0 = block0;
-            it.slot = slot;
-            std::memcpy(dst, &it, sizeof(it));
-        } else if (c.kind == KIND_UMMA) {
-            UmmaItem it{};
-            for (int par = 0; par < 2; ++par)
-                it.io[par] = make_stage_io<float>(h, par ? 1 - base : base, b->dt[slot], stage, b->d_status);
-            it.a = UmmaArgs{h->d_umma_img, h->d_umma_planes, h->d_umma_tile_elems, h->d_umma_tile_mats, h->d_lin_nbr,
-                            h->umma_tiles, h->lin_mats, kUmmaPolls};
-            it.block0 = block0;
-            it.slot = slot;
-            std::memcpy(dst, &it, sizeof(it));
-        } else if (c.kind == KIND_LINEAR) {
-            LinearItem<KT> it{};
-            for (int par = 0; par < 2; ++par)
-                it.io[par] = make_stage_io<KT>(h, par ? 1 - base : base, b->dt[slot], stage, b->d_status);
-            it.g = LinearGeom{h->d_lin_table, h->d_lin_table_rm, h->d_lin_table_f, h->d_lin_self, h->d_lin_nbr,
-                              h->d_lin_mat, h->lin_R, h->lin_slots, std::max(1, 256 / h->lin_R), h->lin_mats};
-            it.t = LinearTiles{h->d_lin_tile_elems, h->d_lin_tile_mats};
-            it.block0 = block0;
-            it.slot = slot;
-            std::memcpy(dst, &it, sizeof(it));
-        } else if (c.kind == KIND_TENSOR) {
-            TensorItem<KT> it{};
-            for (int par = 0; par < 2; ++par)
-                it.io[par] = make_stage_io<KT>(h, par ? 1 - base : base, b->dt[slot], stage, b->d_status);
-            it.geo = TensorGeom{h->d_ahat, h->d_tnbr, h->d_tmode, h->d_tsigma};
-            it.block0 = block0;
-            it.slot = slot;
-            std::memcpy(dst, &it, sizeof(it));
-        } else {
-            SliceItem<KT> it{};
-            for (int par = 0; par < 2; ++par)
-                it.io[par] = make_stage_io<KT>(h, par ? 1 - base : base, b->dt[slot], stage, b->d_status);
-            it.geo = h->d_slice_geo;
-            it.block0 = block0;
-            it.slot = slot;
-            std::memcpy(dst, &it, sizeof(it));
+        auto &cache = b->item_cache[slot];
+        if (cache.size() != c.item_bytes * c.S || b->cache_epb[slot] != c.epb) {
+            cache.assign(c.item_bytes * c.S, 0);
+            for (int st = 0; st < c.S; ++st) fill_member<KT>(b, c, slot, st, 0, cache.data() + st * c.item_bytes);
+            b->cache_epb[slot] = c.epb;
+            b->slot_blocks[slot] = item_blocks(c, b->handles[slot]);
         }
-        block0 += item_blocks(c, h);
+        unsigned char *dst = buf.data() + m * c.item_bytes;
+        std::memcpy(dst, cache.data() + stage * c.item_bytes, c.item_bytes);
+        set_block0<KT>(c, dst, block0);
+        block0 += b->slot_blocks[slot];
     }
 }
 
@@ -439,7 +503,7 @@ int upload_class(hgg_batch *b, BatchClass &c) {
 
 template <typename KT, int DIM, int NFL, int WAVE>
 void launch_grouped_dense(const hgg_batch *b, const BatchClass &c, int st, unsigned grid, cudaStream_t s) {
-    const int nB = b->handles[c.slots[0]]->op.nB;
+    const int nB = c.rep.nB;
     const int threads = dense_threads(DIM, WAVE, nB, c.epb);
     dense_dispatch<DIM, NFL, WAVE>(nB, [&](auto nbc) {
         constexpr int NB = decltype(nbc)::value;
@@ -458,11 +522,26 @@ void launch_grouped_dense_any(const hgg_batch *b, const BatchClass &c, int st, u
     else launch_grouped_dense<double, DIM, NFL, WAVE>(b, c, st, grid, s);
 }
 
+template <typename KT, int DIM, int NFL>
+void launch_grouped_wave(const hgg_batch *b, const BatchClass &c, int st, unsigned grid, cudaStream_t s) {
+    const int nB = c.rep.nB;
+    dense_dispatch<DIM, NFL, 1>(nB, [&](auto nbc) {
+        constexpr int NB = decltype(nbc)::value;
+        if constexpr (DIM >= 2 && NB <= kGroupMaxRows) {
+            constexpr size_t smem = group_smem<DenseCT<KT, NB>, DIM, NFL, NB>();
+            cudaFuncSetAttribute(grouped_wave_tiles<KT, DIM, NFL, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem);
+            grouped_wave_tiles<KT, DIM, NFL, NB><<<grid, kGroupTile * NB, smem, s>>>(
+                static_cast<const DenseItem<KT> *>(c.d_items[st]), c.d_n, c.d_total, b->d_parity, b->d_remaining);
+        }
+    });
+}
+
 template <int P, int DIM>
 void launch_grouped_tensor(const hgg_batch *b, const BatchClass &c, int st, unsigned grid, cudaStream_t s) {
     constexpr int NB = TensorConsts<P, DIM>::NB;
     constexpr int EPB = (256 / NB) > 0 ? (256 / NB) : 1;
-    const TensorConsts<P, DIM> tc = tensor_consts<P, DIM>(b->handles[c.slots[0]]->op);
+    const TensorConsts<P, DIM> tc = tensor_consts<P, DIM>(c.rep);
     if (c.mixed)
         grouped_tensor<float, P, DIM, EPB><<<grid, EPB * NB, 0, s>>>(
             static_cast<const TensorItem<float> *>(c.d_items[st]), c.d_n, c.d_total, b->d_parity, b->d_remaining, tc);
@@ -473,14 +552,19 @@ void launch_grouped_tensor(const hgg_batch *b, const BatchClass &c, int st, unsi
 
 template <typename KT>
 void launch_grouped_slice(const hgg_batch *b, const BatchClass &c, int st, unsigned grid, cudaStream_t s) {
-    const hgg_handle *h = b->handles[c.slots[0]];
     SliceOps sops;
-    for (int i = 0; i < 16; ++i) sops.D[i] = h->op.D1[i];
+    for (int i = 0; i < 16; ++i) sops.D[i] = c.rep.D1[i];
     for (int sd = 0; sd < 2; ++sd)
-        for (int a = 0; a < 4; ++a) sops.L[sd][a] = h->op.lift[sd * 4 + a];
-    // the stage's shape is the same for every member (same tableau): take it from the first
-    const StageIOT<KT> io = make_stage_io<KT>(h, 0, 1.0, st, nullptr);
-    const bool fin = io.unew != nullptr;
+        for (int a = 0; a < 4; ++a) sops.L[sd][a] = c.rep.lift[sd * 4 + a];
+    // the stage's shape is the same for every member (same tableau): its stage-input
+    // vectors (nonzero a_ij) and, in the final stage, the earlier vectors of the update
+    struct {
+        int nin = 0, nfin = 0;
+    } io;
+    for (int j = 0; j < st; ++j) io.nin += c.rk_a[st * c.S + j] != 0.0;
+    const bool fin = st == c.S - 1;
+    if (fin)
+        for (int j = 0; j < c.S - 1; ++j) io.nfin += c.rk_b[j] != 0.0;
     const auto *items = static_cast<const SliceItem<KT> *>(c.d_items[st]);
     const dim3 g(grid), blk(SliceShape::THREADS);
     if (io.nin == 0 && (!fin || io.nfin == 0))
@@ -494,9 +578,23 @@ void launch_grouped_slice(const hgg_batch *b, const BatchClass &c, int st, unsig
 }
 
 // one stage of one class
+// Persistent grid of a class: ctas_per_sm CTAs per SM, or fewer for a class with
+// fewer virtual blocks (its block count rounded up to a power of two, and never less
+// than the grid it was last captured with), so that the kernels of small classes leave
+// SMs to the other classes of the step, which run as parallel branches of the captured
+// graph.  A captured grid stays valid while the class's membership changes (the CTAs
+// loop over the virtual blocks); the step is captured again only when a class outgrows
+// its grid or a class that is not in the graph gains members.
+unsigned class_grid(const hgg_batch *b, const BatchClass &c) {
+    const int64_t full = (int64_t)c.ctas_per_sm * b->num_sms;
+    if (c.total_blocks >= full) return (unsigned)full;
+    int64_t g = 1;
+    while (g < c.total_blocks) g <<= 1;
+    return (unsigned)std::min(std::max(g, (int64_t)c.grid_floor), full);
+}
+
 void launch_class_stage(hgg_batch *b, const BatchClass &c, int st, cudaStream_t s) {
-    // a fixed persistent grid: membership changes leave the launch (and the graph) as it is
-    const unsigned grid = (unsigned)(c.ctas_per_sm * b->num_sms);
+    const unsigned grid = class_grid(b, c);
     if (c.kind == KIND_UMMA) {
         const int kind = c.precision == HGG_PRECISION_BF16X3 ? kUmmaBF16 : kUmmaTF32;
         const UmmaShape sh = umma_shape(c.rows, c.lslots, kind);
@@ -505,7 +603,10 @@ void launch_class_stage(hgg_batch *b, const BatchClass &c, int st, cudaStream_t 
         if (!(c.rows % 4 == 0 && nin <= 1)) nin = -1;
         const size_t smem = umma_smem(sh);
         const UmmaItem *it = static_cast<const UmmaItem *>(c.d_items[st]);
-        const dim3 pgrid((unsigned)(2 * b->num_sms), (unsigned)b->cap);
+        // members along y (a power of two at least their count, looping past it)
+        unsigned my = 1;
+        while (my < c.slots.size() && my < 1024) my <<= 1;
+        const dim3 pgrid((unsigned)(2 * b->num_sms), my);
         auto planes = [&](auto kc, auto nc) {
             constexpr int K = decltype(kc)::value, NIN = decltype(nc)::value;
             grouped_umma_planes<K, NIN><<<pgrid, 256, 0, s>>>(it, c.d_n, b->d_parity, b->d_remaining, sh);
@@ -543,6 +644,21 @@ void launch_class_stage(hgg_batch *b, const BatchClass &c, int st, cudaStream_t 
     } else if (c.kind == KIND_SLICE) {
         if (c.mixed) launch_grouped_slice<float>(b, c, st, grid, s);
         else launch_grouped_slice<double>(b, c, st, grid, s);
+    } else if (c.kind == KIND_WAVE_TILES) {
+        switch (c.shape) {
+            case HGG_SHAPE_TRIANGLE:
+                c.mixed ? launch_grouped_wave<float, 2, 3>(b, c, st, grid, s) : launch_grouped_wave<double, 2, 3>(b, c, st, grid, s);
+                break;
+            case HGG_SHAPE_SQUARE:
+                c.mixed ? launch_grouped_wave<float, 2, 4>(b, c, st, grid, s) : launch_grouped_wave<double, 2, 4>(b, c, st, grid, s);
+                break;
+            case HGG_SHAPE_TETRAHEDRON:
+                c.mixed ? launch_grouped_wave<float, 3, 4>(b, c, st, grid, s) : launch_grouped_wave<double, 3, 4>(b, c, st, grid, s);
+                break;
+            case HGG_SHAPE_CUBE:
+                c.mixed ? launch_grouped_wave<float, 3, 6>(b, c, st, grid, s) : launch_grouped_wave<double, 3, 6>(b, c, st, grid, s);
+                break;
+        }
     } else if (c.kind == KIND_TENSOR) {
 #define HGG_GT(P)                                                  \
     case P:                                                        \
@@ -709,18 +825,28 @@ int prepare_batch(hgg_batch *b) {
             HGG_BCUDA(b, cudaStreamSynchronize(b->stream));
         }
     }
+    // classes of the step: those with members and those already in the graph (a class
+    // that empties stays in the captured step with n = 0, so that it can refill without
+    // a new capture)
+    auto in_graph = [&](int i) {
+        for (size_t j = 0; j + 3 < b->graph_sig.size(); j += 4)
+            if (b->graph_sig[j] == i) return true;
+        return false;
+    };
     std::vector<int> sig;
     bool covered = b->graph != nullptr;
     for (size_t i = 0; i < b->classes.size(); ++i) {
         const auto &c = b->classes[i];
-        if (c.slots.empty()) continue;
+        if (c.slots.empty() && !(b->graph && in_graph((int)i))) continue;
+        const int grid = (int)class_grid(b, c);
         sig.push_back((int)i);
         sig.push_back(c.epb);
         sig.push_back(c.ctas_per_sm);
+        sig.push_back(grid);
         bool found = false;
-        for (size_t j = 0; j + 2 < b->graph_sig.size(); j += 3)
+        for (size_t j = 0; j + 3 < b->graph_sig.size(); j += 4)
             found = found || (b->graph_sig[j] == (int)i && b->graph_sig[j + 1] == c.epb &&
-                              b->graph_sig[j + 2] == c.ctas_per_sm);
+                              b->graph_sig[j + 2] == c.ctas_per_sm && b->graph_sig[j + 3] >= grid);
         covered = covered && found;
     }
     if (covered) {
@@ -732,12 +858,13 @@ int prepare_batch(hgg_batch *b) {
     HGG_BCUDA(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
     const int64_t before = b->launches;
     cudaEventRecord(b->fork, b->stream);
-    for (auto &c : b->classes) {
-        if (c.slots.empty()) continue;
+    for (size_t j = 0; j + 3 < sig.size(); j += 4) {
+        BatchClass &c = b->classes[sig[j]];
         cudaStreamWaitEvent(c.stream, b->fork, 0);
         for (int st = 0; st < c.S; ++st) launch_class_stage(b, c, st, c.stream);
         cudaEventRecord(c.done, c.stream);
         cudaStreamWaitEvent(b->stream, c.done, 0);
+        c.grid_floor = (unsigned)sig[j + 3];
     }
     batch_advance<<<(b->cap + 255) / 256, 256, 0, b->stream>>>(b->d_parity, b->d_remaining, b->cap);
     cudaError_t ce = cudaStreamEndCapture(b->stream, &g);
@@ -755,7 +882,7 @@ int prepare_batch(hgg_batch *b) {
 // classes also form the split stage input before each stage), then the counters advance
 int launches_per_step(const hgg_batch *b) {
     int n = 1;
-    for (size_t j = 0; j < b->graph_sig.size(); j += 3) {
+    for (size_t j = 0; j < b->graph_sig.size(); j += 4) {
         const BatchClass &c = b->classes[b->graph_sig[j]];
         n += c.kind == KIND_UMMA ? 2 * c.S : c.S;
     }
@@ -768,13 +895,13 @@ void destroy_batch(hgg_batch *b) {
     release_batch_graph(b);
     for (auto &c : b->classes) {
         if (c.stream) cudaStreamSynchronize(c.stream);
-        for (void *p : c.d_items) cudaFree(p);
+        for (void *p : c.d_items) cudaFreeAsync(p, b->stream);
         for (int i = 0; i < 2; ++i) {
             if (c.h_up[i]) cudaFreeHost(c.h_up[i]);
             if (c.up_done[i]) cudaEventDestroy(c.up_done[i]);
         }
-        cudaFree(c.d_n);
-        cudaFree(c.d_total);
+        cudaFreeAsync(c.d_n, b->stream);
+        cudaFreeAsync(c.d_total, b->stream);
         if (c.done) cudaEventDestroy(c.done);
         if (c.stream) cudaStreamDestroy(c.stream);
     }
@@ -798,6 +925,7 @@ int remove_member(hgg_batch *b, int slot, int parity) {
     b->handles[slot] = nullptr;
     b->cls[slot] = -1;
     b->remaining_host[slot] = 0;
+    b->item_cache[slot].clear();
     batch_set_slot<<<1, 1, 0, b->stream>>>(b->d_parity, b->d_remaining, slot, 0);
     HGG_BCUDA(b, cudaGetLastError());
     b->dirty = true;
@@ -821,6 +949,9 @@ int hgg_batch_create(int32_t capacity, hgg_batch **out) {
     b->base.assign(capacity, 0);
     b->cls.assign(capacity, -1);
     b->remaining_host.assign(capacity, 0);
+    b->item_cache.assign(capacity, {});
+    b->cache_epb.assign(capacity, -1);
+    b->slot_blocks.assign(capacity, 0);
     b->parity_host.assign(capacity, 0);
     auto fail_create = [&](cudaError_t e, const char *what) {
         g_batch_create_error = std::string(what) + ": " + cudaGetErrorString(e);
@@ -887,13 +1018,25 @@ int hgg_batch_add(hgg_batch *b, hgg_handle *h, double dt, int32_t nsteps, int32_
         c.precision = h->precision;
         c.rows = h->lin_R;
         c.lslots = h->lin_slots;
+        c.rep.shape = h->op.shape;
+        c.rep.dim = h->op.dim;
+        c.rep.order = h->op.order;
+        c.rep.nB = h->op.nB;
+        c.rep.V = h->op.V;
+        c.rep.physics = h->op.physics;
+        c.rep.nfl = h->op.nfl;
+        c.rep.np = h->op.np;
+        c.rep.D1 = h->op.D1;
+        c.rep.lift = h->op.lift;
+        c.rep.trace_pos[0] = h->op.trace_pos[0];
+        c.rep.trace_pos[1] = h->op.trace_pos[1];
         c.epb = c.kind == KIND_DENSE ? std::max(1, 256 / dense_rows(h->op.dim, h->op.physics != HGG_PHYSICS_ADVECTION, h->op.nB)) : 1;
         c.item_bytes = class_item_bytes(c);
         c.d_items.assign(c.S, nullptr);
         for (int st = 0; st < c.S; ++st)
-            HGG_BCUDA(b, cudaMalloc(&c.d_items[st], c.item_bytes * (size_t)b->cap));
-        HGG_BCUDA(b, cudaMalloc(&c.d_n, sizeof(int)));
-        HGG_BCUDA(b, cudaMalloc(&c.d_total, sizeof(int64_t)));
+            HGG_BCUDA(b, cudaMallocAsync(&c.d_items[st], c.item_bytes * (size_t)b->cap, b->stream));
+        HGG_BCUDA(b, cudaMallocAsync(&c.d_n, sizeof(int), b->stream));
+        HGG_BCUDA(b, cudaMallocAsync(&c.d_total, sizeof(int64_t), b->stream));
         HGG_BCUDA(b, cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
         HGG_BCUDA(b, cudaEventCreateWithFlags(&c.done, cudaEventDisableTiming));
         b->classes.push_back(std::move(c));
@@ -901,6 +1044,7 @@ int hgg_batch_add(hgg_batch *b, hgg_handle *h, double dt, int32_t nsteps, int32_
     }
     b->classes[ci].slots.push_back(free_slot);
     b->classes[ci].table_dirty = true;
+    b->item_cache[free_slot].clear();  // formed at the next table upload
     b->handles[free_slot] = h;
     b->dt[free_slot] = dt;
     b->base[free_slot] = h->cur;

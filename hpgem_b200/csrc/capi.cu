@@ -38,10 +38,27 @@ int fail(hgg_handle *h, int code, const std::string &msg) {
 
 int alloc(hgg_handle *h, size_t bytes, void **dst) {
     void *p = nullptr;
-    cudaError_t e = cudaMalloc(&p, bytes);
-    if (e != cudaSuccess) return fail(h, HGG_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    cudaError_t e = cudaMallocAsync(&p, bytes, h->stream);
+    if (e != cudaSuccess) return fail(h, HGG_ERR_NOMEM, std::string("cudaMallocAsync: ") + cudaGetErrorString(e));
     h->bufs.push_back({p, bytes});
     *dst = p;
+    return 0;
+}
+
+int solution_to_host(hgg_handle *h, double *staging, double *out) {
+    const double *d = h->sol[h->cur];
+    const int64_t n = h->tensor_layout ? h->N_alloc : h->N;
+    HGG_CUDA(h, cudaMemcpyAsync(staging, d, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream));
+    HGG_CUDA(h, cudaStreamSynchronize(h->stream));
+    if (!h->tensor_layout) {
+        std::memcpy(out, staging, sizeof(double) * h->N);
+        return 0;
+    }
+    const int nb = h->op.nB;
+    const int64_t ne = h->N / nb;
+    for (int64_t e = 0; e < ne; ++e)
+        for (int k = 0; k < nb; ++k)
+            out[e * nb + k] = h->op.tsign[k] * staging[device_index(e, (int)h->op.tpos[k], nb, h->tiled)];
     return 0;
 }
 
@@ -203,6 +220,16 @@ int init_device_vectors(hgg_handle *h) {
     HGG_CUDA(h, cudaGetDevice(&h->device));
     HGG_CUDA(h, cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
     h->stream = h->own_stream;
+    // the default pool keeps freed handle memory for the next handles instead of
+    // returning it to the driver at every synchronisation (which waits for the device)
+    static std::once_flag pool_once;
+    std::call_once(pool_once, [&] {
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, h->device) == cudaSuccess) {
+            uint64_t keep = ~0ull;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+    });
     int rc;
     HGG_CUDA(h, cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device));
     for (int i = 0; i < 2; ++i)
@@ -303,13 +330,14 @@ int create_from_desc(const hgg_problem_desc *desc, hgg_handle *h, bool linear = 
         // ms per step at p = 4, 0.48 against 0.87 at p = 5; in the mixed form p = 4
         // measured 0.33 against 0.29 and stays on the dense kernel).  Only when the
         // mesh forms tiles (structured meshes); otherwise the dense kernel runs.
-        // The mixed forms run folded tiles on the tensor cores (tcgen05) where the mesh
-        // forms them: split-BF16 always (it has no other kernel), the FP32 form for the
-        // wave and for advection on triangles at p = 5.
+        // Split-BF16 runs folded tiles on the tensor cores (tcgen05) where the mesh forms
+        // them (it has no other kernel); the FP32 form folds advection on triangles at
+        // p = 5.  The FP32 form of the wave stays matrix-free: on the served request mix
+        // its dense kernel measured 2-5x the DoF-updates/s of the TF32 tiles (triangles
+        // at p = 1: 8.1e9 against 2.0e9; tetrahedra at p = 2: 5.2e9 against 3.5e9).
         const bool fold_tri = op.physics == HGG_PHYSICS_ADVECTION && op.shape == HGG_SHAPE_TRIANGLE &&
                               (op.nB >= 21 || (op.nB >= 15 && !h->mixed));
-        const bool fold_tc = h->precision == HGG_PRECISION_BF16X3 ||
-                             (h->precision == HGG_PRECISION_FP32 && op.physics != HGG_PHYSICS_ADVECTION);
+        const bool fold_tc = h->precision == HGG_PRECISION_BF16X3;
         if (fold_tri || fold_tc) {
             LinearSystem sys;
             bool assembled = true;
@@ -544,7 +572,8 @@ void destroy_handle(hgg_handle *h) {
     destroy_sources(h);
     if (h->stream) cudaStreamSynchronize(h->stream);
     if (h->own_stream) cudaStreamSynchronize(h->own_stream);
-    for (auto &b : h->bufs) cudaFree(b.p);
+    for (auto &b : h->bufs) cudaFreeAsync(b.p, h->stream);
+    if (h->stream) cudaStreamSynchronize(h->stream);
     if (h->own_stream) cudaStreamDestroy(h->own_stream);
     delete h;
 }
@@ -1441,10 +1470,9 @@ int hpgem_order_view(hgg_handle *h, int vec, const double **view) {
 int exact_on_device(hgg_handle *h, const double *exact, size_t count, const double **out) {
     if (count > h->exact_cap) {
         if (h->d_exact) {
-            cudaStreamSynchronize(h->stream);
             for (auto it = h->bufs.begin(); it != h->bufs.end(); ++it)
                 if (it->p == h->d_exact) {
-                    cudaFree(it->p);
+                    cudaFreeAsync(it->p, h->stream);
                     h->bufs.erase(it);
                     break;
                 }

@@ -119,6 +119,11 @@ int fail(hgg_handle *h, int code, const std::string &msg);
             return fail(h, HGG_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(_e)); \
     } while (0)
 
+// Device memory of a handle is stream-ordered (cudaMallocAsync / cudaFreeAsync on the
+// handle's stream, from the device's default pool): freeing a handle never waits for
+// work of other streams, so a solve that finishes inside a batch or a server is freed
+// while the other members keep stepping.
+
 // device copy of a host vector, owned by the handle
 template <typename T>
 int upload(hgg_handle *h, const std::vector<T> &v, T **dst) {
@@ -126,8 +131,8 @@ int upload(hgg_handle *h, const std::vector<T> &v, T **dst) {
     if (v.empty()) return 0;
     void *p = nullptr;
     size_t bytes = v.size() * sizeof(T);
-    cudaError_t e = cudaMalloc(&p, bytes);
-    if (e != cudaSuccess) return fail(h, HGG_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    cudaError_t e = cudaMallocAsync(&p, bytes, h->stream);
+    if (e != cudaSuccess) return fail(h, HGG_ERR_NOMEM, std::string("cudaMallocAsync: ") + cudaGetErrorString(e));
     h->bufs.push_back({p, bytes});
     e = cudaMemcpyAsync(p, v.data(), bytes, cudaMemcpyHostToDevice, h->stream);
     if (e != cudaSuccess) return fail(h, HGG_ERR_CUDA, std::string("cudaMemcpyAsync: ") + cudaGetErrorString(e));
@@ -137,6 +142,9 @@ int upload(hgg_handle *h, const std::vector<T> &v, T **dst) {
 
 int alloc(hgg_handle *h, size_t bytes, void **dst);
 void release_graphs(hgg_handle *h);
+// the current solution in hpGEM order with no kernel on the device: one copy of the
+// device vector into `staging` (pinned, h->N_alloc doubles), the layout change on the host
+int solution_to_host(hgg_handle *h, double *staging, double *out);
 
 template <int P, int DIM>
 TensorConsts<P, DIM> tensor_consts(const HostOperators &op) {
@@ -156,7 +164,7 @@ TensorConsts<P, DIM> tensor_consts(const HostOperators &op) {
 
 // layout conversion index (hpGEM order <-> tensor order, signs folded; tiled:
 // 32-element tiles, coefficient-major inside a tile)
-__device__ __forceinline__ int64_t device_index(int64_t e, int pos, int nb, bool tiled) {
+__host__ __device__ __forceinline__ int64_t device_index(int64_t e, int pos, int nb, bool tiled) {
     return tiled ? (e >> 5) * ((int64_t)nb << 5) + (int64_t)pos * 32 + (e & 31) : e * nb + pos;
 }
 // stage vectors and per-stage coefficients of the error estimate and the rewind

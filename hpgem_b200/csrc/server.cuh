@@ -69,15 +69,17 @@ struct hgg_server {
     bool gpu_done = false;  // the GPU thread has ended: the retire thread empties its queue and ends
     std::vector<std::thread> setup_threads;
     std::thread gpu_thread, retire_thread;
+    std::vector<cudaStream_t> side_streams;  // set-up threads' and retire thread's (high priority)
     hgg_batch *batch = nullptr;
     std::string err = "no error";
     int gpu_error = 0;
     // counters
     int64_t completed = 0, dof_updates = 0, chunks = 0;
-    // GPU thread: waiting for chunks, membership work (joins, removals, tables,
-    // graph, issuing launches), waiting for work; retire thread busy; device time
-    // of the chunks (CUDA events around each chunk on the batch stream)
+    // GPU thread: stepping (issuing graph launches, waiting for chunks), membership
+    // work (joins, removals, tables, graph captures), waiting for work; retire thread
+    // busy; device time of the chunks (CUDA events around each chunk on the batch stream)
     double t_step = 0, t_members = 0, t_idle = 0, t_retire = 0, t_device = 0;
+    double t_join = 0, t_prepare = 0, t_copyback = 0;  // parts: joins, table uploads and captures, copies back
 };
 
 namespace {
@@ -92,7 +94,7 @@ int64_t estimate_footprint(const hgg_problem_desc &d) {
     return (3 * 8 + d.n_stages * kbytes) * (N + 64 * 64) + d.n_elements * 640 + (8 << 20);
 }
 
-void setup_loop(hgg_server *s) {
+void setup_loop(hgg_server *s, cudaStream_t stream) {
     cudaSetDevice(s->device);
     for (;;) {
         ServerRequest *r = nullptr;
@@ -138,6 +140,9 @@ void setup_loop(hgg_server *s) {
             rc = hgg_create_structured(r->description.c_str(), r->order, r->physics, r->params.data(),
                                        r->tableau.c_str(), r->precision, &r->h);
             if (rc) r->message = hgg_last_error(nullptr);
+            // the projection on this thread's high-priority stream: its kernels take SMs
+            // ahead of the waiting CTAs of the running batch
+            else if ((rc = hgg_set_stream(r->h, stream))) r->message = hgg_last_error(r->h);
         }
         if (rc == 0) {
             if (!r->u0.empty()) {
@@ -160,8 +165,9 @@ void setup_loop(hgg_server *s) {
             }
             if (rc) r->message = hgg_last_error(r->h);
             else hgg_set_store_last_stage(r->h, 0);
-            // the batch reads the handle's buffers on its own stream
-            if (rc == 0 && cudaStreamSynchronize(r->h->stream) != cudaSuccess) {
+            // the batch reads the handle's buffers on its own stream: the set-up work is
+            // finished, and the handle goes back to its own (idle) stream
+            if (rc == 0 && (cudaStreamSynchronize(r->h->stream) != cudaSuccess || hgg_set_stream(r->h, nullptr))) {
                 rc = HGG_ERR_CUDA;
                 r->message = "set-up copies failed";
             }
@@ -260,6 +266,7 @@ void gpu_loop_body(hgg_server *s, ChunkSnapshot *snap) {
         const double t1 = now_s();
         // 2. joins: stream-ordered after the chunks in flight
         for (ServerRequest *r : joining) {
+            const double tj = now_s();
             int32_t slot = -1;
             int rc = hgg_batch_add(b, r->h, r->dt, r->nsteps, &slot);
             if (rc) {
@@ -278,17 +285,28 @@ void gpu_loop_body(hgg_server *s, ChunkSnapshot *snap) {
             std::lock_guard<std::mutex> lk(s->mu);
             r->state = 3;
             r->t_start = now_s();
+            s->t_join += r->t_start - tj;
         }
         // 3. issue the next chunk: the most steps any member still needs, capped
         int chunk = 0;
         for (int i = 0; i < cap; ++i)
             if (member[i]) chunk = std::max(chunk, member[i]->nsteps - member[i]->issued);
         chunk = std::min(chunk, s->max_chunk);
+        double t_issue = 0.0;  // graph launches: they block while the device's launch queue is full
+        double t_prepare = 0.0;
         if (chunk > 0) {
             ChunkSnapshot &sn = snap[next_snap];
             cudaEventRecord(sn.start, b->stream);
-            int rc = hgg_batch_step(b, chunk);
+            const double tp = now_s();
+            int rc = prepare_batch(b);  // tables of the classes whose members changed, capture if needed
             if (rc) return fail_unfinished(s, rc, hgg_batch_last_error(b));
+            const double ti = now_s();
+            t_prepare = ti - tp;
+            for (int k = 0; k < chunk; ++k)
+                if (cudaGraphLaunch(b->graph, b->stream) != cudaSuccess)
+                    return fail_unfinished(s, HGG_ERR_CUDA, "serving loop: graph launch failed");
+            b->launches += (int64_t)chunk * launches_per_step(b);
+            t_issue = now_s() - ti;
             cudaMemcpyAsync(sn.host, b->d_parity, sizeof(int) * cap, cudaMemcpyDeviceToHost, b->stream);
             cudaMemcpyAsync(sn.host + cap, b->d_remaining, sizeof(int) * cap, cudaMemcpyDeviceToHost, b->stream);
             cudaMemcpyAsync(sn.host + 2 * cap, b->d_status, sizeof(int), cudaMemcpyDeviceToHost, b->stream);
@@ -305,7 +323,9 @@ void gpu_loop_body(hgg_server *s, ChunkSnapshot *snap) {
         const double t2 = now_s();
         {
             std::lock_guard<std::mutex> lk(s->mu);
-            s->t_members += t2 - t1;
+            s->t_members += t2 - t1 - t_issue;
+            s->t_step += t_issue;
+            s->t_prepare += t_prepare;
             if (chunk > 0) s->chunks++;
         }
         // 4. wait for the oldest chunk once two are in flight (or nothing more can be issued)
@@ -363,7 +383,7 @@ void gpu_loop(hgg_server *s) {
 
 // copies finished solutions back (the handle's own stream, a pinned buffer) and frees
 // their device memory, off the GPU thread
-void retire_loop(hgg_server *s) {
+void retire_loop(hgg_server *s, cudaStream_t stream) {
     cudaSetDevice(s->device);
     double *pinned = nullptr;
     size_t pinned_n = 0;
@@ -385,8 +405,11 @@ void retire_loop(hgg_server *s) {
             }
             int rc = 0;
             std::string msg;
-            if (!failed_already) {
-                const size_t n = (size_t)hgg_vector_length(r->h);
+            if (!failed_already) rc = hgg_set_stream(r->h, stream);  // high priority, see setup_loop
+            if (!failed_already && rc == 0) {
+                // one copy engine transfer into pinned memory, the layout change on the host: a
+                // kernel here would wait for SMs behind the batch's persistent kernels
+                const size_t n = (size_t)r->h->N_alloc;
                 if (n > pinned_n) {
                     if (pinned) cudaFreeHost(pinned);
                     pinned = nullptr;
@@ -394,10 +417,17 @@ void retire_loop(hgg_server *s) {
                     if (cudaHostAlloc((void **)&pinned, sizeof(double) * n, cudaHostAllocDefault) == cudaSuccess)
                         pinned_n = n;
                 }
-                r->result.resize(n);
-                rc = hgg_get_state(r->h, 0, pinned ? pinned : r->result.data());
-                if (rc == 0 && pinned) std::memcpy(r->result.data(), pinned, sizeof(double) * n);
-                if (rc) msg = hgg_last_error(r->h);
+                const double tc = now_s();
+                if (!pinned) {
+                    rc = HGG_ERR_NOMEM;
+                    msg = "pinned staging buffer could not be allocated";
+                } else {
+                    r->result.resize((size_t)r->h->N);
+                    rc = hgg::solution_to_host(r->h, pinned, r->result.data());
+                    if (rc) msg = hgg_last_error(r->h);
+                }
+                std::lock_guard<std::mutex> lk(s->mu);
+                s->t_copyback += now_s() - tc;
             }
             hgg_destroy(r->h);
             r->h = nullptr;
@@ -443,9 +473,22 @@ int hgg_server_start(int64_t budget_bytes, int32_t max_chunk, int32_t setup_thre
     }
     // fixed launch shapes: timing candidates would wait for the chunks in flight
     hgg_batch_set_autotune(s->batch, 0);
-    for (int i = 0; i < setup_threads; ++i) s->setup_threads.emplace_back(setup_loop, s);
+    // high-priority streams of the set-up threads and the retire thread
+    int lo = 0, hi = 0;
+    cudaDeviceGetStreamPriorityRange(&lo, &hi);
+    s->side_streams.assign(setup_threads + 1, nullptr);
+    for (auto &st : s->side_streams)
+        if (cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, hi) != cudaSuccess) {
+            g_server_create_error = "cudaStreamCreateWithPriority failed";
+            for (auto &t : s->side_streams)
+                if (t) cudaStreamDestroy(t);
+            hgg_batch_destroy(s->batch);
+            delete s;
+            return HGG_ERR_CUDA;
+        }
+    for (int i = 0; i < setup_threads; ++i) s->setup_threads.emplace_back(setup_loop, s, s->side_streams[i]);
     s->gpu_thread = std::thread(gpu_loop, s);
-    s->retire_thread = std::thread(retire_loop, s);
+    s->retire_thread = std::thread(retire_loop, s, s->side_streams[setup_threads]);
     *out = s;
     return 0;
 }
@@ -561,17 +604,20 @@ int hgg_server_stats(hgg_server *s, int64_t *stats4) {
     return 0;
 }
 
-// seconds: GPU thread waiting for chunks, GPU thread membership work (joins,
-// removals, tables, graph, issuing launches), GPU thread waiting for work, retire
-// thread (copies back, frees), device time of the chunks
-int hgg_server_timing(hgg_server *s, double *t5) {
-    if (!s || !t5) return sfail(s, HGG_ERR_INVALID, "null argument");
+// seconds: GPU thread stepping (issuing launches, waiting for chunks), GPU thread
+// membership work (joins, removals, tables, graph captures), GPU thread waiting for
+// work, retire thread (copies back, frees), device time of the chunks
+int hgg_server_timing(hgg_server *s, double *t8) {
+    if (!s || !t8) return sfail(s, HGG_ERR_INVALID, "null argument");
     std::lock_guard<std::mutex> lk(s->mu);
-    t5[0] = s->t_step;
-    t5[1] = s->t_members;
-    t5[2] = s->t_idle;
-    t5[3] = s->t_retire;
-    t5[4] = s->t_device;
+    t8[0] = s->t_step;
+    t8[1] = s->t_members;
+    t8[2] = s->t_idle;
+    t8[3] = s->t_retire;
+    t8[4] = s->t_device;
+    t8[5] = s->t_join;
+    t8[6] = s->t_prepare;
+    t8[7] = s->t_copyback;
     return 0;
 }
 
@@ -605,6 +651,7 @@ int hgg_server_stop(hgg_server *s) {
     hgg_batch_destroy(s->batch);
     for (auto &kv : s->requests)
         if (kv.second->h) hgg_destroy(kv.second->h);
+    for (auto &t : s->side_streams) cudaStreamDestroy(t);
     delete s;
     return rc;
 }

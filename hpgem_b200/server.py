@@ -88,11 +88,13 @@ class Server:
     def stats(self):
         st = np.zeros(4, dtype=np.int64)
         self._check(self._lib.hgg_server_stats(self._raw, ctypes.c_void_p(st.ctypes.data)))
-        t = np.zeros(5)
+        t = np.zeros(8)
         self._check(self._lib.hgg_server_timing(self._raw, ctypes.c_void_p(t.ctypes.data)))
         return dict(completed=int(st[0]), dof_updates=int(st[1]), chunks=int(st[2]), reserved_bytes=int(st[3]),
                     gpu_thread_step_s=float(t[0]), gpu_thread_members_s=float(t[1]),
-                    gpu_thread_idle_s=float(t[2]), retire_thread_s=float(t[3]), device_chunk_s=float(t[4]))
+                    gpu_thread_idle_s=float(t[2]), retire_thread_s=float(t[3]), device_chunk_s=float(t[4]),
+                    gpu_thread_join_s=float(t[5]), gpu_thread_tables_s=float(t[6]),
+                    retire_copyback_s=float(t[7]))
 
     def stop(self):
         if self._raw:

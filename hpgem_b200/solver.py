@@ -413,8 +413,9 @@ class HpgemAPILinear(HpgemAPISimplified):
 
     def __init__(self, dim, order, physics="advection", advection=None, c_inv=1.0,
                  tableau="RK4_4", precision=_native.PRECISION_FP64):
-        if physics not in ("advection", "wave"):
-            raise ValueError("the linear applications are 'advection' and 'wave' (central flux)")
+        if physics not in ("advection", "wave", "wave_upwind"):
+            raise ValueError("the linear applications are 'advection' and 'wave' (the reference's central "
+                             "flux; 'wave_upwind' folds the upwind flux of the matrix-free wave the same way)")
         super().__init__(dim, order, physics, advection=advection, c_inv=c_inv, tableau=tableau,
                          precision=precision)
 

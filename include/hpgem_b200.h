@@ -524,12 +524,14 @@ int hgg_server_times(hgg_server *s, int64_t id, double *t4);
 /* Completed solves, their DoF-updates, chunks stepped, device bytes reserved now. */
 int hgg_server_stats(hgg_server *s, int64_t *stats4);
 
-/* Seconds so far: [0] the GPU thread waiting for chunks of steps, [1] the GPU
- * thread's membership work (joins, removals, table uploads, graph captures,
- * issuing launches), [2] the GPU thread waiting for work, [3] the retire thread
+/* Seconds so far: [0] the GPU thread stepping (issuing the chunks' graph launches,
+ * which block while the device's launch queue is full, and waiting for chunks),
+ * [1] the GPU thread's membership work (joins, removals, table uploads, graph
+ * captures), [2] the GPU thread waiting for work, [3] the retire thread
  * (solutions copied back, device memory freed), [4] device time of the chunks
- * (CUDA events on the batch stream). */
-int hgg_server_timing(hgg_server *s, double *t5);
+ * (CUDA events on the batch stream); parts of [1]: [5] joins, [6] table uploads
+ * and graph captures; part of [3]: [7] copies back. */
+int hgg_server_timing(hgg_server *s, double *t8);
 
 const char *hgg_server_last_error(hgg_server *s);
 

@@ -39,7 +39,8 @@ PROBLEMS = [
     ([4, 3, 5], False, 3, "advection", [-0.5, 0.2, 0.9], "RK4_4", 2e-3, 8),
     ([4, 4, 2], False, 2, "advection", [0.3, 0.3, -0.6], "RK4_4", 1e-3, 3),  # tensor, 3D
     ([2, 2, 2], True, 2, "wave", [1.0], "RK4_4", 1e-3, 5),              # dense, tets, wave
-    ([6, 6], False, 1, "wave", [2.0], "RK4_4", 1e-3, 4),                # dense, squares, wave
+    ([6, 6], False, 1, "wave", [2.0], "RK4_4", 1e-3, 4),                # wave tiles, squares
+    ([4, 4, 4], True, 2, "wave", [1.0], "RK4_4", 1e-3, 5),              # wave tiles, tets
     ([8, 8], False, 2, "advection", [1.0, 0.5], "DormandPrince", 1e-3, 3),  # other tableau
     ([32, 32], True, 4, "advection", [0.8, -0.6], "RK4_4", 2e-4, 4),  # folded operator, tiles
     ([32, 32], True, 5, "advection", [-0.6, 0.8], "RK4_4", 1e-4, 6),

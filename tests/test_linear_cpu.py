@@ -87,9 +87,10 @@ def test_boundary_face_matrices_match_oracle_assembly(description, p, physics, p
 
 @pytest.mark.parametrize("description,p", [(CASES[7][0], 2), (CASES[8][0], 2), (CASES[6][0], 3)])
 def test_upwind_wave_matrices_give_the_matrix_free_upwind_operator(description, p):
-    """The folded form of the upwind wave (the mixed forms fold the wave onto the
-    tensor-core tiles): its stored matrices, applied as HpgemAPILinear applies them,
-    give the matrix-free oracle's upwind right-hand side."""
+    """The folded form of the upwind wave (split-BF16 runs the wave as folded
+    tensor-core tiles; HpgemAPILinear takes 'wave_upwind'): its stored matrices,
+    applied as HpgemAPILinear applies them, give the matrix-free oracle's upwind
+    right-hand side."""
     from oracle.dg import WAVE_UPWIND
     prob = Problem(mesh_from_description(description), p, WAVE_UPWIND, cinv=0.7)
     D = linear_descriptor(description, p, 2, [0.7])
@@ -164,7 +165,9 @@ def test_linear_create_reports_a_missing_device_or_succeeds():
 
 def test_python_class_takes_the_linear_applications_only():
     with pytest.raises(ValueError):
-        hpgem_b200.HpgemAPILinear(2, 2, "wave_upwind")
+        hpgem_b200.HpgemAPILinear(2, 2, "euler")
+    # the upwind wave folds the same way as the reference's central one
+    assert hpgem_b200.HpgemAPILinear(2, 2, "wave_upwind").numberOfVariables == 3
 
 
 def test_linear_mesh_file_reports_a_missing_device_or_succeeds():
