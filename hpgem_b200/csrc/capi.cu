@@ -665,7 +665,8 @@ int hgg_step(hgg_handle *h, double *time, double dt, int32_t nsteps) {
             int64_t before = h->launches;
             int rc = enqueue_step(h, from, dt);
             cudaError_t ce = cudaStreamEndCapture(h->stream, &g);
-            h->launches = before;  // capture does not launch
+            h->graph_launches = h->launches - before;  // kernels of one captured step
+            h->launches = before;                      // capture does not launch
             if (rc) {
                 if (g) cudaGraphDestroy(g);
                 return rc;
@@ -685,7 +686,7 @@ int hgg_step(hgg_handle *h, double *time, double dt, int32_t nsteps) {
             if (rc) return rc;
         }
         HGG_CUDA(h, cudaGraphLaunch(h->graph[h->cur], h->stream));
-        h->launches += h->S;
+        h->launches += h->graph_launches;
         h->cur = 1 - h->cur;
         if (time) *time += dt;
     }

@@ -100,6 +100,7 @@ struct hgg_handle {
     hgg::SourceState *src = nullptr;    // set: every stage adds the caller's source terms
     bool store_last = true;
     int64_t launches = 0;
+    int64_t graph_launches = 0;  // kernels in one captured step
     // graph of one full step, per starting buffer, valid for (dt, store_last)
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     double graph_dt = 0.0;
