@@ -33,7 +33,7 @@ EXPORTED = ["hgg_create", "hgg_destroy", "hgg_last_error", "hgg_set_state", "hgg
             "hgg_batch_create", "hgg_batch_destroy", "hgg_batch_last_error", "hgg_batch_add",
             "hgg_batch_remove", "hgg_batch_step", "hgg_batch_synchronize", "hgg_batch_remaining",
             "hgg_batch_set_autotune", "hgg_batch_launch_count", "hgg_batch_num_classes",
-            "hgg_batch_class_info", "hgg_batch_profile_step",
+            "hgg_batch_class_info", "hgg_batch_profile_step", "hgg_batch_stream",
             "hgg_server_start", "hgg_server_submit", "hgg_server_poll", "hgg_server_result_length",
             "hgg_server_release", "hgg_server_times", "hgg_server_stats", "hgg_server_timing",
             "hgg_server_last_error",
@@ -131,6 +131,7 @@ def load():
         "hgg_batch_num_classes": (ctypes.c_int32, [B]),
         "hgg_batch_class_info": (ctypes.c_int, [B, ctypes.c_int32, P]),
         "hgg_batch_profile_step": (ctypes.c_int, [B, P, ctypes.c_int32]),
+        "hgg_batch_stream": (ctypes.c_void_p, [B]),
         "hgg_server_start": (ctypes.c_int, [ctypes.c_int64, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                             ctypes.POINTER(ctypes.c_void_p)]),
         "hgg_server_submit": (ctypes.c_int, [B, ctypes.c_char_p, ctypes.c_int32, ctypes.c_int32, P, ctypes.c_int32,

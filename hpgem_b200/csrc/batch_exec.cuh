@@ -1114,6 +1114,8 @@ int32_t hgg_batch_num_classes(const hgg_batch *b) {
     return n;
 }
 
+void *hgg_batch_stream(const hgg_batch *b) { return b ? (void *)b->stream : nullptr; }
+
 int hgg_batch_class_info(const hgg_batch *b, int32_t i, int64_t *info10) {
     if (!b || !info10) return HGG_ERR_INVALID;
     int k = -1;

@@ -55,6 +55,15 @@ __device__ __forceinline__ double stage_input(const StageIOT<KT> &io, int64_t id
     return w;
 }
 
+// the same for the common case of at most one stage vector in the input (the explicit
+// RK4, midpoint and Heun tableaux), without a loop the compiler cannot unroll
+template <typename KT>
+__device__ __forceinline__ double stage_input_few(const StageIOT<KT> &io, int64_t idx) {
+    if (io.nin == 0) return io.u[idx];
+    if (io.nin == 1) return io.u[idx] + io.cin[0] * (double)io.kin[0][idx];
+    return stage_input(io, idx);
+}
+
 // this stage's derivative k of entry idx (stored as KT) and, in the final stage,
 // the new solution u + sum_j bfin_j k_j + blast k accumulated in FP64
 template <typename KT>
@@ -659,29 +668,48 @@ __device__ __forceinline__ void wave_group_body(const StageIOT<KT> &io, const De
     group_tile_setup<NFL>(g, tiles, tile, io.n_elements, ti);
     group_stage_geometry<CT, EG, NFL * DIM>(g, ti.tel, io.n_elements, GE, GS);
     group_stage_operators<CT, DIM, NFL, NB>(g, ti.self_pair, ti.nbr_pair, OP);
-    for (int k = tid; k < TE * R; k += blockDim.x) {
+    // The block has exactly TE * NB threads, so both gathers below take a fixed number of
+    // passes per thread (V and NFL): unrolled, every pass's loads are issued before the
+    // first is used.
+    constexpr int T = TE * NB;
+#pragma unroll
+    for (int it = 0; it < SH::V; ++it) {
+        const int k = tid + it * T;
         const int l = k / R, rr = k % R;
         const int32_t ee = ti.tel[l];
         double v = 0.0;
-        if (ee >= 0 && ee < io.n_elements) v = stage_input(io, (int64_t)ee * R + rr);
+        if (ee >= 0 && ee < io.n_elements) v = stage_input_few(io, (int64_t)ee * R + rr);
         W[l * WS + rr] = (CT)v;
+    }
+    // neighbour indices of every pass first, then their values
+    int32_t nbi[NFL];
+#pragma unroll
+    for (int it = 0; it < NFL; ++it) {
+        const int k = tid + it * T;
+        const int l = k / (NFL * NB), f = (k / NB) % NFL;
+        const int32_t ee = ti.tel[l];
+        nbi[it] = -2;  // padding element
+        if (ee >= 0 && ee < io.n_elements) {
+            const int32_t n = g.nbr[(int64_t)ee * NFL + f];
+            nbi[it] = n >= 0 && n < io.n_elements ? n : -1;
+        }
     }
     __syncthreads();  // GE staged (the neighbour loop reads the normals)
     // neighbours: pressure and n . s (this element's normal) per face and basis row
-    for (int k = tid; k < TE * NFL * NB; k += blockDim.x) {
-        const int l = k / (NFL * NB), f = (k / NB) % NFL, j = k % NB;
-        const int32_t ee = ti.tel[l];
-        double pn = 0.0, jn = 0.0;
-        if (ee >= 0 && ee < io.n_elements) {
-            const int32_t n = g.nbr[(int64_t)ee * NFL + f];
-            if (n >= 0 && n < io.n_elements) {
-                const double *nu = GE + l * GS + EG + f * DIM;
-                pn = stage_input(io, (int64_t)n * R + j);
 #pragma unroll
-                for (int d = 0; d < DIM; ++d) jn += nu[d] * (double)(CT)stage_input(io, (int64_t)n * R + (d + 1) * NB + j);
-            } else {
-                atomicOr(io.status, 1);
-            }
+    for (int it = 0; it < NFL; ++it) {
+        const int k = tid + it * T;
+        const int l = k / (NFL * NB), f = (k / NB) % NFL, j = k % NB;
+        const int32_t n = nbi[it];
+        double pn = 0.0, jn = 0.0;
+        if (n >= 0) {
+            const double *nu = GE + l * GS + EG + f * DIM;
+            pn = stage_input_few(io, (int64_t)n * R + j);
+#pragma unroll
+            for (int d = 0; d < DIM; ++d)
+                jn += nu[d] * (double)(CT)stage_input_few(io, (int64_t)n * R + (d + 1) * NB + j);
+        } else if (n == -1) {
+            atomicOr(io.status, 1);
         }
         WN[l * WNS + f * 2 * NB + j] = (CT)pn;
         WN[l * WNS + f * 2 * NB + NB + j] = (CT)jn;

@@ -465,6 +465,10 @@ int hgg_batch_set_autotune(hgg_batch *b, int32_t enable);
 int64_t hgg_batch_launch_count(const hgg_batch *b);
 int32_t hgg_batch_num_classes(const hgg_batch *b);
 
+/* The batch's own CUDA stream (every step is enqueued on it): for timing with
+ * CUDA events.  No counterpart in the reference. */
+void *hgg_batch_stream(const hgg_batch *b);
+
 /* Kernel class i (0 .. hgg_batch_num_classes - 1, classes with members):
  * info10 = kind (0 matrix-free dense, 1 sum-factorised, 2 sum-factorised slices,
  * 3 stored-matrix tiles, 4 tensor-core tiles), shape, dim, order, physics,
