@@ -146,10 +146,32 @@ void *vector_ptr(hgg_handle *h, int vec) {
 bool vector_is_float(const hgg_handle *h, int vec) { return h->mixed && vec >= 1; }
 
 
+// the stages run the grouped wave kernel (the choice launch_dense makes) and every stage
+// input has exactly one earlier vector, the previous one: each stage then forms the next
+// stage's input in its output phase (the value the next stage would form itself)
+bool forms_next_input(const hgg_handle *h) {
+    if (!h->d_win[0] || h->src || h->linear || h->op.tensor || h->group_tiles <= 0) return false;
+    const bool fp64_contraction = !h->mixed || h->op.nB > kMixedFp32MaxBasis;
+    if (!(h->variant == 2 || (h->variant == 0 && fp64_contraction))) return false;
+    const int S = h->S;
+    for (int i = 1; i < S; ++i)
+        for (int j = 0; j < i; ++j)
+            if ((h->rk_a[i * S + j] != 0.0) != (j == i - 1)) return false;
+    return true;
+}
+
 template <typename KT>
 int enqueue_step_t(hgg_handle *h, int from, double dt) {
+    const bool fuse = forms_next_input(h);
     for (int i = 0; i < h->S; ++i) {
-        const StageIOT<KT> io = make_stage_io<KT>(h, from, dt, i, h->d_status);
+        StageIOT<KT> io = make_stage_io<KT>(h, from, dt, i, h->d_status);
+        if (fuse) {
+            if (i > 0) io.win = h->d_win[(i - 1) & 1];
+            if (i < h->S - 1) {
+                io.wnext = h->d_win[i & 1];
+                io.wcoef = dt * h->rk_a[(i + 1) * h->S + i];
+            }
+        }
         int rc = launch_stage(h, io);
         if (!rc && h->src) rc = enqueue_source(h, from, i, io.kout, io.unew, io.blast);
         if (rc) return rc;
@@ -414,6 +436,8 @@ int create_from_desc(const hgg_problem_desc *desc, hgg_handle *h, bool linear = 
             if (n_tiles * kGroupTile <= 2 * op.nE) {
                 if ((rc = upload(h, tiles, &h->d_group_tiles))) return rc;
                 h->group_tiles = n_tiles;
+                for (int i = 0; i < 2; ++i)
+                    if ((rc = alloc(h, sizeof(double) * h->N_alloc, (void **)&h->d_win[i]))) return rc;
             }
         }
         if ((rc = upload(h, transposed(op.vol), &h->d_vol)) || (rc = upload(h, transposed(op.pairs), &h->d_pairs)) ||

@@ -43,6 +43,13 @@ struct StageIOT {
     double blast;                    // dt * b_S for the derivative computed in this stage
     int64_t n_elements;
     int *status;                     // device status word, bit 0: bad neighbour index
+    // The grouped wave kernel with a tableau whose every stage input has one earlier
+    // vector, the previous one (explicit RK4, midpoint): the stage input was formed by
+    // the previous stage (win, else null), and this stage forms the next one
+    // (wnext = u + wcoef k, else null), so the gathers read one vector instead of two.
+    const double *win;
+    double *wnext;
+    double wcoef;
 };
 using StageIO = StageIOT<double>;
 
@@ -59,6 +66,7 @@ __device__ __forceinline__ double stage_input(const StageIOT<KT> &io, int64_t id
 // RK4, midpoint and Heun tableaux), without a loop the compiler cannot unroll
 template <typename KT>
 __device__ __forceinline__ double stage_input_few(const StageIOT<KT> &io, int64_t idx) {
+    if (io.win) return io.win[idx];  // the same value, formed by the previous stage
     if (io.nin == 0) return io.u[idx];
     if (io.nin == 1) return io.u[idx] + io.cin[0] * (double)io.kin[0][idx];
     return stage_input(io, idx);
@@ -73,6 +81,22 @@ __device__ __forceinline__ void stage_output(const StageIOT<KT> &io, int64_t idx
         double r = u;
 #pragma unroll 1
         for (int j = 0; j < io.nfin; ++j) r += io.bfin[j] * (double)io.kfin[j][idx];
+        r += io.blast * k;
+        io.unew[idx] = r;
+    }
+}
+
+// stage_output with the final update's loop unrolled (predicated on nfin, same
+// summation order), so its loads issue together
+template <typename KT>
+__device__ __forceinline__ void stage_output_few(const StageIOT<KT> &io, int64_t idx, double u, double k) {
+    if (io.kout) io.kout[idx] = (KT)k;
+    if (io.wnext) io.wnext[idx] = u + io.wcoef * (double)(KT)k;  // as stage_input_few forms it
+    if (io.unew) {
+        double r = u;
+#pragma unroll
+        for (int j = 0; j < kMaxStages; ++j)
+            if (j < io.nfin) r += io.bfin[j] * (double)io.kfin[j][idx];
         r += io.blast * k;
         io.unew[idx] = r;
     }
@@ -295,17 +319,16 @@ __device__ __forceinline__ void dense_stage_body(const StageIOT<KT> &io, const D
     if (active) {
         const int64_t idx = e * R + r;
         u_own = io.u[idx];
-        double w = u_own;
-        for (int j = 0; j < io.nin; ++j) w += io.cin[j] * (double)io.kin[j][idx];
-        W[el * R + r] = (CT)w;
+        W[el * R + r] = (CT)stage_input_few(io, idx);
     }
+#pragma unroll 4
     for (int i = tid; i < epb * NFL * R; i += blockDim.x) {
         const int l = i / (NFL * R), f = (i / R) % NFL, rr = i % R;
         const int64_t ee = e0 + l;
         double v = 0.0;
         if (ee < io.n_elements && !(WAVE == 0 && g.mode[ee * NFL + f] == 1)) {
             const int32_t n = g.nbr[ee * NFL + f];
-            if (n >= 0 && n < io.n_elements) v = stage_input(io, (int64_t)n * R + rr);
+            if (n >= 0 && n < io.n_elements) v = stage_input_few(io, (int64_t)n * R + rr);
             else atomicOr(io.status, 1);
         }
         WN[(size_t)(l * NFL + f) * R + rr] = (CT)v;
@@ -426,18 +449,17 @@ __device__ __forceinline__ void wave_stage_body(const StageIOT<KT> &io, const De
         for (int v = 0; v < V; ++v) {
             const int64_t idx = e * R + v * NB + i;
             u_own[v] = io.u[idx];
-            double w = u_own[v];
-            for (int j = 0; j < io.nin; ++j) w += io.cin[j] * (double)io.kin[j][idx];
-            W[el * R + v * NB + i] = (CT)w;
+            W[el * R + v * NB + i] = (CT)stage_input_few(io, idx);
         }
     }
+#pragma unroll 4
     for (int k = tid; k < epb * NFL * R; k += blockDim.x) {
         const int l = k / (NFL * R), f = (k / R) % NFL, rr = k % R;
         const int64_t ee = e0 + l;
         double v = 0.0;
         if (ee < io.n_elements) {
             const int32_t n = g.nbr[ee * NFL + f];
-            if (n >= 0 && n < io.n_elements) v = stage_input(io, (int64_t)n * R + rr);
+            if (n >= 0 && n < io.n_elements) v = stage_input_few(io, (int64_t)n * R + rr);
             else atomicOr(io.status, 1);
         }
         WN[(size_t)(l * NFL + f) * R + rr] = (CT)v;
@@ -602,41 +624,6 @@ __device__ __forceinline__ void group_tile_setup(const DenseGeom &g, const int32
     __syncthreads();
 }
 
-// geometry record of tile element l: elem_geo (EG values) then face_geo (FG values)
-template <typename CT, int EG, int FG>
-__device__ __forceinline__ void group_stage_geometry(const DenseGeom &g, const int32_t *tel, int64_t n_elements,
-                                                     double *GE, int GS) {
-    for (int k = threadIdx.x; k < kGroupTile * (EG + FG); k += blockDim.x) {
-        const int l = k / (EG + FG), q = k % (EG + FG);
-        const int32_t e = tel[l];
-        double v = 0.0;
-        if (e >= 0 && e < n_elements) v = q < EG ? g.elem_geo[(int64_t)e * EG + q] : g.face_geo[(int64_t)e * FG + q - EG];
-        GE[l * GS + q] = v;
-    }
-}
-
-// The tile's operators in shared memory, transposed as in global memory
-// ([..][j][i]): the DIM volume operators, then per face the self-pair and the
-// neighbour-pair operator of the tile's signature (faces whose upwind mode
-// does not use one get zeros there; they are not read).
-template <typename CT, int DIM, int NFL, int NB>
-__device__ __forceinline__ void group_stage_operators(const DenseGeom &g, const int32_t *self_pair,
-                                                      const int32_t *nbr_pair, CT *OP) {
-    const CT *gvol = dense_vol<CT>(g), *gpairs = dense_pairs<CT>(g);
-    constexpr int NN = NB * NB, TOT = (DIM + 2 * NFL) * NN;
-    for (int k = threadIdx.x; k < TOT; k += blockDim.x) {
-        const int m = k / NN, q = k % NN;
-        CT v;
-        if (m < DIM) v = gvol[(size_t)m * NN + q];
-        else {
-            const int f = (m - DIM) >> 1;
-            const int32_t pair = ((m - DIM) & 1) ? nbr_pair[f] : self_pair[f];
-            v = gpairs[(size_t)pair * NN + q];
-        }
-        OP[k] = v;
-    }
-}
-
 // Acoustic wave in 2D and 3D (the arithmetic of wave_stage_body).  Shared:
 // W [tile][R] stage inputs (then the outputs), WN [tile][NFL][2 NB] neighbour
 // pressure and n . s_n per face, X [tile][DIM + NFL][NB] t_c and n . s, GE
@@ -666,12 +653,42 @@ __device__ __forceinline__ void wave_group_body(const StageIOT<KT> &io, const De
     __shared__ GroupTileInfo<NFL> ti;
     const int tid = threadIdx.x, el = tid & (TE - 1), i = tid / TE;
     group_tile_setup<NFL>(g, tiles, tile, io.n_elements, ti);
-    group_stage_geometry<CT, EG, NFL * DIM>(g, ti.tel, io.n_elements, GE, GS);
-    group_stage_operators<CT, DIM, NFL, NB>(g, ti.self_pair, ti.nbr_pair, OP);
-    // The block has exactly TE * NB threads, so both gathers below take a fixed number of
-    // passes per thread (V and NFL): unrolled, every pass's loads are issued before the
-    // first is used.
-    constexpr int T = TE * NB;
+    constexpr int T = TE * NB;  // the block's threads (see the gathers below)
+    {
+        constexpr int Q = EG + NFL * DIM, NG = (TE * Q + T - 1) / T;
+#pragma unroll
+        for (int it = 0; it < NG; ++it) {
+            const int k = tid + it * T;
+            if (k < TE * Q) {
+                const int l = k / Q, q = k % Q;
+                const int32_t e = ti.tel[l];
+                double v = 0.0;
+                if (e >= 0 && e < io.n_elements)
+                    v = q < EG ? g.elem_geo[(int64_t)e * EG + q] : g.face_geo[(int64_t)e * (NFL * DIM) + q - EG];
+                GE[l * GS + q] = v;
+            }
+        }
+        constexpr int NN = NB * NB, TOT = (DIM + 2 * NFL) * NN, NO = (TOT + T - 1) / T;
+        const CT *gvol = dense_vol<CT>(g), *gpairs = dense_pairs<CT>(g);
+#pragma unroll 1
+        for (int it = 0; it < NO; ++it) {
+            const int k = tid + it * T;
+            if (k < TOT) {
+                const int m = k / NN, q = k % NN;
+                CT v;
+                if (m < DIM) v = gvol[(size_t)m * NN + q];
+                else {
+                    const int f = (m - DIM) >> 1;
+                    const int32_t pair = ((m - DIM) & 1) ? ti.nbr_pair[f] : ti.self_pair[f];
+                    v = gpairs[(size_t)pair * NN + q];
+                }
+                OP[k] = v;
+            }
+        }
+    }
+    // The block has exactly T = TE * NB threads, so every staging loop takes a fixed
+    // number of passes per thread (the gathers below: V and NFL): unrolled, every pass's
+    // loads are issued before the first is used.
 #pragma unroll
     for (int it = 0; it < SH::V; ++it) {
         const int k = tid + it * T;
@@ -800,12 +817,14 @@ __device__ __forceinline__ void wave_group_body(const StageIOT<KT> &io, const De
         }
     }
     __syncthreads();
-    for (int k = tid; k < TE * R; k += blockDim.x) {
+#pragma unroll
+    for (int it = 0; it < SH::V; ++it) {
+        const int k = tid + it * T;
         const int l = k / R, rr = k % R;
         const int32_t ee = ti.tel[l];
         if (ee < 0 || ee >= io.n_elements) continue;
         const int64_t idx = (int64_t)ee * R + rr;
-        stage_output(io, idx, io.u[idx], (double)W[l * WS + rr]);
+        stage_output_few(io, idx, io.u[idx], (double)W[l * WS + rr]);
     }
 }
 

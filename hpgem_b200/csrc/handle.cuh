@@ -89,6 +89,7 @@ struct hgg_handle {
     unsigned char *d_umma_planes = nullptr;  // split stage input, two planes [E][KP]
     // grouped dense kernel: tiles of kGroupTile elements with the same operator signature
     int32_t *d_group_tiles = nullptr;
+    double *d_win[2] = {nullptr, nullptr};  // stage inputs formed ahead (grouped wave kernel)
     int64_t group_tiles = 0;
     int num_sms = 148;
     int *d_status = nullptr;

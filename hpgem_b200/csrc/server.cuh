@@ -91,7 +91,8 @@ thread_local std::string g_server_create_error = "no error";
 int64_t estimate_footprint(const hgg_problem_desc &d) {
     const int64_t N = d.n_elements * (int64_t)d.n_vars * d.n_basis;
     const int64_t kbytes = d.precision == HGG_PRECISION_FP32 ? 4 : 8;
-    return (3 * 8 + d.n_stages * kbytes) * (N + 64 * 64) + d.n_elements * 640 + (8 << 20);
+    const int64_t ahead = d.physics == HGG_PHYSICS_ADVECTION ? 0 : 2 * 8;  // wave: stage inputs formed ahead
+    return (3 * 8 + ahead + d.n_stages * kbytes) * (N + 64 * 64) + d.n_elements * 640 + (8 << 20);
 }
 
 void setup_loop(hgg_server *s, cudaStream_t stream) {
