@@ -57,11 +57,11 @@ class Batch:
         self._check(self._lib.hgg_batch_set_autotune(self._raw, 1 if enable else 0))
 
     @property
-    @property
     def cuda_stream(self):
         """The batch's CUDA stream handle (an integer, for torch.cuda.ExternalStream)."""
         return int(self._lib.hgg_batch_stream(self._raw) or 0)
 
+    @property
     def launch_count(self):
         return int(self._lib.hgg_batch_launch_count(self._raw))
 
