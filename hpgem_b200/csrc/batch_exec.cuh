@@ -320,8 +320,7 @@ int batch_kind(const hgg_handle *h) {
     if (h->slice_ok) return KIND_SLICE;
     if (h->op.tensor) return KIND_TENSOR;
     // the same choice as the handle's own dense launch: tiles where the contraction is FP64
-    const bool fp64_contraction = !h->mixed || h->op.nB > kMixedFp32MaxBasis;
-    if (h->group_tiles > 0 && (h->variant == 2 || (h->variant == 0 && fp64_contraction))) return KIND_WAVE_TILES;
+    if (group_wave_wanted(h)) return KIND_WAVE_TILES;
     return KIND_DENSE;
 }
 

@@ -149,10 +149,23 @@ bool vector_is_float(const hgg_handle *h, int vec) { return h->mixed && vec >= 1
 // the stages run the grouped wave kernel (the choice launch_dense makes) and every stage
 // input has exactly one earlier vector, the previous one: each stage then forms the next
 // stage's input in its output phase (the value the next stage would form itself)
+bool group_wave_wanted(const hgg_handle *h) {
+    if (h->group_tiles <= 0 || h->linear || h->op.tensor) return false;
+    if (h->variant == 2) return true;
+    if (h->variant != 0) return false;
+    const int nb = h->op.nB;
+    if (!h->mixed || nb > kMixedFp32MaxBasis) return true;  // FP64 contractions
+    // FP32 contractions: where the tile kernel measured faster than the per-row one
+    // (RK4 steps: tetrahedra p = 1 on 40^3 x 5 cells 0.57 against 0.72 ms, p = 2 on
+    // 32^3 x 5 0.83 against 0.92; triangles p = 4 on 256^2 x 2 0.84 against 0.96; meshes
+    // below 2^15 elements, e.g. 64^2 x 2 triangles p = 2, 0.035 against 0.045); the
+    // per-row kernel elsewhere (tetrahedra p = 3 on 24^3 x 5: 1.06 against 1.24 ms;
+    // triangles p <= 3 on large meshes, within 6 %)
+    return (h->op.dim == 3 && nb <= 10) || (h->op.dim == 2 && nb >= 15) || h->op.nE < 32768;
+}
+
 bool forms_next_input(const hgg_handle *h) {
-    if (!h->d_win[0] || h->src || h->linear || h->op.tensor || h->group_tiles <= 0) return false;
-    const bool fp64_contraction = !h->mixed || h->op.nB > kMixedFp32MaxBasis;
-    if (!(h->variant == 2 || (h->variant == 0 && fp64_contraction))) return false;
+    if (!h->d_win[0] || h->src || !group_wave_wanted(h)) return false;
     const int S = h->S;
     for (int i = 1; i < S; ++i)
         for (int j = 0; j < i; ++j)

@@ -143,6 +143,9 @@ int upload(hgg_handle *h, const std::vector<T> &v, T **dst) {
 }
 
 int alloc(hgg_handle *h, size_t bytes, void **dst);
+// the wave runs the grouped tile kernel (alone and in a batch): kernel variant 2, or
+// the automatic choice where it measured faster than the per-row kernel
+bool group_wave_wanted(const hgg_handle *h);
 void release_graphs(hgg_handle *h);
 // the current solution in hpGEM order with no kernel on the device: one copy of the
 // device vector into `staging` (pinned, h->N_alloc doubles), the layout change on the host

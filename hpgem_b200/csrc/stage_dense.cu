@@ -27,12 +27,12 @@ int launch_dense(hgg_handle *h, const StageIOT<KT> &io) {
     const int threads = dense_threads(DIM, WAVE, op.nB, epb);
     const bool ok = dense_dispatch<DIM, NFL, WAVE>(op.nB, [&](auto nbc) {
         constexpr int NB = decltype(nbc)::value;
-        // the grouped kernel where it measured faster: the wave with FP64 contractions
-        // (32^3 x 5 tetrahedra, p = 2, RK4: 1.12 against 2.01 ms per step upwind, 1.00
-        // against 1.71 central); with FP32 contractions, and for advection, the
-        // per-row kernel was as fast or faster (0.97 against 1.09 ms; 0.38 both)
+        // the grouped kernel where it measured faster (group_wave_wanted): the wave with
+        // FP64 contractions (32^3 x 5 tetrahedra, p = 2, RK4: 1.12 against 2.01 ms per
+        // step upwind when it was introduced), and with FP32 contractions on the meshes
+        // and orders listed there; for advection the per-row kernel was as fast (0.38 both)
         if constexpr (DIM >= 2 && NB <= kGroupMaxRows && WAVE) {
-            const bool want = h->variant == 2 || (h->variant == 0 && std::is_same_v<DenseCT<KT, NB>, double>);
+            const bool want = group_wave_wanted(h);
             if (h->group_tiles > 0 && want) {
                 constexpr size_t gsmem = group_smem<DenseCT<KT, NB>, DIM, NFL, NB>();
                 if (gsmem > 48 * 1024)
