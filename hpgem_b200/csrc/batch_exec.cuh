@@ -98,7 +98,7 @@ __global__ void __launch_bounds__(256)
 
 // the wave on tiles of elements with equal operators (one virtual block per tile)
 template <typename KT, int DIM, int NFL, int NB>
-__global__ void __launch_bounds__(kGroupTile *NB, 1024 / (kGroupTile * NB) > 0 ? 1024 / (kGroupTile * NB) : 1)
+__global__ void __launch_bounds__(group_threads(NB), 1024 / group_threads(NB) > 0 ? 1024 / group_threads(NB) : 1)
     grouped_wave_tiles(const DenseItem<KT> *items, const int *n_items, const int64_t *total, const int *parity,
                        const int *remaining) {
     const int n = *n_items;
@@ -526,11 +526,11 @@ void launch_grouped_wave(const hgg_batch *b, const BatchClass &c, int st, unsign
     const int nB = c.rep.nB;
     dense_dispatch<DIM, NFL, 1>(nB, [&](auto nbc) {
         constexpr int NB = decltype(nbc)::value;
-        if constexpr (DIM >= 2 && NB <= kGroupMaxRows) {
+        if constexpr (DIM >= 2 && NB <= kGroupMaxBasis) {
             constexpr size_t smem = group_smem<DenseCT<KT, NB>, DIM, NFL, NB>();
             cudaFuncSetAttribute(grouped_wave_tiles<KT, DIM, NFL, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem);
-            grouped_wave_tiles<KT, DIM, NFL, NB><<<grid, kGroupTile * NB, smem, s>>>(
+            grouped_wave_tiles<KT, DIM, NFL, NB><<<grid, group_threads(NB), smem, s>>>(
                 static_cast<const DenseItem<KT> *>(c.d_items[st]), c.d_n, c.d_total, b->d_parity, b->d_remaining);
         }
     });

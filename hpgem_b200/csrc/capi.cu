@@ -154,6 +154,10 @@ bool group_wave_wanted(const hgg_handle *h) {
     if (h->variant == 2) return true;
     if (h->variant != 0) return false;
     const int nb = h->op.nB;
+    // 16-element tiles (above 24 basis functions): faster on large meshes only (RK4 steps:
+    // tetrahedra p = 4 on 24^3 x 5 cells 4.21 against 4.65 ms, quadrilaterals p = 4 on
+    // 192^2 0.88 against 1.08; equal on 16^3 x 5 tetrahedra and hexahedra p = 2 on 40^3)
+    if (nb > kGroupMaxRows) return h->op.nE >= 65536;
     if (!h->mixed || nb > kMixedFp32MaxBasis) return true;  // FP64 contractions
     // FP32 contractions: where the tile kernel measured faster than the per-row one
     // (RK4 steps: tetrahedra p = 1 on 40^3 x 5 cells 0.57 against 0.72 ms, p = 2 on
@@ -406,9 +410,10 @@ int create_from_desc(const hgg_problem_desc *desc, hgg_handle *h, bool linear = 
                 return rc;
         }
         // tiles of the grouped kernel (the wave): elements ordered by their operator
-        // signature (pair operators of every face), kGroupTile per tile within a
+        // signature (pair operators of every face), group_tile_elems(nB) per tile within a
         // group; used when the tiles are at least half full on average
         if (group_rows(op.dim, op.physics != HGG_PHYSICS_ADVECTION, op.nB) > 0) {
+            const int TE = group_tile_elems(op.nB);
             const int nf = op.nfl;
             auto sig_less = [&](int64_t x, int64_t y) {
                 for (int f = 0; f < nf; ++f) {
@@ -423,30 +428,30 @@ int create_from_desc(const hgg_problem_desc *desc, hgg_handle *h, bool linear = 
             for (int64_t e = 0; e < op.nE; ++e) order[e] = e;
             std::stable_sort(order.begin(), order.end(), sig_less);
             std::vector<int32_t> tiles;
-            int fill = kGroupTile;
+            int fill = TE;
             for (size_t i = 0; i < order.size(); ++i) {
                 const bool same = i > 0 && !sig_less(order[i - 1], order[i]) && !sig_less(order[i], order[i - 1]);
-                if (!same || fill == kGroupTile) {
-                    tiles.insert(tiles.end(), kGroupTile, -1);
+                if (!same || fill == TE) {
+                    tiles.insert(tiles.end(), TE, -1);
                     fill = 0;
                 }
-                tiles[tiles.size() - kGroupTile + fill++] = (int32_t)order[i];
+                tiles[tiles.size() - TE + fill++] = (int32_t)order[i];
             }
-            const int64_t n_tiles = (int64_t)(tiles.size() / kGroupTile);
+            const int64_t n_tiles = (int64_t)(tiles.size() / TE);
             // run the tiles in the order of their first element, not group by group:
             // the neighbours a tile gathers then belong to tiles of the other groups
             // that run at about the same time, while they are still in L2
             std::vector<int64_t> torder(n_tiles);
             for (int64_t t = 0; t < n_tiles; ++t) torder[t] = t;
             std::stable_sort(torder.begin(), torder.end(), [&](int64_t x, int64_t y) {
-                return tiles[x * kGroupTile] < tiles[y * kGroupTile];
+                return tiles[x * TE] < tiles[y * TE];
             });
             std::vector<int32_t> sorted(tiles.size());
             for (int64_t t = 0; t < n_tiles; ++t)
-                std::copy(tiles.begin() + torder[t] * kGroupTile, tiles.begin() + (torder[t] + 1) * kGroupTile,
-                          sorted.begin() + t * kGroupTile);
+                std::copy(tiles.begin() + torder[t] * TE, tiles.begin() + (torder[t] + 1) * TE,
+                          sorted.begin() + t * TE);
             tiles.swap(sorted);
-            if (n_tiles * kGroupTile <= 2 * op.nE) {
+            if (n_tiles * TE <= 2 * op.nE) {
                 if ((rc = upload(h, tiles, &h->d_group_tiles))) return rc;
                 h->group_tiles = n_tiles;
                 for (int i = 0; i < 2; ++i)

@@ -592,7 +592,10 @@ __global__ void __launch_bounds__(256) dense_stage(const StageIOT<KT> io, const 
 // odd strides (in elements of CT), so the lanes' reads hit distinct banks.  The
 // stage inputs are staged and the outputs written through shared memory, both
 // coalesced along an element's coefficients.
-constexpr int kGroupTile = 32;
+constexpr int kGroupTile = 32;  // elements per tile up to 24 basis functions
+// elements per tile: 32 (a warp of lanes per basis row), 16 above 24 basis functions (a
+// warp then covers two basis rows of 16 elements; the block stays within 1024 threads)
+__host__ __device__ constexpr int group_tile_elems(int nb) { return nb <= 24 ? 32 : 16; }
 
 // odd stride (in CT elements) at least n
 __host__ __device__ constexpr int odd_stride(int n) { return n | 1; }
@@ -609,13 +612,13 @@ struct GroupTileInfo {
     int8_t mode[NFL];
 };
 
-template <int NFL>
+template <int NFL, int TE>
 __device__ __forceinline__ void group_tile_setup(const DenseGeom &g, const int32_t *tiles, int64_t tile,
                                                  int64_t n_elements, GroupTileInfo<NFL> &ti) {
     const int tid = threadIdx.x;
-    if (tid < kGroupTile) ti.tel[tid] = tiles[tile * kGroupTile + tid];
+    if (tid < TE) ti.tel[tid] = tiles[tile * TE + tid];
     if (tid < NFL) {
-        const int32_t e0 = tiles[tile * kGroupTile];  // the first slot of a tile is never padding
+        const int32_t e0 = tiles[tile * TE];  // the first slot of a tile is never padding
         const bool ok = e0 >= 0 && e0 < n_elements;
         ti.self_pair[tid] = ok ? g.self_pair[(int64_t)e0 * NFL + tid] : 0;
         ti.nbr_pair[tid] = ok ? g.nbr_pair[(int64_t)e0 * NFL + tid] : 0;
@@ -630,12 +633,13 @@ __device__ __forceinline__ void group_tile_setup(const DenseGeom &g, const int32
 // [tile][DIM^2 + NFL DIM] geometry (FP64).
 template <int DIM, int NFL, int NB>
 struct WaveGroupShape {
+    static constexpr int TE = group_tile_elems(NB);
     static constexpr int V = DIM + 1, R = V * NB, EG = DIM * DIM, FG = NFL * DIM;
     static constexpr int WS = odd_stride(R), WNS = odd_stride(NFL * 2 * NB), XS = odd_stride((DIM + NFL) * NB);
     static constexpr int GS = odd_stride(EG + FG);
     static constexpr int OPS = (DIM + 2 * NFL) * NB * NB;
-    static constexpr int ELEMS = kGroupTile * (WS + WNS + XS) + OPS;  // CT elements after GE (doubles)
-    static constexpr int GEO = kGroupTile * GS;
+    static constexpr int ELEMS = TE * (WS + WNS + XS) + OPS;  // CT elements after GE (doubles)
+    static constexpr int GEO = TE * GS;
 };
 
 template <typename KT, int DIM, int NFL, int NB>
@@ -643,7 +647,7 @@ __device__ __forceinline__ void wave_group_body(const StageIOT<KT> &io, const De
                                                 int64_t tile) {
     using CT = DenseCT<KT, NB>;
     using SH = WaveGroupShape<DIM, NFL, NB>;
-    constexpr int R = SH::R, WS = SH::WS, WNS = SH::WNS, XS = SH::XS, GS = SH::GS, EG = SH::EG, TE = kGroupTile;
+    constexpr int R = SH::R, WS = SH::WS, WNS = SH::WNS, XS = SH::XS, GS = SH::GS, EG = SH::EG, TE = SH::TE;
     extern __shared__ __align__(16) unsigned char dense_shared[];
     double *GE = reinterpret_cast<double *>(dense_shared);
     CT *W = reinterpret_cast<CT *>(GE + SH::GEO);
@@ -652,7 +656,7 @@ __device__ __forceinline__ void wave_group_body(const StageIOT<KT> &io, const De
     CT *OP = X + TE * XS;  // [DIM + 2 NFL][NB][NB]
     __shared__ GroupTileInfo<NFL> ti;
     const int tid = threadIdx.x, el = tid & (TE - 1), i = tid / TE;
-    group_tile_setup<NFL>(g, tiles, tile, io.n_elements, ti);
+    group_tile_setup<NFL, TE>(g, tiles, tile, io.n_elements, ti);
     constexpr int T = TE * NB;  // the block's threads (see the gathers below)
     {
         constexpr int Q = EG + NFL * DIM, NG = (TE * Q + T - 1) / T;
@@ -828,15 +832,17 @@ __device__ __forceinline__ void wave_group_body(const StageIOT<KT> &io, const De
     }
 }
 
-// rows (warps) of a grouped block; 0: no grouped kernel (the wave in 2D and
-// 3D only).  One warp per basis row; above kGroupMaxRows rows the register
-// budget of the large block (65536 / (32 rows) per thread) makes the compiler
-// spill, and the per-element-row kernel runs instead.
+// basis rows of a grouped block; 0: no grouped kernel (the wave in 2D and 3D
+// only).  Up to 24 basis functions a tile is 32 elements (32 x NB threads), up to
+// 35 (tetrahedra at p = 4) 16 elements, whose operators (11 x 35^2 doubles) still
+// fit one block's shared memory; above that the per-element-row kernel runs.
 constexpr int kGroupMaxRows = 24;
+constexpr int kGroupMaxBasis = 35;
 __host__ __device__ inline int group_rows(int dim, int wave, int nb) {
     if (dim < 2 || !wave) return 0;
-    return nb <= kGroupMaxRows ? nb : 0;
+    return nb <= kGroupMaxBasis ? nb : 0;
 }
+__host__ __device__ constexpr int group_threads(int nb) { return group_tile_elems(nb) * nb; }
 template <typename CT, int DIM, int NFL, int NB>
 constexpr size_t group_smem() {
     using SH = WaveGroupShape<DIM, NFL, NB>;
@@ -844,8 +850,7 @@ constexpr size_t group_smem() {
 }
 
 template <typename KT, int DIM, int NFL, int NB>
-__global__ void __launch_bounds__(kGroupTile *(NB < kGroupMaxRows ? NB : kGroupMaxRows),
-                                  1024 / (kGroupTile * NB) > 0 ? 1024 / (kGroupTile * NB) : 1)
+__global__ void __launch_bounds__(group_threads(NB), 1024 / group_threads(NB) > 0 ? 1024 / group_threads(NB) : 1)
     dense_group_stage(const StageIOT<KT> io, const DenseGeom g, const int32_t *tiles) {
     wave_group_body<KT, DIM, NFL, NB>(io, g, tiles, blockIdx.x);
 }

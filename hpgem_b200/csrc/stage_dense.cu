@@ -31,7 +31,7 @@ int launch_dense(hgg_handle *h, const StageIOT<KT> &io) {
         // FP64 contractions (32^3 x 5 tetrahedra, p = 2, RK4: 1.12 against 2.01 ms per
         // step upwind when it was introduced), and with FP32 contractions on the meshes
         // and orders listed there; for advection the per-row kernel was as fast (0.38 both)
-        if constexpr (DIM >= 2 && NB <= kGroupMaxRows && WAVE) {
+        if constexpr (DIM >= 2 && NB <= kGroupMaxBasis && WAVE) {
             const bool want = group_wave_wanted(h);
             if (h->group_tiles > 0 && want) {
                 constexpr size_t gsmem = group_smem<DenseCT<KT, NB>, DIM, NFL, NB>();
@@ -39,7 +39,7 @@ int launch_dense(hgg_handle *h, const StageIOT<KT> &io) {
                     cudaFuncSetAttribute(dense_group_stage<KT, DIM, NFL, NB>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gsmem);
                 dense_group_stage<KT, DIM, NFL, NB>
-                    <<<(unsigned)h->group_tiles, kGroupTile * NB, gsmem, h->stream>>>(io, g, h->d_group_tiles);
+                    <<<(unsigned)h->group_tiles, group_threads(NB), gsmem, h->stream>>>(io, g, h->d_group_tiles);
                 return;
             }
         }
