@@ -1,6 +1,6 @@
 """GPU: the grouped dense kernel of the wave (tiles of 32 elements with the
-same operator signature; lane = element, warp = basis row; FP64
-contractions) against the per-element-row kernel it replaces (kernel variant
+same operator signature, 16 above 24 basis functions; lane = element, warp =
+basis row; FP64 contractions) against the per-element-row kernel it replaces (kernel variant
 1) and against the oracle.
 
 Meshes are large enough that every group fills whole tiles (the grouped kernel
@@ -39,6 +39,9 @@ CASES = [
     ("tetrahedra p2 wave", [4, 4, 4], 2, "wave", [1.3], 1e-3, 5, True),
     ("tetrahedra p2 upwind wave", [4, 4, 4], 2, "wave_upwind", [0.8], 1e-3, 5, True),
     ("tetrahedra p3 upwind wave", [4, 4, 4], 3, "wave_upwind", [1.0], 5e-4, 3, True),
+    # above 24 basis functions: tiles of 16 elements (a warp covers two basis rows)
+    ("tetrahedra p4 upwind wave, 16-element tiles", [4, 4, 4], 4, "wave_upwind", [1.0], 2e-4, 3, True),
+    ("quadrilaterals p4 wave, 16-element tiles", [8, 8], 4, "wave", [1.1], 2e-4, 4, False),
 ]
 
 
@@ -58,7 +61,7 @@ def test_grouped_kernel_matches_row_kernel_and_oracle(name, cells, order, physic
     prob = oracle_for(cells, order, physics, params, tri)
     u0 = np.random.default_rng(9).standard_normal(prob.n_dof)
     out = {}
-    for variant in (0, 1):
+    for variant in (2, 1):  # the grouped kernel wherever the mesh forms tiles, the per-row kernel
         s = solver_for(cells, order, physics, params, tri)
         assert s.handle.kernel_kind == "dense"
         h = s.handle
@@ -72,17 +75,17 @@ def test_grouped_kernel_matches_row_kernel_and_oracle(name, cells, order, physic
     M = np.einsum("q,qi,qj->ij", prob.rule.weights, prob.phi, prob.phi)
     stage_tol = max(RTOL, 4.0 * np.linalg.cond(M) * EPS)
     # the two organisations do the same arithmetic up to the compiler's FMA contraction
-    assert rel_err(out[0][0], out[1][0]) < stage_tol, name
-    assert rel_err(out[0][1], out[1][1]) < RTOL, name
-    assert rel_err(out[0][0], prob.time_derivative(u0).reshape(-1)) < stage_tol, name
-    assert rel_err(out[0][1], prob.step(u0, dt, steps).reshape(-1)) < RTOL, name
+    assert rel_err(out[2][0], out[1][0]) < stage_tol, name
+    assert rel_err(out[2][1], out[1][1]) < RTOL, name
+    assert rel_err(out[2][0], prob.time_derivative(u0).reshape(-1)) < stage_tol, name
+    assert rel_err(out[2][1], prob.step(u0, dt, steps).reshape(-1)) < RTOL, name
 
 
 @pytest.mark.parametrize("name,cells,order,physics,params,dt,steps,tri", [CASES[1], CASES[6]],
                          ids=[CASES[i][0] for i in (1, 6)])
 def test_mixed_form_beside_the_grouped_fp64_kernel(name, cells, order, physics, params, dt, steps, tri):
-    """The FP32-mixed form (per-row kernel, FP32 contractions) stays within 1e-6 (L2)
-    of the grouped FP64 solution."""
+    """The FP32-mixed form (FP32 contractions) stays within 1e-6 (L2) of the grouped
+    FP64 solution."""
     u0 = np.random.default_rng(9).standard_normal(oracle_for(cells, order, physics, params, tri).n_dof)
     res = {}
     for prec in (_native.PRECISION_FP64, _native.PRECISION_FP32):
