@@ -295,6 +295,10 @@ struct hgg_batch {
     std::vector<int> graph_sig;  // (class, epb, ctas per SM, grid) of the captured step
     bool dirty = true;
     bool autotune = true;
+    // launch_class_stage in query mode: the class's kernel is not launched, its resident
+    // CTAs per SM are recorded instead (the default persistent grid)
+    bool occ_query = false;
+    mutable int occ_result = 0;
     int64_t launches = 0;
     std::string err = "no error";
 };
@@ -500,6 +504,19 @@ int upload_class(hgg_batch *b, BatchClass &c) {
     return 0;
 }
 
+// launches a class kernel, or in query mode records how many of its CTAs fit on an SM
+template <typename Kern, typename... A>
+void class_kernel(const hgg_batch *b, Kern kern, unsigned grid, unsigned threads, size_t smem, cudaStream_t s,
+                  A... args) {
+    if (b->occ_query) {
+        int n = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kern, (int)threads, smem) == cudaSuccess)
+            b->occ_result = n;
+        return;
+    }
+    kern<<<grid, threads, smem, s>>>(args...);
+}
+
 template <typename KT, int DIM, int NFL, int WAVE>
 void launch_grouped_dense(const hgg_batch *b, const BatchClass &c, int st, unsigned grid, cudaStream_t s) {
     const int nB = c.rep.nB;
@@ -510,8 +527,9 @@ void launch_grouped_dense(const hgg_batch *b, const BatchClass &c, int st, unsig
         if (smem > 48 * 1024)
             cudaFuncSetAttribute(grouped_dense<KT, DIM, NFL, WAVE, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem);
-        grouped_dense<KT, DIM, NFL, WAVE, NB><<<grid, threads, smem, s>>>(
-            static_cast<const DenseItem<KT> *>(c.d_items[st]), c.d_n, c.d_total, b->d_parity, b->d_remaining);
+        class_kernel(b, grouped_dense<KT, DIM, NFL, WAVE, NB>, grid, threads, smem, s,
+                     static_cast<const DenseItem<KT> *>(c.d_items[st]), c.d_n, c.d_total, b->d_parity,
+                     b->d_remaining);
     });
 }
 
@@ -530,8 +548,9 @@ void launch_grouped_wave(const hgg_batch *b, const BatchClass &c, int st, unsign
             constexpr size_t smem = group_smem<DenseCT<KT, NB>, DIM, NFL, NB>();
             cudaFuncSetAttribute(grouped_wave_tiles<KT, DIM, NFL, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem);
-            grouped_wave_tiles<KT, DIM, NFL, NB><<<grid, group_threads(NB), smem, s>>>(
-                static_cast<const DenseItem<KT> *>(c.d_items[st]), c.d_n, c.d_total, b->d_parity, b->d_remaining);
+            class_kernel(b, grouped_wave_tiles<KT, DIM, NFL, NB>, grid, group_threads(NB), smem, s,
+                         static_cast<const DenseItem<KT> *>(c.d_items[st]), c.d_n, c.d_total, b->d_parity,
+                         b->d_remaining);
         }
     });
 }
@@ -542,11 +561,13 @@ void launch_grouped_tensor(const hgg_batch *b, const BatchClass &c, int st, unsi
     constexpr int EPB = (256 / NB) > 0 ? (256 / NB) : 1;
     const TensorConsts<P, DIM> tc = tensor_consts<P, DIM>(c.rep);
     if (c.mixed)
-        grouped_tensor<float, P, DIM, EPB><<<grid, EPB * NB, 0, s>>>(
-            static_cast<const TensorItem<float> *>(c.d_items[st]), c.d_n, c.d_total, b->d_parity, b->d_remaining, tc);
+        class_kernel(b, grouped_tensor<float, P, DIM, EPB>, grid, EPB * NB, 0, s,
+                     static_cast<const TensorItem<float> *>(c.d_items[st]), c.d_n, c.d_total, b->d_parity,
+                     b->d_remaining, tc);
     else
-        grouped_tensor<double, P, DIM, EPB><<<grid, EPB * NB, 0, s>>>(
-            static_cast<const TensorItem<double> *>(c.d_items[st]), c.d_n, c.d_total, b->d_parity, b->d_remaining, tc);
+        class_kernel(b, grouped_tensor<double, P, DIM, EPB>, grid, EPB * NB, 0, s,
+                     static_cast<const TensorItem<double> *>(c.d_items[st]), c.d_n, c.d_total, b->d_parity,
+                     b->d_remaining, tc);
 }
 
 template <typename KT>
@@ -567,13 +588,17 @@ void launch_grouped_slice(const hgg_batch *b, const BatchClass &c, int st, unsig
     const auto *items = static_cast<const SliceItem<KT> *>(c.d_items[st]);
     const dim3 g(grid), blk(SliceShape::THREADS);
     if (io.nin == 0 && (!fin || io.nfin == 0))
-        grouped_slice<KT, 0, 0><<<g, blk, 0, s>>>(items, c.d_n, c.d_total, b->d_parity, b->d_remaining, sops);
+        class_kernel(b, grouped_slice<KT, 0, 0>, grid, SliceShape::THREADS, 0, s, items, c.d_n, c.d_total,
+                     b->d_parity, b->d_remaining, sops);
     else if (io.nin == 1 && (!fin || io.nfin == 0))
-        grouped_slice<KT, 1, 0><<<g, blk, 0, s>>>(items, c.d_n, c.d_total, b->d_parity, b->d_remaining, sops);
+        class_kernel(b, grouped_slice<KT, 1, 0>, grid, SliceShape::THREADS, 0, s, items, c.d_n, c.d_total,
+                     b->d_parity, b->d_remaining, sops);
     else if (io.nin == 1 && fin && io.nfin == 3)
-        grouped_slice<KT, 1, 3><<<g, blk, 0, s>>>(items, c.d_n, c.d_total, b->d_parity, b->d_remaining, sops);
+        class_kernel(b, grouped_slice<KT, 1, 3>, grid, SliceShape::THREADS, 0, s, items, c.d_n, c.d_total,
+                     b->d_parity, b->d_remaining, sops);
     else
-        grouped_slice<KT, -1, -1><<<g, blk, 0, s>>>(items, c.d_n, c.d_total, b->d_parity, b->d_remaining, sops);
+        class_kernel(b, grouped_slice<KT, -1, -1>, grid, SliceShape::THREADS, 0, s, items, c.d_n, c.d_total,
+                     b->d_parity, b->d_remaining, sops);
 }
 
 // one stage of one class
@@ -608,13 +633,14 @@ void launch_class_stage(hgg_batch *b, const BatchClass &c, int st, cudaStream_t 
         const dim3 pgrid((unsigned)(2 * b->num_sms), my);
         auto planes = [&](auto kc, auto nc) {
             constexpr int K = decltype(kc)::value, NIN = decltype(nc)::value;
-            grouped_umma_planes<K, NIN><<<pgrid, 256, 0, s>>>(it, c.d_n, b->d_parity, b->d_remaining, sh);
+            if (!b->occ_query)  // the planes kernel's grid is not the class's persistent grid
+                grouped_umma_planes<K, NIN><<<pgrid, 256, 0, s>>>(it, c.d_n, b->d_parity, b->d_remaining, sh);
         };
         auto tiles = [&](auto kc) {
             constexpr int K = decltype(kc)::value;
             cudaFuncSetAttribute(grouped_umma<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            grouped_umma<K><<<grid, kUmmaThreads, smem, s>>>(it, c.d_n, c.d_total, b->d_parity, b->d_remaining, sh,
-                                                             b->d_status);
+            class_kernel(b, grouped_umma<K>, grid, kUmmaThreads, smem, s, it, c.d_n, c.d_total, b->d_parity,
+                         b->d_remaining, sh, b->d_status);
         };
         using I0 = std::integral_constant<int, 0>;
         using I1 = std::integral_constant<int, 1>;
@@ -632,14 +658,15 @@ void launch_class_stage(hgg_batch *b, const BatchClass &c, int st, cudaStream_t 
             else planes(KB16{}, IM{});
             tiles(KB16{});
         }
-        b->launches++;  // the planes launch
+        if (!b->occ_query) b->launches++;  // the planes launch
     } else if (c.kind == KIND_LINEAR) {
         if (c.mixed)
-            grouped_linear<float><<<grid, 256, 0, s>>>(static_cast<const LinearItem<float> *>(c.d_items[st]), c.d_n,
-                                                       c.d_total, b->d_parity, b->d_remaining);
+            class_kernel(b, grouped_linear<float>, grid, 256, 0, s, static_cast<const LinearItem<float> *>(c.d_items[st]),
+                         c.d_n, c.d_total, b->d_parity, b->d_remaining);
         else
-            grouped_linear<double><<<grid, 256, 0, s>>>(static_cast<const LinearItem<double> *>(c.d_items[st]),
-                                                        c.d_n, c.d_total, b->d_parity, b->d_remaining);
+            class_kernel(b, grouped_linear<double>, grid, 256, 0, s,
+                         static_cast<const LinearItem<double> *>(c.d_items[st]), c.d_n, c.d_total, b->d_parity,
+                         b->d_remaining);
     } else if (c.kind == KIND_SLICE) {
         if (c.mixed) launch_grouped_slice<float>(b, c, st, grid, s);
         else launch_grouped_slice<double>(b, c, st, grid, s);
@@ -676,7 +703,7 @@ void launch_class_stage(hgg_batch *b, const BatchClass &c, int st, cudaStream_t 
             case HGG_SHAPE_CUBE: wave ? launch_grouped_dense_any<3, 6, 1>(b, c, st, grid, s) : launch_grouped_dense_any<3, 6, 0>(b, c, st, grid, s); break;
         }
     }
-    b->launches++;
+    if (!b->occ_query) b->launches++;
 }
 
 int size_bucket(int64_t elements) {
@@ -1040,6 +1067,13 @@ int hgg_batch_add(hgg_batch *b, hgg_handle *h, double dt, int32_t nsteps, int32_
         HGG_BCUDA(b, cudaEventCreateWithFlags(&c.done, cudaEventDisableTiming));
         b->classes.push_back(std::move(c));
         ci = (int)b->classes.size() - 1;
+        // default persistent grid: as many CTAs per SM as the class's kernel fits (the
+        // autotuner, where on, times the alternatives)
+        b->occ_query = true;
+        b->occ_result = 0;
+        launch_class_stage(b, b->classes[ci], 0, b->stream);
+        b->occ_query = false;
+        if (b->occ_result > 0) b->classes[ci].ctas_per_sm = std::min(b->occ_result, 8);
     }
     b->classes[ci].slots.push_back(free_slot);
     b->classes[ci].table_dirty = true;
