@@ -585,14 +585,15 @@ __global__ void __launch_bounds__(256) dense_stage(const StageIOT<KT> io, const 
 // The elements of a structured mesh fall into a few groups with the same
 // operator signature (the pair operators of every face; for the wave, whose
 // per-element work is the largest).  A
-// tile holds kGroupTile elements of one group; a block of kGroupTile * rows
-// threads runs it with lane = element and warp = output row, so every operator
+// tile holds group_tile_elems(NB) elements of one group (32, or 16 above 24 basis
+// functions); a block of that many threads per basis row runs it with lane =
+// element and warp = output row (two rows above 24), so every operator
 // entry a warp reads is the same address for all its lanes (one broadcast
 // instead of one sector per element), and the per-element staging arrays have
 // odd strides (in elements of CT), so the lanes' reads hit distinct banks.  The
 // stage inputs are staged and the outputs written through shared memory, both
 // coalesced along an element's coefficients.
-constexpr int kGroupTile = 32;  // elements per tile up to 24 basis functions
+constexpr int kGroupTile = 32;  // the largest tile (elements)
 // elements per tile: 32 (a warp of lanes per basis row), 16 above 24 basis functions (a
 // warp then covers two basis rows of 16 elements; the block stays within 1024 threads)
 __host__ __device__ constexpr int group_tile_elems(int nb) { return nb <= 24 ? 32 : 16; }

@@ -87,7 +87,7 @@ struct hgg_handle {
     int32_t *d_umma_tile_elems = nullptr, *d_umma_tile_mats = nullptr;
     unsigned char *d_umma_img = nullptr;
     unsigned char *d_umma_planes = nullptr;  // split stage input, two planes [E][KP]
-    // grouped dense kernel: tiles of kGroupTile elements with the same operator signature
+    // grouped dense kernel: tiles of group_tile_elems(nB) elements with the same operator signature
     int32_t *d_group_tiles = nullptr;
     double *d_win[2] = {nullptr, nullptr};  // stage inputs formed ahead (grouped wave kernel)
     int64_t group_tiles = 0;
