@@ -30,7 +30,7 @@
 namespace hgg {
 
 template <typename KT>
-struct DenseItem {
+struct alignas(16) DenseItem {
     StageIOT<KT> io[2];  // [parity]: from sol[base] / from sol[1 - base]
     DenseGeom g;
     const int32_t *tiles;  // the wave on tiles of equal operators: the member's tiles (else null)
@@ -38,14 +38,14 @@ struct DenseItem {
     int slot;
 };
 template <typename KT>
-struct TensorItem {
+struct alignas(16) TensorItem {
     StageIOT<KT> io[2];
     TensorGeom geo;
     int64_t block0;
     int slot;
 };
 template <typename KT>
-struct SliceItem {
+struct alignas(16) SliceItem {
     StageIOT<KT> io[2];
     const double *geo;
     int64_t block0;
@@ -61,7 +61,7 @@ struct UmmaItem {
 };
 
 template <typename KT>
-struct LinearItem {
+struct alignas(16) LinearItem {
     StageIOT<KT> io[2];
     LinearGeom g;
     LinearTiles t;
@@ -81,6 +81,20 @@ __device__ __forceinline__ int find_item(const Item *items, int n, int64_t vb) {
     return lo;
 }
 
+// The item of the virtual block in shared memory: the stage bodies read its fields
+// (pointers, coefficients, sizes) many times, which from shared memory costs what the
+// one-problem kernels pay for their parameters, not an L1 load each.  Ends with a
+// barrier; the caller's loop begins with one, so the previous block is done with it.
+template <typename Item>
+__device__ __forceinline__ const Item &item_to_shared(const Item *items, int i, Item &s_item) {
+    static_assert(sizeof(Item) % 16 == 0, "items are copied in 16-byte chunks");
+    const int4 *src = reinterpret_cast<const int4 *>(items + i);
+    int4 *dst = reinterpret_cast<int4 *>(&s_item);
+    for (int k = threadIdx.x; k < (int)(sizeof(Item) / 16); k += blockDim.x) dst[k] = src[k];
+    __syncthreads();
+    return s_item;
+}
+
 template <typename KT, int DIM, int NFL, int WAVE, int NB>
 __global__ void __launch_bounds__(256)
     grouped_dense(const DenseItem<KT> *items, const int *n_items, const int64_t *total, const int *parity,
@@ -92,7 +106,9 @@ __global__ void __launch_bounds__(256)
         const int slot = items[i].slot;
         __syncthreads();  // shared memory of the previous virtual block is free
         if (remaining[slot] <= 0) continue;
-        dense_any_body<KT, DIM, NFL, WAVE, NB>(items[i].io[parity[slot]], items[i].g, vb - items[i].block0);
+        __shared__ DenseItem<KT> s_it;
+        const DenseItem<KT> &it = item_to_shared(items, i, s_it);
+        dense_any_body<KT, DIM, NFL, WAVE, NB>(it.io[parity[slot]], it.g, vb - it.block0);
     }
 }
 
@@ -108,8 +124,9 @@ __global__ void __launch_bounds__(group_threads(NB), 1024 / group_threads(NB) > 
         const int slot = items[i].slot;
         __syncthreads();
         if (remaining[slot] <= 0) continue;
-        wave_group_body<KT, DIM, NFL, NB>(items[i].io[parity[slot]], items[i].g, items[i].tiles,
-                                          vb - items[i].block0);
+        __shared__ DenseItem<KT> s_it;
+        const DenseItem<KT> &it = item_to_shared(items, i, s_it);
+        wave_group_body<KT, DIM, NFL, NB>(it.io[parity[slot]], it.g, it.tiles, vb - it.block0);
     }
 }
 
@@ -124,7 +141,9 @@ __global__ void __launch_bounds__(EPB *TensorConsts<P, DIM>::NB)
         const int slot = items[i].slot;
         __syncthreads();
         if (remaining[slot] <= 0) continue;
-        tensor_stage_body<KT, P, DIM, EPB>(items[i].io[parity[slot]], items[i].geo, tc, vb - items[i].block0);
+        __shared__ TensorItem<KT> s_it;
+        const TensorItem<KT> &it = item_to_shared(items, i, s_it);
+        tensor_stage_body<KT, P, DIM, EPB>(it.io[parity[slot]], it.geo, tc, vb - it.block0);
     }
 }
 
@@ -139,7 +158,9 @@ __global__ void __launch_bounds__(SliceShape::THREADS, sizeof(KT) == 4 ? 5 : (NF
         const int slot = items[i].slot;
         __syncthreads();
         if (remaining[slot] <= 0) continue;
-        tensor_slice_body<KT, NIN, NFIN>(items[i].io[parity[slot]], items[i].geo, op, vb - items[i].block0);
+        __shared__ SliceItem<KT> s_it;
+        const SliceItem<KT> &it = item_to_shared(items, i, s_it);
+        tensor_slice_body<KT, NIN, NFIN>(it.io[parity[slot]], it.geo, op, vb - it.block0);
     }
 }
 
@@ -154,7 +175,9 @@ __global__ void __launch_bounds__(256)
         const int slot = items[i].slot;
         __syncthreads();
         if (remaining[slot] <= 0) continue;
-        linear_tile_body<KT>(items[i].io[parity[slot]], items[i].g, items[i].t, vb - items[i].block0);
+        __shared__ LinearItem<KT> s_it;
+        const LinearItem<KT> &it = item_to_shared(items, i, s_it);
+        linear_tile_body<KT>(it.io[parity[slot]], it.g, it.t, vb - it.block0);
     }
 }
 
