@@ -69,13 +69,16 @@ struct alignas(16) LinearItem {
     int slot;
 };
 
-// item whose virtual blocks contain vb (items sorted by block0, block0[0] = 0)
-template <typename Item>
-__device__ __forceinline__ int find_item(const Item *items, int n, int64_t vb) {
+// item whose virtual blocks contain vb: binary search of the items' first blocks,
+// which the class table keeps as one compact array after the block total (total[1 + m]
+// = item m's block0, ascending, total[1] = 0), so the probes stay in a few cache lines
+// instead of touching one item record each
+__device__ __forceinline__ int find_item(const int64_t *total, int n, int64_t vb) {
+    const int64_t *block0 = total + 1;
     int lo = 0, hi = n - 1;
     while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
-        if (items[mid].block0 <= vb) lo = mid;
+        if (block0[mid] <= vb) lo = mid;
         else hi = mid - 1;
     }
     return lo;
@@ -102,7 +105,7 @@ __global__ void __launch_bounds__(256)
     const int n = *n_items;
     const int64_t nb = *total;
     for (int64_t vb = blockIdx.x; vb < nb; vb += gridDim.x) {
-        const int i = find_item(items, n, vb);
+        const int i = find_item(total, n, vb);
         const int slot = items[i].slot;
         __syncthreads();  // shared memory of the previous virtual block is free
         if (remaining[slot] <= 0) continue;
@@ -120,7 +123,7 @@ __global__ void __launch_bounds__(group_threads(NB), 1024 / group_threads(NB) > 
     const int n = *n_items;
     const int64_t nb = *total;
     for (int64_t vb = blockIdx.x; vb < nb; vb += gridDim.x) {
-        const int i = find_item(items, n, vb);
+        const int i = find_item(total, n, vb);
         const int slot = items[i].slot;
         __syncthreads();
         if (remaining[slot] <= 0) continue;
@@ -137,7 +140,7 @@ __global__ void __launch_bounds__(EPB *TensorConsts<P, DIM>::NB)
     const int n = *n_items;
     const int64_t nb = *total;
     for (int64_t vb = blockIdx.x; vb < nb; vb += gridDim.x) {
-        const int i = find_item(items, n, vb);
+        const int i = find_item(total, n, vb);
         const int slot = items[i].slot;
         __syncthreads();
         if (remaining[slot] <= 0) continue;
@@ -154,7 +157,7 @@ __global__ void __launch_bounds__(SliceShape::THREADS, sizeof(KT) == 4 ? 5 : (NF
     const int n = *n_items;
     const int64_t nb = *total;
     for (int64_t vb = blockIdx.x; vb < nb; vb += gridDim.x) {
-        const int i = find_item(items, n, vb);
+        const int i = find_item(total, n, vb);
         const int slot = items[i].slot;
         __syncthreads();
         if (remaining[slot] <= 0) continue;
@@ -171,7 +174,7 @@ __global__ void __launch_bounds__(256)
     const int n = *n_items;
     const int64_t nb = *total;
     for (int64_t vb = blockIdx.x; vb < nb; vb += gridDim.x) {
-        const int i = find_item(items, n, vb);
+        const int i = find_item(total, n, vb);
         const int slot = items[i].slot;
         __syncthreads();
         if (remaining[slot] <= 0) continue;
@@ -186,10 +189,11 @@ struct UmmaGroupedTiles {
     const UmmaItem *items;
     int n;
     int64_t nb;
+    const int64_t *totals;  // the block total, then the items' first blocks
     const int *parity, *remaining;
     __device__ int64_t total() const { return nb; }
     __device__ bool get(int64_t vt, StageIOT<float> &io, UmmaArgs &a, int64_t &tile) const {
-        const int i = find_item(items, n, vt);
+        const int i = find_item(totals, n, vt);
         const int slot = items[i].slot;
         if (remaining[slot] <= 0) return false;
         io = items[i].io[parity[slot]];
@@ -203,7 +207,7 @@ template <int KIND>
 __global__ void __launch_bounds__(kUmmaThreads, 1)
     grouped_umma(const UmmaItem *items, const int *n_items, const int64_t *total, const int *parity,
                  const int *remaining, const UmmaShape sh, int *status) {
-    umma_persistent<KIND>(sh, UmmaGroupedTiles{items, *n_items, *total, parity, remaining}, status);
+    umma_persistent<KIND>(sh, UmmaGroupedTiles{items, *n_items, *total, total, parity, remaining}, status);
 }
 
 // the split stage input of every member (blockIdx.y, then in steps of gridDim.y: member)
@@ -489,9 +493,10 @@ int upload_class(hgg_batch *b, BatchClass &c) {
         c.total_blocks += item_blocks(c, b->handles[slot]);
         c.total_elements += b->handles[slot]->op.nE;
     }
-    // layout of a staging buffer: the S item arrays, then n and the block total
+    // layout of a staging buffer: the S item arrays, then the block total followed by
+    // every item's first block, then n
     const size_t items = c.item_bytes * (size_t)b->cap;
-    const size_t need = items * c.S + 16;
+    const size_t need = items * c.S + 8 * (size_t)(b->cap + 1) + 16;
     const int u = c.up_next;
     c.up_next ^= 1;
     if (!c.h_up[u] || c.up_bytes < need) {
@@ -519,10 +524,17 @@ int upload_class(hgg_batch *b, BatchClass &c) {
     }
     unsigned char *tail = stage + items * c.S;
     const int n = (int)c.slots.size();
-    std::memcpy(tail, &c.total_blocks, sizeof(int64_t));
-    std::memcpy(tail + 8, &n, sizeof(int));
-    HGG_BCUDA(b, cudaMemcpyAsync(c.d_total, tail, sizeof(int64_t), cudaMemcpyHostToDevice, b->stream));
-    HGG_BCUDA(b, cudaMemcpyAsync(c.d_n, tail + 8, sizeof(int), cudaMemcpyHostToDevice, b->stream));
+    int64_t *totals = reinterpret_cast<int64_t *>(tail);
+    totals[0] = c.total_blocks;
+    int64_t first = 0;
+    for (int m = 0; m < n; ++m) {
+        totals[1 + m] = first;
+        first += b->slot_blocks[c.slots[m]];
+    }
+    unsigned char *ntail = tail + 8 * (size_t)(b->cap + 1);
+    std::memcpy(ntail, &n, sizeof(int));
+    HGG_BCUDA(b, cudaMemcpyAsync(c.d_total, tail, sizeof(int64_t) * (1 + n), cudaMemcpyHostToDevice, b->stream));
+    HGG_BCUDA(b, cudaMemcpyAsync(c.d_n, ntail, sizeof(int), cudaMemcpyHostToDevice, b->stream));
     HGG_BCUDA(b, cudaEventRecord(c.up_done[u], b->stream));
     return 0;
 }
@@ -1085,7 +1097,7 @@ int hgg_batch_add(hgg_batch *b, hgg_handle *h, double dt, int32_t nsteps, int32_
         for (int st = 0; st < c.S; ++st)
             HGG_BCUDA(b, cudaMallocAsync(&c.d_items[st], c.item_bytes * (size_t)b->cap, b->stream));
         HGG_BCUDA(b, cudaMallocAsync(&c.d_n, sizeof(int), b->stream));
-        HGG_BCUDA(b, cudaMallocAsync(&c.d_total, sizeof(int64_t), b->stream));
+        HGG_BCUDA(b, cudaMallocAsync(&c.d_total, sizeof(int64_t) * (1 + (size_t)b->cap), b->stream));
         HGG_BCUDA(b, cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking));
         HGG_BCUDA(b, cudaEventCreateWithFlags(&c.done, cudaEventDisableTiming));
         b->classes.push_back(std::move(c));
