@@ -182,10 +182,11 @@ __device__ __forceinline__ void linear_tile_body(const StageIOT<KT> &io, const L
                         if (r < rows && lane < kmax) v = A[(size_t)(r0 + r) * R + kc + lane];
                         As[r * kLinStride + lane] = v;
                     }
-                    for (int n = warp; n < kLinTileN; n += 8) {
+#pragma unroll
+                    for (int n = warp; n < kLinTileN; n += 8) {  // eight passes: loads issue together
                         const int32_t se = src[n];
                         double v = 0.0;
-                        if (se >= 0 && lane < kmax) v = stage_input(io, (int64_t)se * R + kc + lane);
+                        if (se >= 0 && lane < kmax) v = stage_input_few(io, (int64_t)se * R + kc + lane);
                         Bs[n * kLinStride + lane] = v;
                     }
                 }
