@@ -41,6 +41,7 @@ PROBLEMS = [
     ([2, 2, 2], True, 2, "wave", [1.0], "RK4_4", 1e-3, 5),              # dense, tets, wave
     ([6, 6], False, 1, "wave", [2.0], "RK4_4", 1e-3, 4),                # wave tiles, squares
     ([4, 4, 4], True, 2, "wave", [1.0], "RK4_4", 1e-3, 5),              # wave tiles, tets
+    ([4, 4, 4], True, 4, "wave", [0.9], "RK4_4", 2e-4, 3),              # 16-element tiles in the batch
     ([8, 8], False, 2, "advection", [1.0, 0.5], "DormandPrince", 1e-3, 3),  # other tableau
     ([32, 32], True, 4, "advection", [0.8, -0.6], "RK4_4", 2e-4, 4),  # folded operator, tiles
     ([32, 32], True, 5, "advection", [-0.6, 0.8], "RK4_4", 1e-4, 6),
@@ -78,7 +79,7 @@ def test_batch_matches_each_problem_alone(autotune):
         solvers.append(s)
         u0s.append(u0)
         slots.append(batch.add(s, pr[6], pr[7]))
-    assert batch.num_classes == 9
+    assert batch.num_classes == 10
     assert solvers[-1].handle.kernel_kind == "linear"
     batch.step(max(pr[7] for pr in PROBLEMS) + 2)  # extra steps: finished problems stay put
     batch.synchronize()
