@@ -371,7 +371,7 @@ int create_from_desc(const hgg_problem_desc *desc, hgg_handle *h, bool linear = 
         // mesh forms tiles (structured meshes); otherwise the dense kernel runs.
         // Split-BF16 runs folded tiles on the tensor cores (tcgen05) where the mesh forms
         // them (it has no other kernel); the FP32 form folds advection on triangles at
-        // p = 5.  The FP32 form of the wave stays matrix-free: on the served request mix
+        // p = 5 onto the FP64 DMMA tiles (FP32 stage vectors).  The FP32 form of the wave stays matrix-free: on the served request mix
         // its dense kernel measured 2-5x the DoF-updates/s of the TF32 tiles (triangles
         // at p = 1: 8.1e9 against 2.0e9; tetrahedra at p = 2: 5.2e9 against 3.5e9).
         const bool fold_tri = op.physics == HGG_PHYSICS_ADVECTION && op.shape == HGG_SHAPE_TRIANGLE &&
@@ -541,7 +541,10 @@ int attach_linear(hgg_handle *h, const LinearSystem &sys, int tiles_only) {
     const int ukind = h->precision == HGG_PRECISION_BF16X3 ? kUmmaBF16 : kUmmaTF32;
     const UmmaShape ush = umma_shape(R, lo.slots, ukind);
     // (plane rows of at most 512 bytes: a thread's copies of one item stay in registers)
-    if (h->mixed && umma_smem(ush) <= 227 * 1024 && ush.NP <= 256 && ush.KP * ush.es <= 512) {
+    // (the FP32 form of a folded matrix-free operator keeps the FP64 DMMA tiles: on the
+    // batched triangles at p = 5 they took 1.06 ms per step against 1.34 ms on TF32 x 3)
+    const bool umma_wanted = h->precision == HGG_PRECISION_BF16X3 || (h->mixed && tiles_only != 1);
+    if (umma_wanted && umma_smem(ush) <= 227 * 1024 && ush.NP <= 256 && ush.KP * ush.es <= 512) {
         u_tiles = make_tiles(kUmmaTileN, utel, utmat);
         if (!(u_tiles * kUmmaTileN <= 2 * lo.E)) u_tiles = 0;
     }
