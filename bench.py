@@ -249,12 +249,10 @@ def run_ours(args):
         if dist is not None:
             dist.barrier()
 
+    from hpgem_b200 import replicas
+
     def max_over_ranks(x):
-        if dist is None:
-            return x
-        tt = torch.tensor([x], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        return float(tt.item())
+        return replicas.max_over_ranks(x, dist, "cuda")
 
     # a dedicated (non-default) stream: the library launches on it, the events are recorded on it
     stream = torch.cuda.Stream()
